@@ -1,0 +1,1630 @@
+/*
+ * CPU oracle of the ray vs displaced-surface query. TEST INFRASTRUCTURE ONLY:
+ * used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+ * the checker, never by the product.
+ *
+ * A double-precision restatement of MangoSister/dmap's hot path
+ * (code/cpp/src, cited below by file:line). Parity is pinned two ways:
+ * against the reference sources compiled here with shim headers
+ * (oracle/_ref, built by oracle/Makefile) and against golden vectors of the
+ * reference's numpy pyramid (tests/golden). Operation order follows the
+ * reference; see dmap_oracle.h for the conventions.
+ */
+#include "dmap_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdatomic.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+/* ------------------------------------------------------------------------ */
+/* Small vector helpers (the Eigen subset the reference uses).               */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { double x, y; } v2;
+typedef struct { double x, y, z; } v3;
+
+static inline double dmin(double a, double b) { return b < a ? b : a; } /* std::min */
+static inline double dmax(double a, double b) { return a < b ? b : a; } /* std::max */
+static inline v2 V2(double x, double y) { v2 r = {x, y}; return r; }
+static inline v3 V3(double x, double y, double z) { v3 r = {x, y, z}; return r; }
+static inline v2 sub2(v2 a, v2 b) { return V2(a.x - b.x, a.y - b.y); }
+static inline v2 add2(v2 a, v2 b) { return V2(a.x + b.x, a.y + b.y); }
+static inline v2 mul2(double s, v2 a) { return V2(s * a.x, s * a.y); }
+static inline v2 min2(v2 a, v2 b) { return V2(dmin(a.x, b.x), dmin(a.y, b.y)); }
+static inline v2 max2(v2 a, v2 b) { return V2(dmax(a.x, b.x), dmax(a.y, b.y)); }
+static inline double dot2(v2 a, v2 b) { return a.x * b.x + a.y * b.y; }
+static inline v3 add3(v3 a, v3 b) { return V3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub3(v3 a, v3 b) { return V3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 mul3(double s, v3 a) { return V3(s * a.x, s * a.y, s * a.z); }
+static inline v3 div3(v3 a, double s) { return V3(a.x / s, a.y / s, a.z / s); }
+static inline double dot3(v3 a, v3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static inline v3 cross3(v3 a, v3 b)
+{
+    return V3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline double norm3(v3 a) { return sqrt(dot3(a, a)); }
+static inline v3 normalized3(v3 a)
+{
+    double z = dot3(a, a);
+    if (z > 0.0)
+        return div3(a, sqrt(z));
+    return a;
+}
+static inline double comp3(v3 a, int k) { return k == 0 ? a.x : k == 1 ? a.y : a.z; }
+static inline void set3(v3 *a, int k, double v)
+{
+    if (k == 0)
+        a->x = v;
+    else if (k == 1)
+        a->y = v;
+    else
+        a->z = v;
+}
+typedef struct { double m[3][3]; } m3;
+static inline v3 m3mul(const m3 *A, v3 v)
+{
+    return V3((A->m[0][0] * v.x + A->m[0][1] * v.y) + A->m[0][2] * v.z,
+              (A->m[1][0] * v.x + A->m[1][1] * v.y) + A->m[1][2] * v.z,
+              (A->m[2][0] * v.x + A->m[2][1] * v.y) + A->m[2][2] * v.z);
+}
+/* 3x3 inverse by cofactors (the Eigen fixed-size routine's structure). */
+static inline double cof3(const m3 *M, int i, int j)
+{
+    int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+    return M->m[i1][j1] * M->m[i2][j2] - M->m[i1][j2] * M->m[i2][j1];
+}
+static m3 m3inverse(const m3 *M)
+{
+    m3 R;
+    double c0 = cof3(M, 0, 0), c1 = cof3(M, 1, 0), c2 = cof3(M, 2, 0);
+    double det = (c0 * M->m[0][0] + c1 * M->m[1][0]) + c2 * M->m[2][0];
+    double invdet = 1.0 / det;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            R.m[i][j] = cof3(M, j, i) * invdet;
+    return R;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Affine forms, affine_form.cpp.                                            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { double c, a, b, k; } af;
+typedef struct { af x, y, z; } af3;
+typedef struct { double lo, hi; } ivl;
+
+static inline af AF(double c, double a, double b, double k) { af r = {c, a, b, k}; return r; }
+static inline ivl af_interval(af f) /* affine_form.h:50-54 */
+{
+    double e = (fabs(f.a) + fabs(f.b)) + f.k;
+    ivl r = {f.c - e, f.c + e};
+    return r;
+}
+static inline af af_add(af x, af y) /* affine_form.cpp:126-133 */
+{
+    return AF(x.c + y.c, x.a + y.a, x.b + y.b, x.k + y.k);
+}
+static inline af af_scale(double s, af x) /* affine_form.cpp:158-165 */
+{
+    return AF(x.c * s, x.a * s, x.b * s, x.k * fabs(s));
+}
+static inline af af_mul(af x, af r) /* affine_form.cpp:146-156 */
+{
+    double u = (fabs(x.a) + fabs(x.b)) + x.k;
+    double v = (fabs(r.a) + fabs(r.b)) + r.k;
+    double c0 = x.c;
+    af o;
+    o.c = c0 * r.c;
+    o.a = c0 * r.a + r.c * x.a;
+    o.b = c0 * r.b + r.c * x.b;
+    o.k = (fabs(r.c) * x.k + fabs(c0) * r.k) + u * v;
+    return o;
+}
+static inline double g_rsqrt(double x) { return 1.0 / sqrt(x); }
+static af af_rsqrt(af f) /* affine_form.cpp:173-185, Min-Range */
+{
+    ivl range = af_interval(f);
+    double lo = range.lo, hi = range.hi;
+    double alpha = -0.5 * g_rsqrt(hi) * g_rsqrt(hi) * g_rsqrt(hi);
+    double beta = 0.5 * (g_rsqrt(lo) + g_rsqrt(hi) - alpha * (lo + hi));
+    double delta = 0.5 * fabs(g_rsqrt(lo) - g_rsqrt(hi) - alpha * (lo - hi));
+    return AF(alpha * f.c + beta, alpha * f.a, alpha * f.b, fabs(alpha) * f.k + delta);
+}
+static inline af3 AF3(v3 c, v3 a, v3 b)
+{
+    af3 r = {AF(c.x, a.x, b.x, 0.0), AF(c.y, a.y, b.y, 0.0), AF(c.z, a.z, b.z, 0.0)};
+    return r;
+}
+static inline af *af3_comp(af3 *v, int k) { return k == 0 ? &v->x : k == 1 ? &v->y : &v->z; }
+static af af3_sq_length(const af3 *v) /* affine_form.cpp:187-194 */
+{
+    v3 xc = V3(v->x.c, v->y.c, v->z.c), xu = V3(v->x.a, v->y.a, v->z.a);
+    v3 xv = V3(v->x.b, v->y.b, v->z.b), xk = V3(v->x.k, v->y.k, v->z.k);
+    v3 dev = V3((fabs(xu.x) + fabs(xv.x)) + xk.x, (fabs(xu.y) + fabs(xv.y)) + xk.y,
+                (fabs(xu.z) + fabs(xv.z)) + xk.z);
+    double offset = 0.5 * dot3(dev, dev);
+    return AF(dot3(xc, xc) + offset, 2.0 * dot3(xc, xu), 2.0 * dot3(xc, xv), 2.0 * fabs(dot3(xc, xk)) + offset);
+}
+static void af3_normalize(af3 *v) /* affine_form.cpp:196-204 */
+{
+    af l = af3_sq_length(v);
+    if (af_interval(l).lo <= 0.0) {
+        v->x = v->y = v->z = AF(0.0, 0.0, 0.0, 1.0);
+        return;
+    }
+    af r = af_rsqrt(l);
+    v->x = af_mul(r, v->x);
+    v->y = af_mul(r, v->y);
+    v->z = af_mul(r, v->z);
+}
+static inline af3 af3_add(af3 a, af3 b) /* affine_form.cpp:206 */
+{
+    af3 r = {af_add(a.x, b.x), af_add(a.y, b.y), af_add(a.z, b.z)};
+    return r;
+}
+static inline af af_dot(v3 a, af3 b) /* affine_form.cpp:210 */
+{
+    return af_add(af_add(af_scale(a.x, b.x), af_scale(a.y, b.y)), af_scale(a.z, b.z));
+}
+static inline af3 af3_matmul(const m3 *A, af3 v) /* affine_form.cpp:212-215 */
+{
+    af3 r;
+    r.x = af_dot(V3(A->m[0][0], A->m[0][1], A->m[0][2]), v);
+    r.y = af_dot(V3(A->m[1][0], A->m[1][1], A->m[1][2]), v);
+    r.z = af_dot(V3(A->m[2][0], A->m[2][1], A->m[2][2]), v);
+    return r;
+}
+static inline af3 af3_scale_form(af s, af3 v) /* affine_form.h:100 */
+{
+    af3 r = {af_mul(s, v.x), af_mul(s, v.y), af_mul(s, v.z)};
+    return r;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Taylor pyramid, taylor_pyramid.cpp.                                       */
+/* ------------------------------------------------------------------------ */
+
+enum { CH_H0, CH_GU, CH_GV, CH_R, CH_RU, CH_RV, CH_HMIN, CH_HMAX, N_CH };
+
+typedef struct {
+    int m;
+    double *ch[N_CH];
+} o_level;
+
+struct o_pyramid {
+    int n_leaf, n_levels, build;
+    o_level *levels;
+};
+
+static void level_alloc(o_level *l, int m)
+{
+    l->m = m;
+    for (int c = 0; c < N_CH; ++c)
+        l->ch[c] = (double *)calloc((size_t)m * m, sizeof(double));
+}
+
+static void leaf_level(o_level *out, const double *V, int nodes, int n_leaf) /* taylor_pyramid.cpp:154-176 */
+{
+    level_alloc(out, n_leaf);
+    double w = 1.0 / n_leaf;
+    double s = 0.5 * w;
+    for (int j = 0; j < n_leaf; ++j) {
+        for (int i = 0; i < n_leaf; ++i) {
+            double v00 = V[(size_t)j * nodes + i], v10 = V[(size_t)j * nodes + i + 1];
+            double v01 = V[(size_t)(j + 1) * nodes + i], v11 = V[(size_t)(j + 1) * nodes + i + 1];
+            size_t k = (size_t)j * n_leaf + i;
+            out->ch[CH_H0][k] = 0.25 * (((v00 + v10) + v01) + v11);
+            out->ch[CH_GU][k] = 0.5 * ((v10 - v00) + (v11 - v01)) / w;
+            out->ch[CH_GV][k] = 0.5 * ((v01 - v00) + (v11 - v10)) / w;
+            double c3 = (((v00 - v10) - v01) + v11) / (w * w);
+            out->ch[CH_R][k] = fabs(c3) * s * s;
+            out->ch[CH_RU][k] = fabs(c3) * s;
+            out->ch[CH_RV][k] = fabs(c3) * s;
+            out->ch[CH_HMIN][k] = dmin(dmin(v00, v10), dmin(v01, v11));
+            out->ch[CH_HMAX][k] = dmax(dmax(v00, v10), dmax(v01, v11));
+        }
+    }
+}
+
+static void fold_level(o_level *out, const o_level *child) /* taylor_pyramid.cpp:186-247 */
+{
+    int m = child->m / 2;
+    level_alloc(out, m);
+    double s = 0.5 / m;
+    const double off[2] = {-0.5 * s, 0.5 * s};
+    const double corner_off[2] = {-0.5 * s, 0.5 * s};
+    for (int J = 0; J < m; ++J) {
+        for (int I = 0; I < m; ++I) {
+            size_t kp = (size_t)J * m + I;
+            double gu_hi = -INFINITY, gu_lo = INFINITY, gv_hi = -INFINITY, gv_lo = INFINITY;
+            double h_min = INFINITY, h_max = -INFINITY;
+            for (int a = 0; a < 2; ++a) {
+                for (int b = 0; b < 2; ++b) {
+                    size_t kc = (size_t)(2 * J + a) * child->m + (2 * I + b);
+                    gu_hi = dmax(gu_hi, child->ch[CH_GU][kc] + child->ch[CH_RU][kc]);
+                    gu_lo = dmin(gu_lo, child->ch[CH_GU][kc] - child->ch[CH_RU][kc]);
+                    gv_hi = dmax(gv_hi, child->ch[CH_GV][kc] + child->ch[CH_RV][kc]);
+                    gv_lo = dmin(gv_lo, child->ch[CH_GV][kc] - child->ch[CH_RV][kc]);
+                    h_min = dmin(h_min, child->ch[CH_HMIN][kc]);
+                    h_max = dmax(h_max, child->ch[CH_HMAX][kc]);
+                }
+            }
+            double gu_p = 0.5 * (gu_hi + gu_lo);
+            double gv_p = 0.5 * (gv_hi + gv_lo);
+            out->ch[CH_GU][kp] = gu_p;
+            out->ch[CH_RU][kp] = 0.5 * (gu_hi - gu_lo);
+            out->ch[CH_GV][kp] = gv_p;
+            out->ch[CH_RV][kp] = 0.5 * (gv_hi - gv_lo);
+            out->ch[CH_HMIN][kp] = h_min;
+            out->ch[CH_HMAX][kp] = h_max;
+            double upper = -INFINITY, lower = INFINITY;
+            for (int a = 0; a < 2; ++a) {
+                for (int b = 0; b < 2; ++b) {
+                    size_t kc = (size_t)(2 * J + a) * child->m + (2 * I + b);
+                    double dx = off[b], dy = off[a];
+                    double du_g = child->ch[CH_GU][kc] - gu_p;
+                    double dv_g = child->ch[CH_GV][kc] - gv_p;
+                    double base = (child->ch[CH_H0][kc] - child->ch[CH_GU][kc] * dx) - child->ch[CH_GV][kc] * dy;
+                    for (int cu = 0; cu < 2; ++cu) {
+                        for (int cv = 0; cv < 2; ++cv) {
+                            double corner = (base + du_g * (dx + corner_off[cu])) + dv_g * (dy + corner_off[cv]);
+                            upper = dmax(upper, corner + child->ch[CH_R][kc]);
+                            lower = dmin(lower, corner - child->ch[CH_R][kc]);
+                        }
+                    }
+                }
+            }
+            out->ch[CH_H0][kp] = 0.5 * (upper + lower);
+            out->ch[CH_R][kp] = 0.5 * (upper - lower);
+        }
+    }
+}
+
+/* taylor_pyramid.cpp:129-148 and :260-310 (the direct construction). */
+static void direct_level(o_level *out, const double *V, int nodes, int n_leaf, int level)
+{
+    int k = 1 << level;
+    int m = n_leaf >> level;
+    level_alloc(out, m);
+    double w = 1.0 / n_leaf;
+    double s_texel = 0.5 / n_leaf;
+    for (int J = 0; J < m; ++J) {
+        for (int I = 0; I < m; ++I) {
+            size_t kp = (size_t)J * m + I;
+            double gu_hi = -INFINITY, gu_lo = INFINITY, gv_hi = -INFINITY, gv_lo = INFINITY;
+            for (int b = 0; b < k; ++b) {
+                for (int a = 0; a < k; ++a) {
+                    int tj = J * k + b, ti = I * k + a;
+                    double v00 = V[(size_t)tj * nodes + ti], v10 = V[(size_t)tj * nodes + ti + 1];
+                    double v01 = V[(size_t)(tj + 1) * nodes + ti], v11 = V[(size_t)(tj + 1) * nodes + ti + 1];
+                    double c1 = 0.5 * ((v10 - v00) + (v11 - v01)) / w;
+                    double c2 = 0.5 * ((v01 - v00) + (v11 - v10)) / w;
+                    double c3 = (((v00 - v10) - v01) + v11) / (w * w);
+                    double spread = fabs(c3) * s_texel;
+                    gu_hi = dmax(gu_hi, c1 + spread);
+                    gu_lo = dmin(gu_lo, c1 - spread);
+                    gv_hi = dmax(gv_hi, c2 + spread);
+                    gv_lo = dmin(gv_lo, c2 - spread);
+                }
+            }
+            double gu = 0.5 * (gu_hi + gu_lo);
+            double gv = 0.5 * (gv_hi + gv_lo);
+            out->ch[CH_GU][kp] = gu;
+            out->ch[CH_RU][kp] = 0.5 * (gu_hi - gu_lo);
+            out->ch[CH_GV][kp] = gv;
+            out->ch[CH_RV][kp] = 0.5 * (gv_hi - gv_lo);
+            double upper = -INFINITY, lower = INFINITY, h_min = INFINITY, h_max = -INFINITY;
+            for (int b = 0; b <= k; ++b) {
+                double dv = (b - 0.5 * k) / n_leaf;
+                for (int a = 0; a <= k; ++a) {
+                    double du = (a - 0.5 * k) / n_leaf;
+                    double value = V[(size_t)(J * k + b) * nodes + (I * k + a)];
+                    double residual = (value - gu * du) - gv * dv;
+                    upper = dmax(upper, residual);
+                    lower = dmin(lower, residual);
+                    h_min = dmin(h_min, value);
+                    h_max = dmax(h_max, value);
+                }
+            }
+            out->ch[CH_H0][kp] = 0.5 * (upper + lower);
+            out->ch[CH_R][kp] = 0.5 * (upper - lower);
+            out->ch[CH_HMIN][kp] = h_min;
+            out->ch[CH_HMAX][kp] = h_max;
+        }
+    }
+}
+
+o_pyramid *o_pyramid_build(const double *values, int nodes, double scale, double offset, int build)
+{
+    /* taylor_pyramid.cpp:324-360 */
+    int n = nodes - 1;
+    if (!(n >= 1 && (n & (n - 1)) == 0))
+        return NULL;
+    o_pyramid *p = (o_pyramid *)calloc(1, sizeof(o_pyramid));
+    p->n_leaf = n;
+    p->n_levels = 1;
+    while ((1 << p->n_levels) <= n)
+        ++p->n_levels;
+    p->build = build;
+    p->levels = (o_level *)calloc((size_t)p->n_levels, sizeof(o_level));
+    double *V = (double *)malloc((size_t)nodes * nodes * sizeof(double));
+    for (size_t k = 0; k < (size_t)nodes * nodes; ++k)
+        V[k] = values[k] * scale;
+    if (build == O_BUILD_FOLD) {
+        leaf_level(&p->levels[0], V, nodes, n);
+        for (int l = 1; l < p->n_levels; ++l)
+            fold_level(&p->levels[l], &p->levels[l - 1]);
+    } else {
+        for (int l = 0; l < p->n_levels; ++l)
+            direct_level(&p->levels[l], V, nodes, n, l);
+    }
+    free(V);
+    if (offset != 0.0) {
+        for (int l = 0; l < p->n_levels; ++l) {
+            size_t cells = (size_t)p->levels[l].m * p->levels[l].m;
+            for (size_t k = 0; k < cells; ++k) {
+                p->levels[l].ch[CH_H0][k] += offset;
+                p->levels[l].ch[CH_HMIN][k] += offset;
+                p->levels[l].ch[CH_HMAX][k] += offset;
+            }
+        }
+    }
+    return p;
+}
+
+void o_pyramid_free(o_pyramid *p)
+{
+    if (!p)
+        return;
+    for (int l = 0; l < p->n_levels; ++l)
+        for (int c = 0; c < N_CH; ++c)
+            free(p->levels[l].ch[c]);
+    free(p->levels);
+    free(p);
+}
+
+int o_pyramid_levels(const o_pyramid *p) { return p->n_levels; }
+int o_pyramid_n_leaf(const o_pyramid *p) { return p->n_leaf; }
+
+void o_pyramid_level(const o_pyramid *p, int level, double *out)
+{
+    size_t cells = (size_t)p->levels[level].m * p->levels[level].m;
+    for (int c = 0; c < N_CH; ++c)
+        memcpy(out + c * cells, p->levels[level].ch[c], cells * sizeof(double));
+}
+
+typedef struct { double h0, gu, gv, r, ru, rv, h_min, h_max; } o_node;
+
+static o_node pyramid_node(const o_pyramid *p, int level, int64_t i, int64_t j) /* taylor_pyramid.cpp:368-383 */
+{
+    o_node n;
+    if (level >= p->n_levels) {
+        const o_level *root = &p->levels[p->n_levels - 1];
+        double lo = root->ch[CH_HMIN][0], hi = root->ch[CH_HMAX][0];
+        n.h0 = 0.5 * (lo + hi);
+        n.gu = 0.0;
+        n.gv = 0.0;
+        n.r = 0.5 * (hi - lo);
+        n.ru = root->ch[CH_RU][0];
+        n.rv = root->ch[CH_RV][0];
+        n.h_min = lo;
+        n.h_max = hi;
+        return n;
+    }
+    const o_level *l = &p->levels[level];
+    int64_t ri = i % l->m, rj = j % l->m;
+    if (ri < 0)
+        ri += l->m;
+    if (rj < 0)
+        rj += l->m;
+    size_t k = (size_t)rj * l->m + ri;
+    n.h0 = l->ch[CH_H0][k];
+    n.gu = l->ch[CH_GU][k];
+    n.gv = l->ch[CH_GV][k];
+    n.r = l->ch[CH_R][k];
+    n.ru = l->ch[CH_RU][k];
+    n.rv = l->ch[CH_RV][k];
+    n.h_min = l->ch[CH_HMIN][k];
+    n.h_max = l->ch[CH_HMAX][k];
+    return n;
+}
+
+void o_pyramid_node(const o_pyramid *p, int level, int64_t i, int64_t j, double *out8)
+{
+    o_node n = pyramid_node(p, level, i, j);
+    memcpy(out8, &n, sizeof(n));
+}
+
+static inline double cell_width(const o_pyramid *p, int level) /* taylor_pyramid.h:94 */
+{
+    return ldexp(1.0, level) / p->n_leaf;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Height grid and base triangle, displaced_surface.cpp.                     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int W, H;
+    double scale;
+    const double *values;
+    double offset;
+    int repeat;
+} o_grid;
+
+static inline double grid_value(const o_grid *g, int j, int i) { return g->values[(size_t)j * g->W + i]; }
+
+static void grid_cell(const o_grid *g, double x, double y, int *i, int *j, double *s, double *t)
+{
+    /* displaced_surface.cpp:364-379 */
+    if (g->repeat) {
+        x -= floor(x);
+        y -= floor(y);
+    } else {
+        x = x < 0.0 ? 0.0 : (1.0 < x ? 1.0 : x);
+        y = y < 0.0 ? 0.0 : (1.0 < y ? 1.0 : y);
+    }
+    double fx = x * (g->W - 1);
+    double fy = y * (g->H - 1);
+    int ii = (int)fx, jj = (int)fy;
+    *i = g->W - 2 < ii ? g->W - 2 : ii;
+    *j = g->H - 2 < jj ? g->H - 2 : jj;
+    *s = fx - *i;
+    *t = fy - *j;
+}
+
+static double grid_h(const o_grid *g, double x, double y) /* displaced_surface.cpp:381-389 */
+{
+    int i, j;
+    double s, t;
+    grid_cell(g, x, y, &i, &j, &s, &t);
+    return g->scale * (((((1.0 - s) * (1.0 - t)) * grid_value(g, j, i) + (s * (1.0 - t)) * grid_value(g, j, i + 1)) +
+                        ((1.0 - s) * t) * grid_value(g, j + 1, i)) +
+                       (s * t) * grid_value(g, j + 1, i + 1)) +
+           g->offset;
+}
+
+static v2 grid_grad(const o_grid *g, double x, double y) /* displaced_surface.cpp:391-399 */
+{
+    int i, j;
+    double s, t;
+    grid_cell(g, x, y, &i, &j, &s, &t);
+    double dh_ds = (1.0 - t) * (grid_value(g, j, i + 1) - grid_value(g, j, i)) +
+                   t * (grid_value(g, j + 1, i + 1) - grid_value(g, j + 1, i));
+    double dh_dt = (1.0 - s) * (grid_value(g, j + 1, i) - grid_value(g, j, i)) +
+                   s * (grid_value(g, j + 1, i + 1) - grid_value(g, j, i + 1));
+    return V2(g->scale * (dh_ds * (g->W - 1)), g->scale * (dh_dt * (g->H - 1)));
+}
+
+typedef struct {
+    v3 q0, e1, e2, m0, Mu, Mv;
+    v3 p0, p1, p2;
+    v2 t0, t1, t2;
+    double J[2][2];
+} o_tri;
+
+static int tri_init(o_tri *T, const double *r) /* displaced_surface.cpp:406-443 */
+{
+    v3 p0 = V3(r[0], r[1], r[2]), p1 = V3(r[3], r[4], r[5]), p2 = V3(r[6], r[7], r[8]);
+    v3 m0 = V3(r[9], r[10], r[11]), m1 = V3(r[12], r[13], r[14]), m2 = V3(r[15], r[16], r[17]);
+    v2 t0 = V2(r[18], r[19]), t1 = V2(r[20], r[21]), t2 = V2(r[22], r[23]);
+    T->p0 = p0;
+    T->p1 = p1;
+    T->p2 = p2;
+    T->t0 = t0;
+    T->t1 = t1;
+    T->t2 = t2;
+    v3 eb1 = sub3(p1, p0), eb2 = sub3(p2, p0);
+    v3 Mb1 = sub3(m1, m0), Mb2 = sub3(m2, m0);
+    double T00 = t1.x - t0.x, T10 = t1.y - t0.y, T01 = t2.x - t0.x, T11 = t2.y - t0.y;
+    double det = T00 * T11 - T10 * T01;
+    if (!(fabs(det) > 1e-30))
+        return 0;
+    double invdet = 1.0 / det;
+    T->J[0][0] = T11 * invdet;
+    T->J[1][0] = -T10 * invdet;
+    T->J[0][1] = -T01 * invdet;
+    T->J[1][1] = T00 * invdet;
+    double (*J)[2] = T->J;
+    /* E = [eb1 eb2], D = [Mb1 Mb2]; EJ = E J, DJ = D J, c = -J t0. */
+    v2 c = V2((-J[0][0]) * t0.x + (-J[0][1]) * t0.y, (-J[1][0]) * t0.x + (-J[1][1]) * t0.y);
+    for (int a = 0; a < 3; ++a) {
+        double E0 = comp3(eb1, a), E1 = comp3(eb2, a), D0 = comp3(Mb1, a), D1 = comp3(Mb2, a);
+        set3(&T->q0, a, comp3(p0, a) + (E0 * c.x + E1 * c.y));
+        set3(&T->e1, a, E0 * J[0][0] + E1 * J[1][0]);
+        set3(&T->e2, a, E0 * J[0][1] + E1 * J[1][1]);
+        set3(&T->m0, a, comp3(m0, a) + (D0 * c.x + D1 * c.y));
+        set3(&T->Mu, a, D0 * J[0][0] + D1 * J[1][0]);
+        set3(&T->Mv, a, D0 * J[0][1] + D1 * J[1][1]);
+    }
+    return 1;
+}
+
+static inline v3 tri_P(const o_tri *T, double s, double t) /* displaced_surface.h:300 */
+{
+    return add3(add3(T->q0, mul3(s, T->e1)), mul3(t, T->e2));
+}
+static inline v3 tri_M(const o_tri *T, double s, double t) /* displaced_surface.h:301 */
+{
+    return add3(add3(T->m0, mul3(s, T->Mu)), mul3(t, T->Mv));
+}
+static inline v2 tri_bary(const o_tri *T, double s, double t) /* displaced_surface.h:303 */
+{
+    double x = s - T->t0.x, y = t - T->t0.y;
+    return V2(T->J[0][0] * x + T->J[0][1] * y, T->J[1][0] * x + T->J[1][1] * y);
+}
+static inline v2 tri_param(const o_tri *T, double u, double v) /* displaced_surface.h:304 */
+{
+    return add2(add2(T->t0, mul2(u, sub2(T->t1, T->t0))), mul2(v, sub2(T->t2, T->t0)));
+}
+
+typedef struct { v3 N, Nu, Nv; } o_nframe;
+
+static o_nframe normal_frame_at(const o_tri *T, double s, double t) /* displaced_surface.cpp:451-460 */
+{
+    v3 M = tri_M(T, s, t);
+    double Mlen = norm3(M);
+    o_nframe f;
+    f.N = div3(M, Mlen);
+    f.Nu = div3(sub3(T->Mu, mul3(dot3(f.N, T->Mu), f.N)), Mlen);
+    f.Nv = div3(sub3(T->Mv, mul3(dot3(f.N, T->Mv), f.N)), Mlen);
+    return f;
+}
+
+static v3 displaced_position(const o_tri *T, const o_grid *g, double s, double t) /* displaced_surface.cpp:514-518 */
+{
+    o_nframe f = normal_frame_at(T, s, t);
+    return add3(tri_P(T, s, t), mul3(grid_h(g, s, t), f.N));
+}
+
+static double mean_edge(const o_tri *T) /* displaced_surface.cpp:520-523 */
+{
+    return ((norm3(sub3(T->p1, T->p0)) + norm3(sub3(T->p2, T->p0))) + norm3(sub3(T->p2, T->p1))) / 3.0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* UV domain, uv_clip.cpp.                                                   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    v2 t[3], n[3];
+    double d[3];
+    v2 lo, hi;
+} o_uvtri;
+
+enum { OUTSIDE = 0, INSIDE = 1, STRADDLE = 2 };
+
+static void uvtri_init(o_uvtri *U, v2 t0, v2 t1, v2 t2) /* uv_clip.cpp:10-25 */
+{
+    U->t[0] = t0;
+    U->t[1] = t1;
+    U->t[2] = t2;
+    v2 a = sub2(t1, t0), b = sub2(t2, t0);
+    double signed_area = 0.5 * (a.x * b.y - a.y * b.x);
+    double orient = signed_area >= 0.0 ? 1.0 : -1.0;
+    for (int k = 0; k < 3; ++k) {
+        v2 e = sub2(U->t[(k + 1) % 3], U->t[k]);
+        U->n[k] = V2(orient * -e.y, orient * e.x);
+        U->d[k] = dot2(U->n[k], U->t[k]);
+    }
+    U->lo = min2(min2(t0, t1), t2);
+    U->hi = max2(max2(t0, t1), t2);
+}
+
+static inline int uvtri_inside(const o_uvtri *U, v2 p) /* uv_clip.h:409-415 */
+{
+    for (int k = 0; k < 3; ++k)
+        if (dot2(U->n[k], p) < U->d[k])
+            return 0;
+    return 1;
+}
+
+static int classify_square(const o_uvtri *U, v2 c, double s) /* uv_clip.cpp:27-44 */
+{
+    if (c.x + s <= U->lo.x || c.x - s >= U->hi.x || c.y + s <= U->lo.y || c.y - s >= U->hi.y)
+        return OUTSIDE;
+    int all_inside = 1;
+    for (int k = 0; k < 3; ++k) {
+        double proj = dot2(U->n[k], c);
+        double ext = (fabs(U->n[k].x) + fabs(U->n[k].y)) * s;
+        if (proj + ext <= U->d[k])
+            return OUTSIDE;
+        if (proj - ext < U->d[k])
+            all_inside = 0;
+    }
+    return all_inside ? INSIDE : STRADDLE;
+}
+
+/* descent_sampler.cpp:15-21,66-83 (TFDM's find_roots). */
+static void footprint_roots(const o_uvtri *U, int n_leaf, int *level, int64_t *i0, int64_t *j0)
+{
+    *level = 0;
+    for (;;) {
+        double w = ldexp(1.0, *level) / n_leaf;
+        int64_t ilo = (int64_t)floor(U->lo.x / w), ihi = (int64_t)ceil(U->hi.x / w) - 1;
+        int64_t jlo = (int64_t)floor(U->lo.y / w), jhi = (int64_t)ceil(U->hi.y / w) - 1;
+        if (ihi - ilo <= 1 && jhi - jlo <= 1) {
+            *i0 = ilo;
+            *j0 = jlo;
+            return;
+        }
+        ++*level;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Node bounds, node_bounds.cpp.                                             */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    m3 to_tangent;
+    v3 origin, ng;
+} o_frame;
+
+static void tangent_frame(o_frame *F, const o_tri *T) /* node_bounds.cpp:13-23 */
+{
+    F->origin = T->q0;
+    F->ng = normalized3(cross3(T->e1, T->e2));
+    m3 from;
+    for (int a = 0; a < 3; ++a) {
+        from.m[a][0] = comp3(T->e1, a);
+        from.m[a][1] = comp3(T->e2, a);
+        from.m[a][2] = comp3(F->ng, a);
+    }
+    F->to_tangent = m3inverse(&from);
+}
+
+typedef struct { v3 lo, hi; } o_box;
+
+static inline double interval_tolerance(double t_scale) /* node_bounds.cpp:128 */
+{
+    return 1e-9 * dmax(1.0, t_scale);
+}
+
+static int box_clip(const o_box *B, v3 o, v3 d, double *t0, double *t1) /* node_bounds.cpp:25-44 */
+{
+    for (int a = 0; a < 3; ++a) {
+        double da = comp3(d, a), oa = comp3(o, a);
+        if (da != 0.0) {
+            double ta = (comp3(B->lo, a) - oa) / da, tb = (comp3(B->hi, a) - oa) / da;
+            if (ta > tb) {
+                double x = ta;
+                ta = tb;
+                tb = x;
+            }
+            *t0 = dmax(*t0, ta);
+            *t1 = dmin(*t1, tb);
+        } else if (oa < comp3(B->lo, a) || oa > comp3(B->hi, a)) {
+            return 0;
+        }
+    }
+    if (*t0 > *t1 + interval_tolerance(dmax(fabs(*t0), fabs(*t1))))
+        return 0;
+    if (*t0 > *t1) {
+        double x = *t0;
+        *t0 = *t1;
+        *t1 = x;
+    }
+    return 1;
+}
+
+static void box_expand(o_box *B, const o_box *o) /* node_bounds.cpp:54-58 */
+{
+    B->lo = V3(dmin(B->lo.x, o->lo.x), dmin(B->lo.y, o->lo.y), dmin(B->lo.z, o->lo.z));
+    B->hi = V3(dmax(B->hi.x, o->hi.x), dmax(B->hi.y, o->hi.y), dmax(B->hi.z, o->hi.z));
+}
+
+static o_box hull(af3 S) /* node_bounds.cpp:70-79 */
+{
+    o_box b;
+    for (int a = 0; a < 3; ++a) {
+        ivl r = af_interval(*af3_comp(&S, a));
+        set3(&b.lo, a, r.lo);
+        set3(&b.hi, a, r.hi);
+    }
+    return b;
+}
+
+typedef struct {
+    int level;
+    int64_t i, j;
+    o_node node;
+    v2 centre;
+    af3 m;
+    o_box box;
+} o_nodebound;
+
+static void node_bound(o_nodebound *nb, const o_tri *T, const o_frame *F, const o_pyramid *P, int level, int64_t i,
+                       int64_t j) /* node_bounds.cpp:83-109 */
+{
+    nb->level = level;
+    nb->i = i;
+    nb->j = j;
+    nb->node = pyramid_node(P, level, i, j);
+    double w = cell_width(P, level);
+    nb->centre = V2((i + 0.5) * w, (j + 0.5) * w);
+    v2 tri_lo = min2(min2(T->t0, T->t1), T->t2), tri_hi = max2(max2(T->t0, T->t1), T->t2);
+    v2 rect_lo = max2(V2(i * w, j * w), tri_lo);
+    v2 rect_hi = min2(V2((i + 1) * w, (j + 1) * w), tri_hi);
+    v2 c = mul2(0.5, add2(rect_lo, rect_hi));
+    v2 hh = mul2(0.5, sub2(rect_hi, rect_lo));
+    v2 half = V2(dmax(hh.x, 0.0), dmax(hh.y, 0.0));
+    /* normal_form, node_bounds.cpp:66-69 */
+    af3 N = AF3(add3(add3(T->m0, mul3(c.x, T->Mu)), mul3(c.y, T->Mv)), mul3(half.x, T->Mu), mul3(half.y, T->Mv));
+    af3_normalize(&N);
+    nb->m = af3_matmul(&F->to_tangent, N);
+    af h = AF(0.5 * (nb->node.h_min + nb->node.h_max), 0.0, 0.0, 0.5 * (nb->node.h_max - nb->node.h_min));
+    af3 p = AF3(V3(c.x, c.y, 0.0), V3(half.x, 0.0, 0.0), V3(0.0, half.y, 0.0));
+    nb->box = hull(af3_add(p, af3_scale_form(h, nb->m)));
+}
+
+static inline ivl IV(double lo, double hi) { ivl r = {lo, hi}; return r; }
+static inline ivl iv_add(ivl a, ivl b) { return IV(a.lo + b.lo, a.hi + b.hi); }
+static inline ivl iv_adds(ivl a, double b) { return IV(a.lo + b, a.hi + b); }
+static inline ivl iv_scale(double s, ivl a) /* affine_form.cpp:121-124 */
+{
+    return s >= 0.0 ? IV(s * a.lo, s * a.hi) : IV(s * a.hi, s * a.lo);
+}
+
+typedef struct {
+    ivl A, B, C, D;
+    double R;
+} o_slab;
+
+static o_slab slab_form(const o_nodebound *nb) /* node_bounds.cpp:111-122 */
+{
+    const o_node *n = &nb->node;
+    ivl mx = af_interval(nb->m.x), my = af_interval(nb->m.y), mz = af_interval(nb->m.z);
+    o_slab f;
+    f.A = iv_add(iv_add(IV(1.0, 1.0), iv_scale(n->gu, mx)), iv_scale(n->gv, my));
+    f.B = iv_scale(-n->gu, mz);
+    f.C = iv_scale(-n->gv, mz);
+    f.D = iv_scale(-((n->h0 - n->gu * nb->centre.x) - n->gv * nb->centre.y), mz);
+    f.R = n->r * dmax(fabs(mz.lo), fabs(mz.hi));
+    return f;
+}
+
+typedef struct {
+    v3 o, d;
+    double t_min, t_max;
+} o_tray;
+
+static int box_interval(const o_nodebound *nb, const o_tray *ray, double *t0, double *t1) /* node_bounds.cpp:130-135 */
+{
+    *t0 = ray->t_min;
+    *t1 = ray->t_max;
+    return box_clip(&nb->box, ray->o, ray->d, t0, t1);
+}
+
+static int slab_interval(const o_nodebound *nb, const o_tray *ray, double *t0, double *t1) /* node_bounds.cpp:137-179 */
+{
+    o_box column = nb->box;
+    column.lo.z = -INFINITY;
+    column.hi.z = INFINITY;
+    *t0 = ray->t_min;
+    *t1 = ray->t_max;
+    if (!box_clip(&column, ray->o, ray->d, t0, t1))
+        return 0;
+    v3 anchor = add3(ray->o, mul3(*t0, ray->d));
+    double span = *t1 - *t0;
+    o_slab f = slab_form(nb);
+    ivl F0 = iv_add(iv_add(iv_add(iv_scale(anchor.z, f.A), iv_scale(anchor.x, f.B)), iv_scale(anchor.y, f.C)), f.D);
+    ivl F1 = iv_add(iv_add(iv_scale(ray->d.z, f.A), iv_scale(ray->d.x, f.B)), iv_scale(ray->d.y, f.C));
+    double s0 = 0.0, s1 = span;
+    if (F1.lo > 0.0)
+        s1 = dmin(s1, (f.R - F0.lo) / F1.lo);
+    else if (F1.lo < 0.0)
+        s0 = dmax(s0, (f.R - F0.lo) / F1.lo);
+    else if (F0.lo > f.R)
+        return 0;
+    if (F1.hi > 0.0)
+        s0 = dmax(s0, (-f.R - F0.hi) / F1.hi);
+    else if (F1.hi < 0.0)
+        s1 = dmin(s1, (-f.R - F0.hi) / F1.hi);
+    else if (F0.hi < -f.R)
+        return 0;
+    if (s0 > s1 + interval_tolerance(fabs(*t0) + span))
+        return 0;
+    if (s0 > s1) {
+        double x = s0;
+        s0 = s1;
+        s1 = x;
+    }
+    *t1 = *t0 + s1;
+    *t0 = *t0 + s0;
+    return 1;
+}
+
+static int both_interval(const o_nodebound *nb, const o_tray *ray, double *t0, double *t1) /* node_bounds.cpp:181-197 */
+{
+    double b0, b1, s0, s1;
+    if (!box_interval(nb, ray, &b0, &b1) || !slab_interval(nb, ray, &s0, &s1))
+        return 0;
+    *t0 = dmax(b0, s0);
+    *t1 = dmin(b1, s1);
+    double tol = interval_tolerance(dmax(fabs(*t0), fabs(*t1)));
+    if (*t0 > *t1 + tol)
+        return 0;
+    if (*t0 > *t1) {
+        double x = *t0;
+        *t0 = *t1;
+        *t1 = x;
+    }
+    return 1;
+}
+
+static int node_interval(const o_nodebound *nb, const o_tray *ray, int bound, int slab_max_level, double *t0,
+                         double *t1) /* node_bounds.cpp:199-211 */
+{
+    int read_slab = nb->level <= slab_max_level;
+    switch (bound) {
+    case O_BOUND_BOX:
+        return box_interval(nb, ray, t0, t1);
+    case O_BOUND_SLAB:
+        return read_slab ? slab_interval(nb, ray, t0, t1) : box_interval(nb, ray, t0, t1);
+    case O_BOUND_BOTH:
+        return read_slab ? both_interval(nb, ray, t0, t1) : box_interval(nb, ray, t0, t1);
+    }
+    return 0;
+}
+
+static void height_range_walk(const o_uvtri *U, const o_pyramid *P, int level, int64_t i, int64_t j, double *h_min,
+                              double *h_max) /* node_bounds.cpp:218-234 */
+{
+    double w = cell_width(P, level);
+    v2 c = V2((i + 0.5) * w, (j + 0.5) * w);
+    int overlap = classify_square(U, c, 0.5 * w);
+    if (overlap == OUTSIDE)
+        return;
+    if (overlap == INSIDE || level == 0) {
+        o_node n = pyramid_node(P, level, i, j);
+        *h_min = dmin(*h_min, n.h_min);
+        *h_max = dmax(*h_max, n.h_max);
+        return;
+    }
+    for (int ch = 0; ch < 4; ++ch)
+        height_range_walk(U, P, level - 1, 2 * i + (ch & 1), 2 * j + (ch >> 1), h_min, h_max);
+}
+
+static void triangle_height_range(const o_tri *T, const o_pyramid *P, double *h_min, double *h_max)
+{
+    /* node_bounds.cpp:238-249 */
+    o_uvtri U;
+    uvtri_init(&U, T->t0, T->t1, T->t2);
+    int level;
+    int64_t i0, j0;
+    footprint_roots(&U, P->n_leaf, &level, &i0, &j0);
+    *h_min = INFINITY;
+    *h_max = -INFINITY;
+    for (int ch = 0; ch < 4; ++ch)
+        height_range_walk(&U, P, level, i0 + (ch & 1), j0 + (ch >> 1), h_min, h_max);
+}
+
+static o_box triangle_aabb(const o_tri *T, double h_min, double h_max) /* node_bounds.cpp:251-269 */
+{
+    const v2 t[3] = {T->t0, T->t1, T->t2};
+    af h = AF(0.5 * (h_min + h_max), 0.0, 0.0, 0.5 * (h_max - h_min));
+    o_box box = {V3(INFINITY, INFINITY, INFINITY), V3(-INFINITY, -INFINITY, -INFINITY)};
+    for (int k = 0; k < 3; ++k) {
+        v2 tk = t[k], tk1 = t[(k + 1) % 3], tk2 = t[(k + 2) % 3];
+        v2 c = add2(add2(mul2(0.5, tk), mul2(0.25, tk1)), mul2(0.25, tk2));
+        v2 du = mul2(0.25, sub2(tk1, tk)), dv = mul2(0.25, sub2(tk2, tk));
+        af3 Pf = AF3(tri_P(T, c.x, c.y), add3(mul3(du.x, T->e1), mul3(du.y, T->e2)),
+                     add3(mul3(dv.x, T->e1), mul3(dv.y, T->e2)));
+        af3 Nf = AF3(tri_M(T, c.x, c.y), add3(mul3(du.x, T->Mu), mul3(du.y, T->Mv)),
+                     add3(mul3(dv.x, T->Mu), mul3(dv.y, T->Mv)));
+        af3_normalize(&Nf);
+        o_box b = hull(af3_add(Pf, af3_scale_form(h, Nf)));
+        box_expand(&box, &b);
+    }
+    return box;
+}
+
+/* ------------------------------------------------------------------------ */
+/* The walk and the leaves, displaced_intersector.cpp.                       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int level;
+    int64_t i, j;
+} o_cell;
+
+static inline int64_t floor_div2(int64_t x) { return x >= 0 ? x / 2 : -((-x + 1) / 2); } /* :18 */
+static inline int floor_mod2(int64_t x) { return (int)(x - 2 * floor_div2(x)); }            /* :19 */
+static inline void cell_up(o_cell *c)                                                       /* :85-90 */
+{
+    ++c->level;
+    c->i = floor_div2(c->i);
+    c->j = floor_div2(c->j);
+}
+static inline void cell_down(o_cell *c, int si, int sj) /* :92-97 */
+{
+    --c->level;
+    c->i = 2 * c->i + (si ? 1 : 0);
+    c->j = 2 * c->j + (sj ? 1 : 0);
+}
+static void cell_next(o_cell *c, int si, int sj, int root_level) /* :99-121 */
+{
+    for (;;) {
+        int code = 2 * floor_mod2(c->i + (si ? 1 : 0)) + floor_mod2(c->j + (sj ? 1 : 0));
+        switch (code) {
+        case 1:
+            c->j += sj ? 1 : -1;
+            c->i += si ? -1 : 1;
+            return;
+        case 3:
+            cell_up(c);
+            if (c->level > root_level)
+                return;
+            break;
+        default:
+            c->j += sj ? -1 : 1;
+            return;
+        }
+    }
+}
+
+typedef struct {
+    const o_tri *tri;
+    const o_pyramid *pyr;
+    const o_grid *field;
+    o_frame frame;
+    o_uvtri domain;
+    int root_level;
+    o_cell roots[4];
+    int n_roots;
+    double residual_tolerance;
+    int max_iterations, subdivision_depth;
+    o_box box;
+    double h_min, h_max;
+} o_isect;
+
+typedef struct {
+    double t;
+    v2 st, bary;
+    v3 ng;
+    int64_t i, j;
+} o_hit;
+
+static void isect_init(o_isect *X, const o_tri *T, const o_pyramid *P, const o_grid *g) /* :135-151 */
+{
+    X->tri = T;
+    X->pyr = P;
+    X->field = g;
+    tangent_frame(&X->frame, T);
+    uvtri_init(&X->domain, T->t0, T->t1, T->t2);
+    int64_t i0, j0;
+    footprint_roots(&X->domain, P->n_leaf, &X->root_level, &i0, &j0);
+    double w = cell_width(P, X->root_level);
+    int64_t i_lo = (int64_t)floor(X->domain.lo.x / w), i_hi = (int64_t)ceil(X->domain.hi.x / w) - 1;
+    int64_t j_lo = (int64_t)floor(X->domain.lo.y / w), j_hi = (int64_t)ceil(X->domain.hi.y / w) - 1;
+    X->n_roots = 0;
+    for (int64_t j = j_lo; j <= j_hi; ++j)
+        for (int64_t i = i_lo; i <= i_hi; ++i) {
+            o_cell c = {X->root_level, i, j};
+            X->roots[X->n_roots++] = c;
+        }
+    X->residual_tolerance = 1e-10 * mean_edge(T);
+    X->max_iterations = 20;
+    X->subdivision_depth = 5;
+}
+
+static void plane_basis(v3 n, v3 *d1, v3 *d2) /* :222-227 */
+{
+    v3 a = fabs(n.x) < 0.9 ? V3(1.0, 0.0, 0.0) : V3(0.0, 1.0, 0.0);
+    *d1 = normalized3(cross3(a, n));
+    *d2 = cross3(n, *d1);
+}
+
+static int ray_triangle(v3 o, v3 d, double t_min, double t_max, v3 A, v3 B, v3 C, double *t, double *b1,
+                        double *b2) /* :230-249 */
+{
+    v3 e1 = sub3(B, A), e2 = sub3(C, A);
+    v3 p = cross3(d, e2);
+    double det = dot3(e1, p);
+    if (det == 0.0)
+        return 0;
+    double inv = 1.0 / det;
+    v3 s = sub3(o, A);
+    *b1 = dot3(s, p) * inv;
+    if (*b1 < 0.0 || *b1 > 1.0)
+        return 0;
+    v3 q = cross3(s, e1);
+    *b2 = dot3(d, q) * inv;
+    if (*b2 < 0.0 || *b1 + *b2 > 1.0)
+        return 0;
+    *t = dot3(e2, q) * inv;
+    return *t > t_min && *t < t_max;
+}
+
+typedef struct {
+    v2 lo;
+    double w;
+    double h00, h10, h01, h11;
+    af3 N_hat;
+    v3 o, d, dn, d1, d2;
+    double d_len;
+} o_leafbound;
+
+static inline af restricted(af f, double a, double b, double rho) /* :272-276 */
+{
+    double alpha = 2.0 * a - 1.0, beta = 2.0 * b - 1.0, r = 2.0 * rho;
+    return AF((f.c + f.a * alpha) + f.b * beta, f.a * r, f.b * r, f.k);
+}
+
+static int newton_from(const o_isect *X, v3 o, v3 d, double t_min, double t_max, int64_t i, int64_t j, v2 guess,
+                       o_hit *hit, int64_t *iters) /* :325-388 */
+{
+    const o_tri *T = X->tri;
+    double w = cell_width(X->pyr, 0);
+    v2 lo = V2(i * w, j * w), hi = V2((i + 1) * w, (j + 1) * w);
+    double d_len = norm3(d);
+    v3 dn = div3(d, d_len), d1, d2;
+    plane_basis(dn, &d1, &d2);
+    double prev_err2 = INFINITY;
+    int err_streak = 0, behind_streak = 0, invalid_streak = 0;
+    for (int iter = 0; iter < X->max_iterations; ++iter) {
+        if (iters)
+            ++*iters;
+        double s = guess.x, t = guess.y;
+        o_nframe f = normal_frame_at(T, s, t);
+        double h = grid_h(X->field, s, t);
+        v2 gh = grid_grad(X->field, s, t);
+        v3 S = add3(tri_P(T, s, t), mul3(h, f.N));
+        v3 delta = sub3(S, o);
+        v2 F = V2(dot3(delta, d1), dot3(delta, d2));
+        double err2 = F.x * F.x + F.y * F.y;
+        double along = dot3(delta, dn);
+        err_streak = err2 > prev_err2 ? err_streak + 1 : 0;
+        behind_streak = along < 0.0 ? behind_streak + 1 : 0;
+        if (err_streak >= 2 || behind_streak >= 2)
+            return 0;
+        prev_err2 = err2;
+        v3 Su = add3(add3(T->e1, mul3(gh.x, f.N)), mul3(h, f.Nu));
+        v3 Sv = add3(add3(T->e2, mul3(gh.y, f.N)), mul3(h, f.Nv));
+        if (err2 < X->residual_tolerance * X->residual_tolerance) {
+            if (along < 0.0 || !uvtri_inside(&X->domain, guess))
+                return 0;
+            double t_hit = along / d_len;
+            if (t_hit <= t_min || t_hit >= t_max)
+                return 0;
+            hit->t = t_hit;
+            hit->st = guess;
+            hit->bary = tri_bary(T, s, t);
+            hit->ng = normalized3(cross3(Su, Sv));
+            hit->i = i;
+            hit->j = j;
+            return 1;
+        }
+        double J00 = dot3(d1, Su), J01 = dot3(d1, Sv), J10 = dot3(d2, Su), J11 = dot3(d2, Sv);
+        double det = J00 * J11 - J01 * J10;
+        if (det == 0.0)
+            return 0;
+        v2 step = V2((J11 * F.x - J01 * F.y) / det, (-J10 * F.x + J00 * F.y) / det);
+        guess = sub2(guess, step);
+        int outside = guess.x < lo.x || guess.x > hi.x || guess.y < lo.y || guess.y > hi.y ||
+                      !uvtri_inside(&X->domain, guess);
+        if (outside) {
+            if (++invalid_streak >= 3)
+                return 0;
+            guess = min2(max2(guess, lo), hi);
+        } else {
+            invalid_streak = 0;
+        }
+    }
+    return 0;
+}
+
+static int sub_square_bound(const o_isect *X, const o_leafbound *L, double a, double b, double rho, double t_min,
+                            double t_max, double *t_lo) /* :266-290 */
+{
+    const o_tri *T = X->tri;
+    v2 c = add2(L->lo, mul2(L->w, V2(a, b)));
+    if (classify_square(&X->domain, c, L->w * rho) == OUTSIDE)
+        return 0;
+    double Tw = ((L->h11 - L->h10) - L->h01) + L->h00;
+    double ha = L->h10 - L->h00, hb = L->h01 - L->h00;
+    af h = AF(((L->h00 + ha * a) + hb * b) + Tw * a * b, (ha + Tw * b) * rho, (hb + Tw * a) * rho,
+              fabs(Tw) * rho * rho);
+    double wr = L->w * rho;
+    af3 P = AF3(tri_P(T, c.x, c.y), mul3(wr, T->e1), mul3(wr, T->e2));
+    af3 Nr = {restricted(L->N_hat.x, a, b, rho), restricted(L->N_hat.y, a, b, rho),
+              restricted(L->N_hat.z, a, b, rho)};
+    af3 S = af3_add(P, af3_scale_form(h, Nr));
+    af F1 = af_dot(L->d1, S), F2 = af_dot(L->d2, S);
+    F1.c -= dot3(L->d1, L->o);
+    F2.c -= dot3(L->d2, L->o);
+    ivl i1 = af_interval(F1), i2 = af_interval(F2);
+    if (!(i1.lo <= 0.0 && 0.0 <= i1.hi) || !(i2.lo <= 0.0 && 0.0 <= i2.hi))
+        return 0;
+    af along = af_dot(L->dn, S);
+    along.c -= dot3(L->dn, L->o);
+    ivl range = af_interval(along);
+    *t_lo = range.lo / L->d_len;
+    return *t_lo < t_max && range.hi / L->d_len > t_min;
+}
+
+static void search_leaf(const o_isect *X, const o_leafbound *L, int64_t i, int64_t j, int depth, double a, double b,
+                        double rho, double t_min, double *t_max, o_hit *hit, int *found, int64_t *sub_squares,
+                        int64_t *iters) /* :292-323 */
+{
+    if (depth == X->subdivision_depth) {
+        o_hit h;
+        if (newton_from(X, L->o, L->d, t_min, *t_max, i, j, add2(L->lo, mul2(L->w, V2(a, b))), &h, iters)) {
+            *hit = h;
+            *t_max = h.t;
+            *found = 1;
+        }
+        return;
+    }
+    struct { double a, b, t_lo; } ch[4];
+    int n = 0;
+    double r = 0.5 * rho;
+    for (int q = 0; q < 4; ++q) {
+        double ca = a + ((q & 1) ? r : -r), cb = b + ((q & 2) ? r : -r), t_lo;
+        ++*sub_squares;
+        if (sub_square_bound(X, L, ca, cb, r, t_min, *t_max, &t_lo)) {
+            ch[n].a = ca;
+            ch[n].b = cb;
+            ch[n].t_lo = t_lo;
+            ++n;
+        }
+    }
+    /* std::sort of at most four: stable insertion by t_lo. */
+    for (int p = 1; p < n; ++p) {
+        for (int q = p; q > 0 && ch[q].t_lo < ch[q - 1].t_lo; --q) {
+            double ta = ch[q].a, tb = ch[q].b, tt = ch[q].t_lo;
+            ch[q] = ch[q - 1];
+            ch[q - 1].a = ta;
+            ch[q - 1].b = tb;
+            ch[q - 1].t_lo = tt;
+        }
+    }
+    for (int q = 0; q < n; ++q) {
+        if (ch[q].t_lo >= *t_max)
+            break;
+        search_leaf(X, L, i, j, depth + 1, ch[q].a, ch[q].b, r, t_min, t_max, hit, found, sub_squares, iters);
+    }
+}
+
+static int intersect_newton(const o_isect *X, v3 o, v3 d, double t_min, double t_max, int64_t i, int64_t j,
+                            o_hit *hit, int64_t *sub_squares, int64_t *iters) /* :239-264 */
+{
+    const o_tri *T = X->tri;
+    o_leafbound L;
+    L.w = cell_width(X->pyr, 0);
+    L.lo = V2(i * L.w, j * L.w);
+    L.h00 = grid_h(X->field, L.lo.x, L.lo.y);
+    L.h10 = grid_h(X->field, L.lo.x + L.w, L.lo.y);
+    L.h01 = grid_h(X->field, L.lo.x, L.lo.y + L.w);
+    L.h11 = grid_h(X->field, L.lo.x + L.w, L.lo.y + L.w);
+    v2 c = add2(L.lo, V2(0.5 * L.w, 0.5 * L.w));
+    double hw = 0.5 * L.w;
+    L.N_hat = AF3(add3(add3(T->m0, mul3(c.x, T->Mu)), mul3(c.y, T->Mv)), mul3(hw, T->Mu), mul3(hw, T->Mv));
+    af3_normalize(&L.N_hat);
+    L.o = o;
+    L.d = d;
+    L.d_len = norm3(d);
+    L.dn = div3(d, L.d_len);
+    plane_basis(L.dn, &L.d1, &L.d2);
+    int found = 0;
+    int64_t count = 0;
+    search_leaf(X, &L, i, j, 0, 0.5, 0.5, 0.5, t_min, &t_max, hit, &found, &count, iters);
+    if (sub_squares)
+        *sub_squares += count;
+    return found;
+}
+
+static int intersect_two_triangle(const o_isect *X, v3 o, v3 d, double t_min, double t_max, int64_t i, int64_t j,
+                                  o_hit *hit) /* :390-426 */
+{
+    const o_tri *T = X->tri;
+    double w = cell_width(X->pyr, 0);
+    v2 st00 = V2(i * w, j * w), st10 = V2((i + 1) * w, j * w), st01 = V2(i * w, (j + 1) * w),
+       st11 = V2((i + 1) * w, (j + 1) * w);
+    v3 S00 = displaced_position(T, X->field, st00.x, st00.y);
+    v3 S10 = displaced_position(T, X->field, st10.x, st10.y);
+    v3 S01 = displaced_position(T, X->field, st01.x, st01.y);
+    v3 S11 = displaced_position(T, X->field, st11.x, st11.y);
+    v3 A[2] = {S00, S10}, B[2] = {S10, S11}, C[2] = {S01, S01};
+    v2 a[2] = {st00, st10}, b[2] = {st10, st11}, c[2] = {st01, st01};
+    int found = 0;
+    for (int k = 0; k < 2; ++k) {
+        double t, b1, b2;
+        if (!ray_triangle(o, d, t_min, t_max, A[k], B[k], C[k], &t, &b1, &b2))
+            continue;
+        v2 st = add2(add2(mul2((1.0 - b1) - b2, a[k]), mul2(b1, b[k])), mul2(b2, c[k]));
+        if (!uvtri_inside(&X->domain, st))
+            continue;
+        hit->t = t;
+        hit->st = st;
+        hit->bary = tri_bary(T, st.x, st.y);
+        hit->ng = normalized3(cross3(sub3(B[k], A[k]), sub3(C[k], A[k])));
+        hit->i = i;
+        hit->j = j;
+        t_max = t;
+        found = 1;
+    }
+    return found;
+}
+
+static int isect_intersect(const o_isect *X, v3 o, v3 d, double t_min, double t_max, int bound, int slab_max_level,
+                           int leaf, o_hit *hit, int64_t *st, int64_t *level_stats) /* :175-237 */
+{
+    o_tray ray = {m3mul(&X->frame.to_tangent, sub3(o, X->frame.origin)), m3mul(&X->frame.to_tangent, d), t_min,
+                  t_max};
+    int si = ray.d.x < 0.0, sj = ray.d.y < 0.0;
+    int found = 0;
+    int64_t nah = 0, lah = 0;
+    for (int r = 0; r < X->n_roots; ++r) {
+        o_cell cur = X->roots[r], end = X->roots[r];
+        cell_next(&end, si, sj, X->root_level);
+        while (!(cur.level == end.level && cur.i == end.i && cur.j == end.j)) {
+            double w = cell_width(X->pyr, cur.level);
+            v2 c = V2((cur.i + 0.5) * w, (cur.j + 0.5) * w);
+            if (classify_square(&X->domain, c, 0.5 * w) == OUTSIDE) {
+                cell_next(&cur, si, sj, X->root_level);
+                continue;
+            }
+            if (st) {
+                ++st[O_ST_NODE_TESTS];
+                ++nah;
+            }
+            if (level_stats)
+                ++level_stats[cur.level < 31 ? cur.level : 31];
+            o_nodebound nb;
+            node_bound(&nb, X->tri, &X->frame, X->pyr, cur.level, cur.i, cur.j);
+            ray.t_max = t_max;
+            double t0, t1;
+            if (!node_interval(&nb, &ray, bound, slab_max_level, &t0, &t1)) {
+                cell_next(&cur, si, sj, X->root_level);
+                continue;
+            }
+            if (cur.level > 0) {
+                cell_down(&cur, si, sj);
+                continue;
+            }
+            if (st) {
+                ++st[O_ST_LEAF_TESTS];
+                ++lah;
+            }
+            o_hit lh;
+            int lf;
+            if (leaf == O_LEAF_NEWTON)
+                lf = intersect_newton(X, o, d, t_min, t_max, cur.i, cur.j, &lh, st ? &st[O_ST_SUB_SQUARES] : NULL,
+                                      st ? &st[O_ST_NEWTON_ITERS] : NULL);
+            else
+                lf = intersect_two_triangle(X, o, d, t_min, t_max, cur.i, cur.j, &lh);
+            if (lf && lh.t < t_max) {
+                *hit = lh;
+                t_max = lh.t;
+                found = 1;
+                nah = 0;
+                lah = 0;
+            }
+            cell_next(&cur, si, sj, X->root_level);
+        }
+    }
+    if (st && found) {
+        st[O_ST_NODE_AFTER_HIT] += nah;
+        st[O_ST_LEAF_AFTER_HIT] += lah;
+    }
+    return found;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Objects and scenes.                                                       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    double *values;
+    o_grid grid;
+    o_pyramid *pyr;
+    int n_tri, first_tri;
+    o_tri *tris;
+    o_isect *isects;
+} o_object;
+
+struct o_scene {
+    int n_obj, cap;
+    o_object *obj;
+    int n_tri;
+};
+
+o_scene *o_scene_create(void) { return (o_scene *)calloc(1, sizeof(o_scene)); }
+
+void o_scene_free(o_scene *s)
+{
+    if (!s)
+        return;
+    for (int k = 0; k < s->n_obj; ++k) {
+        free(s->obj[k].values);
+        o_pyramid_free(s->obj[k].pyr);
+        free(s->obj[k].tris);
+        free(s->obj[k].isects);
+    }
+    free(s->obj);
+    free(s);
+}
+
+int o_scene_add_object(o_scene *s, const double *values, int W, double scale, double offset, int repeat, int build,
+                       const double *tris, int n_tri)
+{
+    if (s->n_obj == s->cap) {
+        s->cap = s->cap ? 2 * s->cap : 8;
+        s->obj = (o_object *)realloc(s->obj, (size_t)s->cap * sizeof(o_object));
+    }
+    o_object *O = &s->obj[s->n_obj];
+    memset(O, 0, sizeof(*O));
+    O->values = (double *)malloc((size_t)W * W * sizeof(double));
+    memcpy(O->values, values, (size_t)W * W * sizeof(double));
+    O->grid.W = W;
+    O->grid.H = W;
+    O->grid.scale = scale;
+    O->grid.values = O->values;
+    O->grid.offset = offset;
+    O->grid.repeat = repeat;
+    O->pyr = o_pyramid_build(O->values, W, scale, offset, build);
+    if (!O->pyr) {
+        free(O->values);
+        return -1;
+    }
+    O->n_tri = n_tri;
+    O->first_tri = s->n_tri;
+    O->tris = (o_tri *)calloc((size_t)n_tri, sizeof(o_tri));
+    O->isects = (o_isect *)calloc((size_t)n_tri, sizeof(o_isect));
+    for (int k = 0; k < n_tri; ++k) {
+        if (!tri_init(&O->tris[k], tris + 24 * (size_t)k)) {
+            o_pyramid_free(O->pyr);
+            free(O->values);
+            free(O->tris);
+            free(O->isects);
+            return -1;
+        }
+    }
+    for (int k = 0; k < n_tri; ++k) { /* displaced_intersector.cpp:666-679 */
+        o_isect *X = &O->isects[k];
+        isect_init(X, &O->tris[k], O->pyr, &O->grid);
+        triangle_height_range(&O->tris[k], O->pyr, &X->h_min, &X->h_max);
+        X->box = triangle_aabb(&O->tris[k], X->h_min, X->h_max);
+    }
+    s->n_tri += n_tri;
+    return s->n_obj++;
+}
+
+int o_scene_triangle_count(const o_scene *s) { return s->n_tri; }
+
+static const o_isect *find_tri(const o_scene *s, int tri, int *obj)
+{
+    for (int k = 0; k < s->n_obj; ++k) {
+        if (tri < s->obj[k].first_tri + s->obj[k].n_tri) {
+            if (obj)
+                *obj = k;
+            return &s->obj[k].isects[tri - s->obj[k].first_tri];
+        }
+    }
+    return NULL;
+}
+
+void o_scene_triangle_info(const o_scene *s, int tri, double *out)
+{
+    const o_isect *X = find_tri(s, tri, NULL);
+    out[0] = X->root_level;
+    out[1] = X->n_roots;
+    out[2] = X->residual_tolerance;
+    out[3] = X->box.lo.x;
+    out[4] = X->box.lo.y;
+    out[5] = X->box.lo.z;
+    out[6] = X->box.hi.x;
+    out[7] = X->box.hi.y;
+    out[8] = X->box.hi.z;
+    out[9] = X->h_min;
+    out[10] = X->h_max;
+}
+
+void o_scene_triangle_frame(const o_scene *s, int tri, double *out)
+{
+    const o_isect *X = find_tri(s, tri, NULL);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            out[3 * i + j] = X->frame.to_tangent.m[i][j];
+    out[9] = X->frame.ng.x;
+    out[10] = X->frame.ng.y;
+    out[11] = X->frame.ng.z;
+}
+
+static void write_hit(double *out, const o_hit *h, int tri, int obj)
+{
+    out[0] = h->t;
+    out[1] = h->st.x;
+    out[2] = h->st.y;
+    out[3] = h->bary.x;
+    out[4] = h->bary.y;
+    out[5] = h->ng.x;
+    out[6] = h->ng.y;
+    out[7] = h->ng.z;
+    out[8] = (double)h->i;
+    out[9] = (double)h->j;
+    out[10] = tri;
+    out[11] = obj;
+}
+
+static void write_miss(double *out)
+{
+    for (int k = 0; k < O_HIT_DOUBLES; ++k)
+        out[k] = 0.0;
+    out[0] = INFINITY;
+    out[10] = -1.0;
+    out[11] = -1.0;
+}
+
+/* The flat loop of ObjectIntersector::intersect_flat (:778-799) over every object. */
+static int scene_intersect1(const o_scene *s, const double *ray, int bound, int slab_max_level, int leaf,
+                            double *out, int64_t *st, int64_t *level_stats)
+{
+    v3 o = V3(ray[0], ray[1], ray[2]), d = V3(ray[3], ray[4], ray[5]);
+    double t_min = ray[6], t_max = ray[7];
+    int found = 0;
+    write_miss(out);
+    for (int ob = 0; ob < s->n_obj; ++ob) {
+        const o_object *O = &s->obj[ob];
+        for (int k = 0; k < O->n_tri; ++k) {
+            double t0 = t_min, t1 = t_max;
+            if (!box_clip(&O->isects[k].box, o, d, &t0, &t1))
+                continue;
+            if (st)
+                ++st[O_ST_TRIANGLE_TESTS];
+            o_hit h;
+            if (isect_intersect(&O->isects[k], o, d, t_min, t_max, bound, slab_max_level, leaf, &h, st,
+                                level_stats)) {
+                write_hit(out, &h, O->first_tri + k, ob);
+                t_max = h.t;
+                found = 1;
+            }
+        }
+    }
+    return found;
+}
+
+typedef struct {
+    const o_scene *s;
+    const double *rays;
+    int64_t n;
+    int bound, slab_max_level, leaf;
+    double *hits;
+    int64_t *stats;
+    atomic_llong next;
+    atomic_llong n_hit;
+    int64_t level_stats[32];
+    pthread_mutex_t mu;
+    int64_t *level_out;
+} o_job;
+
+static void *worker(void *arg)
+{
+    o_job *J = (o_job *)arg;
+    int64_t local_levels[32] = {0};
+    int64_t local_hits = 0;
+    const int64_t chunk = 4096;
+    for (;;) {
+        int64_t b = atomic_fetch_add(&J->next, chunk);
+        if (b >= J->n)
+            break;
+        int64_t e = b + chunk < J->n ? b + chunk : J->n;
+        for (int64_t r = b; r < e; ++r) {
+            int64_t *st = J->stats ? J->stats + r * O_ST_COUNT : NULL;
+            if (st)
+                memset(st, 0, O_ST_COUNT * sizeof(int64_t));
+            local_hits += scene_intersect1(J->s, J->rays + 8 * r, J->bound, J->slab_max_level, J->leaf,
+                                           J->hits + O_HIT_DOUBLES * r, st, J->level_out ? local_levels : NULL);
+        }
+    }
+    atomic_fetch_add(&J->n_hit, local_hits);
+    if (J->level_out) {
+        pthread_mutex_lock(&J->mu);
+        for (int l = 0; l < 32; ++l)
+            J->level_out[l] += local_levels[l];
+        pthread_mutex_unlock(&J->mu);
+    }
+    return NULL;
+}
+
+int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
+                          double *hits, int64_t *stats, int64_t *level_stats, int threads)
+{
+    if (threads <= 0)
+        threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (threads < 1)
+        threads = 1;
+    o_job J;
+    memset(&J, 0, sizeof(J));
+    J.s = s;
+    J.rays = rays;
+    J.n = n;
+    J.bound = bound;
+    J.slab_max_level = slab_max_level;
+    J.leaf = leaf;
+    J.hits = hits;
+    J.stats = stats;
+    J.level_out = level_stats;
+    atomic_init(&J.next, 0);
+    atomic_init(&J.n_hit, 0);
+    pthread_mutex_init(&J.mu, NULL);
+    if (threads == 1) {
+        worker(&J);
+    } else {
+        pthread_t *th = (pthread_t *)malloc((size_t)threads * sizeof(pthread_t));
+        for (int k = 0; k < threads; ++k)
+            pthread_create(&th[k], NULL, worker, &J);
+        for (int k = 0; k < threads; ++k)
+            pthread_join(th[k], NULL);
+        free(th);
+    }
+    pthread_mutex_destroy(&J.mu);
+    return (int64_t)atomic_load(&J.n_hit);
+}
+
+int o_triangle_intersect(const o_scene *s, int tri, const double *ray, int bound, int slab_max_level, int leaf,
+                         double *out, int64_t *stats)
+{
+    int ob = -1;
+    const o_isect *X = find_tri(s, tri, &ob);
+    o_hit h;
+    write_miss(out);
+    if (stats)
+        memset(stats, 0, O_ST_COUNT * sizeof(int64_t));
+    int f = isect_intersect(X, V3(ray[0], ray[1], ray[2]), V3(ray[3], ray[4], ray[5]), ray[6], ray[7], bound,
+                            slab_max_level, leaf, &h, stats, NULL);
+    if (f)
+        write_hit(out, &h, tri, ob);
+    return f;
+}
+
+void o_node_bound(const o_scene *s, int tri, int level, int64_t i, int64_t j, const double *ray, int bound,
+                  int slab_max_level, double *out)
+{
+    const o_isect *X = find_tri(s, tri, NULL);
+    o_nodebound nb;
+    node_bound(&nb, X->tri, &X->frame, X->pyr, level, i, j);
+    o_tray tr = {m3mul(&X->frame.to_tangent, sub3(V3(ray[0], ray[1], ray[2]), X->frame.origin)),
+                 m3mul(&X->frame.to_tangent, V3(ray[3], ray[4], ray[5])), ray[6], ray[7]};
+    out[0] = nb.box.lo.x;
+    out[1] = nb.box.lo.y;
+    out[2] = nb.box.lo.z;
+    out[3] = nb.box.hi.x;
+    out[4] = nb.box.hi.y;
+    out[5] = nb.box.hi.z;
+    ivl mx = af_interval(nb.m.x), my = af_interval(nb.m.y), mz = af_interval(nb.m.z);
+    out[6] = mx.lo;
+    out[7] = mx.hi;
+    out[8] = my.lo;
+    out[9] = my.hi;
+    out[10] = mz.lo;
+    out[11] = mz.hi;
+    double t0, t1;
+    out[12] = box_interval(&nb, &tr, &t0, &t1);
+    out[13] = slab_interval(&nb, &tr, &t0, &t1);
+    int pass = node_interval(&nb, &tr, bound, slab_max_level, &t0, &t1);
+    out[14] = pass ? t0 : NAN;
+    out[15] = pass ? t1 : NAN;
+}
+
+void o_displaced_position(const o_scene *s, int tri, double sp, double tp, double *out)
+{
+    const o_isect *X = find_tri(s, tri, NULL);
+    v3 S = displaced_position(X->tri, X->field, sp, tp);
+    out[0] = S.x;
+    out[1] = S.y;
+    out[2] = S.z;
+}
+
+void o_triangle_param(const o_scene *s, int tri, double u, double v, double *out)
+{
+    const o_isect *X = find_tri(s, tri, NULL);
+    v2 p = tri_param(X->tri, u, v);
+    out[0] = p.x;
+    out[1] = p.y;
+}

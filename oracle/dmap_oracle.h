@@ -1,0 +1,106 @@
+/*
+ * CPU oracle of the ray vs displaced-surface query. TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, double-precision restatement of the reference's hot path
+ * (MangoSister/dmap, code/cpp/src): the Taylor bound pyramid, the per-triangle
+ * setup, the stackless quadtree walk with its node tests, and the certified
+ * Newton leaf. Every function cites the reference file:line it follows and
+ * keeps the reference's operation order, so that results agree bit for bit
+ * with the reference compiled here (oracle/_ref) and with the FP64 GPU path.
+ *
+ * Only the tests, the smoke check and the CPU-baseline leg of bench.py use
+ * this library, and only as the checker; the product never links it.
+ *
+ * Operation order conventions shared by this file, the reference shim
+ * (oracle/ref_shim/ks/maths.h) and the FP64 device code:
+ *   dot(a, b)   = (a0*b0 + a1*b1) + a2*b2
+ *   cross(a, b) = (a1*b2 - a2*b1, a2*b0 - a0*b2, a0*b1 - a1*b0)
+ *   norm(a)     = sqrt(dot(a, a));  normalized(a) = a / norm(a) per component
+ *   M * v       = row i: (M_i0*v0 + M_i1*v1) + M_i2*v2
+ *   std::min(a, b) = b < a ? b : a;  std::max(a, b) = a < b ? b : a
+ * No fused multiply-add: build with -ffp-contract=off.
+ */
+#ifndef DMAP_ORACLE_H
+#define DMAP_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct o_pyramid o_pyramid;
+typedef struct o_scene o_scene;
+
+/* Pyramid build modes (taylor_pyramid.h:41-45). */
+enum { O_BUILD_FOLD = 0, O_BUILD_DIRECT = 1 };
+/* Traversal options (traversal_options.h:587-608). */
+enum { O_BOUND_BOX = 0, O_BOUND_SLAB = 1, O_BOUND_BOTH = 2 };
+enum { O_LEAF_NEWTON = 0, O_LEAF_TWO_TRIANGLE = 1 };
+
+/* Per-ray statistics (TraversalStats, displaced_intersector.h:89-105), plus a
+ * Newton-iteration counter that the reference does not keep. */
+enum {
+    O_ST_TRIANGLE_TESTS = 0,
+    O_ST_NODE_TESTS = 1,
+    O_ST_LEAF_TESTS = 2,
+    O_ST_SUB_SQUARES = 3,
+    O_ST_NEWTON_ITERS = 4,
+    O_ST_NODE_AFTER_HIT = 5,
+    O_ST_LEAF_AFTER_HIT = 6,
+    O_ST_COUNT = 8
+};
+
+/* Hit record, 12 doubles per ray: t, st[2], bary[2], ng[3], i, j,
+ * triangle (scene-global index, -1 on a miss), object. */
+enum { O_HIT_DOUBLES = 12 };
+
+/* TaylorPyramid(values, nodes, scale, build, offset), taylor_pyramid.cpp:324-360. */
+o_pyramid *o_pyramid_build(const double *values, int nodes, double scale, double offset, int build);
+void o_pyramid_free(o_pyramid *p);
+int o_pyramid_levels(const o_pyramid *p);
+int o_pyramid_n_leaf(const o_pyramid *p);
+/* Level l as 8 channel planes (h0, gu, gv, r, ru, rv, h_min, h_max), each m*m, [j*m + i]. */
+void o_pyramid_level(const o_pyramid *p, int level, double *out);
+/* TaylorPyramid::node (taylor_pyramid.cpp:368-383), 8 doubles. */
+void o_pyramid_node(const o_pyramid *p, int level, int64_t i, int64_t j, double *out8);
+
+/* A scene: objects in order, each an ObjectIntersector (displaced_intersector.cpp:666-679)
+ * over triangles that share one height grid and its pyramid. */
+o_scene *o_scene_create(void);
+void o_scene_free(o_scene *s);
+/* values: the (W x W) node grid; the pyramid is built from it with scale/offset.
+ * tris: n_tri x 24 doubles (p0, p1, p2, m0, m1, m2 as xyz; t0, t1, t2 as uv).
+ * Returns the object index, or -1 when a triangle is degenerate. */
+int o_scene_add_object(o_scene *s, const double *values, int W, double scale, double offset, int repeat,
+                       int build, const double *tris, int n_tri);
+int o_scene_triangle_count(const o_scene *s);
+/* Per triangle: root_level, n_roots, residual_tolerance, aabb lo[3], hi[3] (9 doubles),
+ * and height range h_min, h_max (2 doubles): 11 doubles. */
+void o_scene_triangle_info(const o_scene *s, int tri, double *out11);
+/* Per triangle: tangent frame to_tangent (9, row major), ng (3). */
+void o_scene_triangle_frame(const o_scene *s, int tri, double *out12);
+
+/* rays: n x 8 doubles (o, d, t_min, t_max). hits: n x O_HIT_DOUBLES.
+ * stats: n x O_ST_COUNT int64 (may be NULL); level_stats: 32 int64 summed (may be NULL).
+ * Flat loop over every triangle of every object, the walk of
+ * ObjectIntersector::intersect_flat (displaced_intersector.cpp:778-799).
+ * threads <= 0 uses every host core. Returns the number of hits. */
+int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
+                          double *hits, int64_t *stats, int64_t *level_stats, int threads);
+
+/* Single-triangle entry points for validation. */
+int o_triangle_intersect(const o_scene *s, int tri, const double *ray8, int bound, int slab_max_level, int leaf,
+                         double *hit, int64_t *stats);
+/* The node test record at (level, i, j): box lo/hi (6), m intervals (6), box pass,
+ * slab pass, t0/t1 of node_interval (4 doubles) = 16 doubles. */
+void o_node_bound(const o_scene *s, int tri, int level, int64_t i, int64_t j, const double *ray8, int bound,
+                  int slab_max_level, double *out16);
+/* displaced_position (displaced_surface.cpp:514-518) on triangle tri at (s, t). */
+void o_displaced_position(const o_scene *s, int tri, double sp, double tp, double *out3);
+/* BaseTriangle::param (displaced_surface.h:304). */
+void o_triangle_param(const o_scene *s, int tri, double u, double v, double *out2);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,176 @@
+"""ctypes bindings of the CPU checkers. TEST INFRASTRUCTURE ONLY.
+
+`Oracle` wraps liboracle.so (the C restatement, dmap_oracle.c); `Reference`
+wraps _ref/libdmap_ref.so (the reference's own sources built in place). Both
+expose the same methods, so a test can run one scene through either and
+compare. Only tests/, the smoke check and bench.py's CPU-baseline leg use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+HIT = 12          # doubles per hit record
+ST = 8            # int64 per-ray statistics
+ST_NAMES = ("triangle_tests", "node_tests", "leaf_tests", "sub_squares", "newton_iters",
+            "node_tests_after_hit", "leaf_tests_after_hit")
+
+BOUND = {"box": 0, "slab": 1, "both": 2}
+LEAF = {"newton": 0, "two_triangle": 1}
+
+_dp = C.POINTER(C.c_double)
+_lp = C.POINTER(C.c_int64)
+
+
+def build(ref: bool = False) -> None:
+    """Builds liboracle.so (and _ref/ when ref and the reference sources exist)."""
+    targets = ["all"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", str(HERE)] + targets, check=True)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class _Lib:
+    prefix = "o_"
+    path = HERE / "liboracle.so"
+
+    def __init__(self):
+        if not self.path.exists():
+            build(ref=self.prefix == "r_")
+        self.lib = C.CDLL(str(self.path))
+        p = self.prefix
+        L = self.lib
+
+        def f(name, res, *args):
+            fn = getattr(L, p + name)
+            fn.restype = res
+            fn.argtypes = list(args)
+            return fn
+
+        self._pyr_build = f("pyramid_build", C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_int)
+        self._pyr_free = f("pyramid_free", None, C.c_void_p)
+        self._pyr_levels = f("pyramid_levels", C.c_int, C.c_void_p)
+        self._pyr_level = f("pyramid_level", None, C.c_void_p, C.c_int, _dp)
+        self._pyr_node = f("pyramid_node", None, C.c_void_p, C.c_int, C.c_int64, C.c_int64, _dp)
+        self._sc_create = f("scene_create", C.c_void_p)
+        self._sc_free = f("scene_free", None, C.c_void_p)
+        self._sc_add = f("scene_add_object", C.c_int, C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_int,
+                         C.c_int, _dp, C.c_int)
+        self._sc_ntri = f("scene_triangle_count", C.c_int, C.c_void_p)
+        self._sc_info = f("scene_triangle_info", None, C.c_void_p, C.c_int, _dp)
+        self._sc_frame = f("scene_triangle_frame", None, C.c_void_p, C.c_int, _dp)
+        self._tri_isect = f("triangle_intersect", C.c_int, C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, C.c_int,
+                            _dp, _lp)
+        self._node_bound = f("node_bound", None, C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int64, _dp, C.c_int,
+                             C.c_int, _dp)
+        self._disp = f("displaced_position", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp)
+        if self.prefix == "o_":
+            self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
+                               _dp, _lp, _lp, C.c_int)
+            self._param = f("triangle_param", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp)
+        else:
+            self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
+                               _dp, _lp)
+
+    # -- pyramid --------------------------------------------------------
+    def pyramid(self, values, scale=1.0, offset=0.0, build="fold"):
+        """Levels of TaylorPyramid(values, scale, build, offset): a list of
+        dicts of (m, m) channel arrays."""
+        v = np.ascontiguousarray(values, np.float64)
+        p = self._pyr_build(_ptr(v), v.shape[0], scale, offset, 0 if build == "fold" else 1)
+        if not p:
+            raise ValueError("pyramid needs a (2^L + 1) x (2^L + 1) node grid")
+        try:
+            out = []
+            n = v.shape[0] - 1
+            for lvl in range(self._pyr_levels(p)):
+                m = n >> lvl
+                buf = np.empty(8 * m * m)
+                self._pyr_level(p, lvl, _ptr(buf))
+                buf = buf.reshape(8, m, m)
+                out.append({k: buf[c].copy() for c, k in enumerate(
+                    ("h0", "gu", "gv", "r", "ru", "rv", "h_min", "h_max"))})
+            return out
+        finally:
+            self._pyr_free(p)
+
+
+class Oracle(_Lib):
+    prefix = "o_"
+    path = HERE / "liboracle.so"
+
+
+class Reference(_Lib):
+    prefix = "r_"
+    path = HERE / "_ref" / "libdmap_ref.so"
+
+    @classmethod
+    def available(cls) -> bool:
+        return cls.path.exists()
+
+
+class CpuScene:
+    """A scene on one of the CPU checkers: objects in asset order, each the
+    reference's ObjectIntersector over its triangles."""
+
+    def __init__(self, lib: _Lib, scene, build="fold"):
+        self.lib = lib
+        self.h = lib._sc_create()
+        self.scene = scene
+        for asset, tris in scene.objects():
+            if len(tris) == 0:
+                continue
+            v = np.ascontiguousarray(asset.nodes, np.float64)
+            t = np.ascontiguousarray(tris, np.float64)
+            k = lib._sc_add(self.h, _ptr(v), v.shape[0], float(asset.scale), float(asset.offset),
+                            int(asset.repeat), 0 if build == "fold" else 1, _ptr(t), len(t))
+            if k < 0:
+                raise ValueError("degenerate base triangle or bad node grid")
+        self.n_tri = lib._sc_ntri(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib._sc_free(self.h)
+            self.h = None
+
+    def intersect(self, rays, bound="both", slab_max_level=1, leaf="newton", stats=False, threads=0):
+        """rays: (n, 8) o, d, t_min, t_max. Returns (hits (n, 12), stats (n, 8) or None)."""
+        r = np.ascontiguousarray(rays, np.float64)
+        n = len(r)
+        hits = np.empty((n, HIT))
+        st = np.zeros((n, ST), np.int64) if stats else None
+        if isinstance(self.lib, Oracle):
+            self.lib._sc_isect(self.h, _ptr(r), n, BOUND[bound], slab_max_level, LEAF[leaf], _ptr(hits),
+                               _ptr(st, _lp), None, threads)
+        else:
+            self.lib._sc_isect(self.h, _ptr(r), n, BOUND[bound], slab_max_level, LEAF[leaf], _ptr(hits),
+                               _ptr(st, _lp))
+        return hits, st
+
+    def triangle_info(self, tri):
+        out = np.empty(11)
+        self.lib._sc_info(self.h, tri, _ptr(out))
+        return out
+
+    def triangle_frame(self, tri):
+        out = np.empty(12)
+        self.lib._sc_frame(self.h, tri, _ptr(out))
+        return out
+
+    def node_bound(self, tri, level, i, j, ray, bound="both", slab_max_level=1):
+        out = np.empty(16)
+        r = np.ascontiguousarray(ray, np.float64)
+        self.lib._node_bound(self.h, tri, level, i, j, _ptr(r), BOUND[bound], slab_max_level, _ptr(out))
+        return out
+
+    def displaced_position(self, tri, s, t):
+        out = np.empty(3)
+        self.lib._disp(self.h, tri, s, t, _ptr(out))
+        return out

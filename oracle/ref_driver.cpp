@@ -1,0 +1,255 @@
+// C entry points over the reference's own hot-path classes, compiled from the
+// reference sources in place (oracle/Makefile) into oracle/_ref. TEST
+// INFRASTRUCTURE ONLY: the tests use it to pin the C oracle (same entry
+// points as dmap_oracle.h, prefixed r_ instead of o_).
+#include "displaced_intersector.h"
+#include "node_bounds.h"
+#include "taylor_pyramid.h"
+
+#include "../dmap_oracle.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+using dmap::BaseTriangle;
+using ks::vec2d;
+using ks::vec3d;
+
+namespace
+{
+
+struct RefObject
+{
+    std::vector<double> values;
+    dmap::HeightGrid field;
+    std::unique_ptr<dmap::TaylorPyramid> pyramid;
+    std::vector<BaseTriangle> tris;
+    std::unique_ptr<dmap::ObjectIntersector> obj;
+    int first_tri = 0;
+};
+
+} // namespace
+
+struct r_scene
+{
+    std::vector<std::unique_ptr<RefObject>> objects;
+    int n_tri = 0;
+};
+
+struct r_pyramid
+{
+    std::unique_ptr<dmap::TaylorPyramid> p;
+};
+
+extern "C" {
+
+r_pyramid *r_pyramid_build(const double *values, int nodes, double scale, double offset, int build)
+{
+    auto *r = new r_pyramid;
+    r->p = std::make_unique<dmap::TaylorPyramid>(values, nodes, scale,
+                                                 build == O_BUILD_FOLD ? dmap::PyramidBuild::Fold
+                                                                       : dmap::PyramidBuild::Direct,
+                                                 offset);
+    return r;
+}
+void r_pyramid_free(r_pyramid *p) { delete p; }
+int r_pyramid_levels(const r_pyramid *p) { return p->p->n_levels; }
+void r_pyramid_level(const r_pyramid *p, int level, double *out)
+{
+    const dmap::TaylorLevel &l = p->p->levels[level];
+    size_t cells = (size_t)l.m * l.m;
+    const std::vector<double> *ch[8] = {&l.h0, &l.gu, &l.gv, &l.r, &l.ru, &l.rv, &l.h_min, &l.h_max};
+    for (int c = 0; c < 8; ++c)
+        std::memcpy(out + c * cells, ch[c]->data(), cells * sizeof(double));
+}
+void r_pyramid_node(const r_pyramid *p, int level, int64_t i, int64_t j, double *out8)
+{
+    dmap::TaylorNode n = p->p->node(level, i, j);
+    std::memcpy(out8, &n, sizeof(n));
+}
+
+r_scene *r_scene_create(void) { return new r_scene; }
+void r_scene_free(r_scene *s) { delete s; }
+
+int r_scene_add_object(r_scene *s, const double *values, int W, double scale, double offset, int repeat, int build,
+                       const double *tris, int n_tri)
+{
+    auto o = std::make_unique<RefObject>();
+    o->values.assign(values, values + (size_t)W * W);
+    o->field = dmap::HeightGrid{W, W, scale, o->values.data(), offset, repeat != 0};
+    o->pyramid = std::make_unique<dmap::TaylorPyramid>(
+        o->field, build == O_BUILD_FOLD ? dmap::PyramidBuild::Fold : dmap::PyramidBuild::Direct);
+    for (int k = 0; k < n_tri; ++k) {
+        const double *r = tris + 24 * (size_t)k;
+        o->tris.emplace_back(vec3d(r[0], r[1], r[2]), vec3d(r[3], r[4], r[5]), vec3d(r[6], r[7], r[8]),
+                             vec3d(r[9], r[10], r[11]), vec3d(r[12], r[13], r[14]), vec3d(r[15], r[16], r[17]),
+                             vec2d(r[18], r[19]), vec2d(r[20], r[21]), vec2d(r[22], r[23]));
+    }
+    o->obj = std::make_unique<dmap::ObjectIntersector>(o->tris, *o->pyramid, o->field);
+    o->first_tri = s->n_tri;
+    s->n_tri += n_tri;
+    s->objects.push_back(std::move(o));
+    return (int)s->objects.size() - 1;
+}
+
+int r_scene_triangle_count(const r_scene *s) { return s->n_tri; }
+
+static const dmap::DisplacedIntersector *find_tri(const r_scene *s, int tri, int *ob, int *local)
+{
+    for (size_t k = 0; k < s->objects.size(); ++k) {
+        const RefObject &o = *s->objects[k];
+        if (tri < o.first_tri + (int)o.tris.size()) {
+            *ob = (int)k;
+            *local = tri - o.first_tri;
+            return &o.obj->triangles[*local];
+        }
+    }
+    return nullptr;
+}
+
+void r_scene_triangle_info(const r_scene *s, int tri, double *out)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    const dmap::Aabb3 &b = s->objects[ob]->obj->boxes[local];
+    double h_min, h_max;
+    dmap::triangle_height_range(*X->tri, *X->pyramid, h_min, h_max);
+    double v[11] = {(double)X->root_level, (double)X->n_roots, X->residual_tolerance, b.lo[0], b.lo[1], b.lo[2],
+                    b.hi[0], b.hi[1], b.hi[2], h_min, h_max};
+    std::memcpy(out, v, sizeof(v));
+}
+
+void r_scene_triangle_frame(const r_scene *s, int tri, double *out)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            out[3 * i + j] = X->frame.to_tangent(i, j);
+    out[9] = X->frame.ng[0];
+    out[10] = X->frame.ng[1];
+    out[11] = X->frame.ng[2];
+}
+
+static dmap::TraversalOptions options_of(int bound, int slab_max_level, int leaf)
+{
+    dmap::TraversalOptions o;
+    o.bound = bound == O_BOUND_BOX ? dmap::BoundMode::Box
+                                   : bound == O_BOUND_SLAB ? dmap::BoundMode::Slab : dmap::BoundMode::Both;
+    o.slab_max_level = slab_max_level;
+    o.leaf = leaf == O_LEAF_NEWTON ? dmap::LeafMode::Newton : dmap::LeafMode::TwoTriangle;
+    return o;
+}
+
+static void write_hit(double *out, const dmap::DisplacedHit &h, int tri, int ob)
+{
+    double v[O_HIT_DOUBLES] = {h.t,       h.st[0],   h.st[1],   h.bary[0],      h.bary[1],      h.ng[0],
+                               h.ng[1],   h.ng[2],   (double)h.i, (double)h.j, (double)tri, (double)ob};
+    std::memcpy(out, v, sizeof(v));
+}
+
+static void write_miss(double *out)
+{
+    for (int k = 0; k < O_HIT_DOUBLES; ++k)
+        out[k] = 0.0;
+    out[0] = INFINITY;
+    out[10] = -1.0;
+    out[11] = -1.0;
+}
+
+static void fill_stats(int64_t *out, const dmap::TraversalStats &st)
+{
+    std::memset(out, 0, O_ST_COUNT * sizeof(int64_t));
+    out[O_ST_TRIANGLE_TESTS] = st.triangle_tests;
+    out[O_ST_NODE_TESTS] = st.node_tests;
+    out[O_ST_LEAF_TESTS] = st.leaf_tests;
+    out[O_ST_SUB_SQUARES] = st.sub_squares;
+    out[O_ST_NEWTON_ITERS] = -1; // the reference keeps no such counter
+    out[O_ST_NODE_AFTER_HIT] = st.node_tests_after_hit;
+    out[O_ST_LEAF_AFTER_HIT] = st.leaf_tests_after_hit;
+}
+
+// Single thread; the object loop carries t_max the way intersect_flat does.
+int64_t r_scene_intersect(const r_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
+                          double *hits, int64_t *stats)
+{
+    dmap::TraversalOptions opt = options_of(bound, slab_max_level, leaf);
+    int64_t n_hit = 0;
+    for (int64_t r = 0; r < n; ++r) {
+        const double *q = rays + 8 * r;
+        vec3d o(q[0], q[1], q[2]), d(q[3], q[4], q[5]);
+        double t_min = q[6], t_max = q[7];
+        double *out = hits + O_HIT_DOUBLES * r;
+        write_miss(out);
+        dmap::TraversalStats st;
+        bool found = false;
+        for (size_t k = 0; k < s->objects.size(); ++k) {
+            const RefObject &ob = *s->objects[k];
+            dmap::DisplacedHit h;
+            int tri = -1;
+            if (ob.obj->intersect(o, d, t_min, t_max, opt, h, tri, stats ? &st : nullptr)) {
+                write_hit(out, h, ob.first_tri + tri, (int)k);
+                t_max = h.t;
+                found = true;
+            }
+        }
+        n_hit += found;
+        if (stats)
+            fill_stats(stats + O_ST_COUNT * r, st);
+    }
+    return n_hit;
+}
+
+int r_triangle_intersect(const r_scene *s, int tri, const double *q, int bound, int slab_max_level, int leaf,
+                         double *out, int64_t *stats)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    dmap::DisplacedHit h;
+    dmap::TraversalStats st;
+    write_miss(out);
+    bool f = X->intersect(vec3d(q[0], q[1], q[2]), vec3d(q[3], q[4], q[5]), q[6], q[7],
+                          options_of(bound, slab_max_level, leaf), h, stats ? &st : nullptr);
+    if (f)
+        write_hit(out, h, tri, ob);
+    if (stats)
+        fill_stats(stats, st);
+    return f;
+}
+
+void r_node_bound(const r_scene *s, int tri, int level, int64_t i, int64_t j, const double *q, int bound,
+                  int slab_max_level, double *out)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    dmap::NodeBound nb = dmap::node_bound(*X->tri, X->frame, *X->pyramid, level, i, j);
+    dmap::TangentRay ray{X->frame.point(vec3d(q[0], q[1], q[2])), X->frame.direction(vec3d(q[3], q[4], q[5])), q[6],
+                         q[7]};
+    for (int a = 0; a < 3; ++a) {
+        out[a] = nb.box.lo[a];
+        out[3 + a] = nb.box.hi[a];
+        dmap::Interval m = nb.m.interval(a);
+        out[6 + 2 * a] = m.lo;
+        out[7 + 2 * a] = m.hi;
+    }
+    double t0, t1;
+    out[12] = dmap::box_interval(nb, ray, t0, t1);
+    out[13] = dmap::slab_interval(nb, ray, t0, t1);
+    bool pass = dmap::node_interval(nb, ray, options_of(bound, slab_max_level, 0), t0, t1);
+    out[14] = pass ? t0 : NAN;
+    out[15] = pass ? t1 : NAN;
+}
+
+void r_displaced_position(const r_scene *s, int tri, double sp, double tp, double *out)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    vec3d S = dmap::displaced_position(*X->tri, X->field, sp, tp);
+    out[0] = S[0];
+    out[1] = S[1];
+    out[2] = S[2];
+}
+
+} // extern "C"

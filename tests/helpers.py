@@ -1,0 +1,69 @@
+"""Ray sets of the reference's traversal tests, generated through the CPU
+oracle (test infrastructure): near-surface rays
+(traversal_test_util.cpp:101-109) and rays aimed at surface points
+(validate_traversal.cpp:392-410). Rays are rounded to float32 so the GPU
+paths and the oracle see the same numbers."""
+import math
+
+import numpy as np
+
+from dmap_b200 import scenes
+
+
+def _uniform_bary(rng, n):
+    r = np.sqrt(rng.random(n))
+    return np.stack([1.0 - r, r * rng.random(n)], axis=1)
+
+
+def _edges(scene):
+    t = scene.tris
+    p0, p1, p2 = t[:, 0:3], t[:, 3:6], t[:, 6:9]
+    return (np.linalg.norm(p1 - p0, axis=1) + np.linalg.norm(p2 - p0, axis=1)
+            + np.linalg.norm(p2 - p1, axis=1)) / 3.0
+
+
+def surface_points(cpu, rng, n):
+    """Uniform points of random triangles: (tri, st, S)."""
+    sc = cpu.scene
+    n_tri = len(sc.tris)
+    tri = np.minimum((rng.random(n) * n_tri).astype(np.int64), n_tri - 1)
+    b = _uniform_bary(rng, n)
+    st = np.empty((n, 2))
+    S = np.empty((n, 3))
+    for k in range(n):
+        t = sc.tris[tri[k]]
+        t0, t1, t2 = t[18:20], t[20:22], t[22:24]
+        st[k] = t0 + b[k, 0] * (t1 - t0) + b[k, 1] * (t2 - t0)
+        S[k] = cpu.displaced_position(int(tri[k]), st[k, 0], st[k, 1])
+    return tri, st, S
+
+
+def near_surface_rays(cpu, n, seed=2027):
+    rng = np.random.default_rng(seed)
+    tri, _, S = surface_points(cpu, rng, n)
+    edges = _edges(cpu.scene)[tri]
+    r = edges * 10.0 ** (-1.0 + 1.5 * rng.random(n))
+    o = S + r[:, None] * scenes.uniform_direction(rng, n)
+    d = scenes.uniform_direction(rng, n)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 3:6], rays[:, 7] = o, d, np.inf
+    return rays
+
+
+def aimed_rays(cpu, n, seed=2028):
+    """Rays that must hit at or before t_s (the never-miss check)."""
+    rng = np.random.default_rng(seed)
+    tri, st, S = surface_points(cpu, rng, n)
+    d = scenes.uniform_direction(rng, n)
+    t_s = _edges(cpu.scene)[tri] * 10.0 ** (-1.5 + 2.0 * rng.random(n))
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 3:6], rays[:, 7] = S - t_s[:, None] * d, d, np.inf
+    # the float32 ray no longer passes exactly through S: recompute t_s along it
+    o32, d32 = rays[:, 0:3].astype(np.float64), rays[:, 3:6].astype(np.float64)
+    t_s = np.sum((S - o32) * d32, axis=1) / np.sum(d32 * d32, axis=1)
+    miss_dist = np.linalg.norm(o32 + t_s[:, None] * d32 - S, axis=1)
+    return rays, t_s, miss_dist, tri
+
+
+def small_sphere(n=32, patches=(0, 1, 5, 16, 40, 95)):
+    return scenes.cube_sphere_scene(n, 4, patches=list(patches))
