@@ -1,0 +1,262 @@
+"""dmap_b200: the ray vs displaced-surface query of MangoSister/dmap on B200.
+
+Python mirror of the reference's C++ interface for this path, over the C ABI
+of include/dmap_b200.h (libdmap_b200.so, built in place by
+``python -m dmap_b200.build``):
+
+- ``Asset``: a displacement map's HeightGrid and its TaylorPyramid, built on
+  the device (taylor_pyramid.h:89-92, displacement_asset.cpp:16-35).
+- ``Scene``: ObjectIntersector over base triangles of one or more assets
+  (displaced_intersector.h:176-198); ``intersect`` answers closest-hit
+  queries (ObjectIntersector::intersect, embree intersect_callback) and
+  occlusion queries (occluded_callback) for a batch of rays.
+- ``TraversalOptions``: the reference's bound / slab_max_level / leaf
+  (traversal_options.h:600-608) plus precision, mode and the FP64 polish
+  threshold.
+
+There is no CPU fallback: without the built library or a CUDA device every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libdmap_b200.so"
+
+F32, F16, F64 = 0, 1, 2
+BOUND = {"box": 0, "slab": 1, "both": 2}
+LEAF = {"newton": 0, "two_triangle": 1}
+PRECISION = {"f64": 0, "f32": 1}
+MODE = {"closest": 0, "occluded": 1}
+KEEP_F64 = 1
+
+HIT32 = np.dtype([("t", "<f4"), ("st", "<f4", 2), ("bary", "<f4", 2), ("ng", "<f4", 3), ("tri", "<i4"),
+                  ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
+HIT64 = np.dtype([("t", "<f8"), ("st", "<f8", 2), ("bary", "<f8", 2), ("ng", "<f8", 3), ("tri", "<i4"),
+                  ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
+STATS = ("triangle_tests", "node_tests", "leaf_tests", "sub_squares", "newton_iters", "node_tests_after_hit",
+         "leaf_tests_after_hit", "reserved")
+HIT_POLISHED, HIT_CAPPED = 1, 2
+
+
+class DmapError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"dmap status {status}: {msg}")
+        self.status = status
+
+
+class _Options(C.Structure):
+    _fields_ = [("bound", C.c_int), ("slab_max_level", C.c_int), ("leaf", C.c_int), ("precision", C.c_int),
+                ("mode", C.c_int), ("polish_cond", C.c_double)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded C library; raises when it is not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise DmapError(-1, f"{LIB_PATH} is not built (python -m dmap_b200.build)")
+        L = C.CDLL(str(LIB_PATH))
+        vp, i32, i64, dbl, u32 = C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_uint
+        sigs = {
+            "dmap_create": (i32, [i32, C.POINTER(vp)]),
+            "dmap_destroy": (None, [vp]),
+            "dmap_status_string": (C.c_char_p, [i32]),
+            "dmap_last_error": (C.c_char_p, [vp]),
+            "dmap_kernel_launches": (i64, [vp]),
+            "dmap_options_default": (None, [C.POINTER(_Options)]),
+            "dmap_asset_create": (i32, [vp, vp, i32, i32, dbl, dbl, i32, u32, C.POINTER(vp)]),
+            "dmap_asset_destroy": (None, [vp]),
+            "dmap_asset_levels": (i32, [vp]),
+            "dmap_asset_bytes": (C.c_size_t, [vp]),
+            "dmap_asset_pyramid_level": (i32, [vp, i32, i32, vp]),
+            "dmap_scene_create": (i32, [vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
+            "dmap_scene_destroy": (None, [vp]),
+            "dmap_scene_triangle_count": (i32, [vp]),
+            "dmap_scene_triangle_info": (i32, [vp, i32, vp]),
+            "dmap_intersect": (i32, [vp, vp, i32, i64, C.POINTER(_Options), vp, i32, vp, vp]),
+            "dmap_intersect_host": (i32, [vp, vp, i32, i64, C.POINTER(_Options), vp, i32, vp]),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> Sequence[str]:
+    """Every function include/dmap_b200.h declares."""
+    import re
+    text = (_PKG.parent / "include" / "dmap_b200.h").read_text()
+    return sorted(set(re.findall(r"^\w[\w\s\*]*?\b(dmap_\w+)\(", text, re.M)))
+
+
+@dataclass
+class TraversalOptions:
+    bound: str = "both"
+    slab_max_level: int = 1
+    leaf: str = "newton"
+    precision: str = "f32"
+    mode: str = "closest"
+    polish_cond: float = 1e4
+
+    def c(self) -> _Options:
+        return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],
+                        MODE[self.mode], self.polish_cond)
+
+
+class Context:
+    """One device: streams, staging and the device status word."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        s = lib().dmap_create(device, C.byref(h))
+        if s:
+            raise DmapError(s, f"dmap_create({device}): {lib().dmap_status_string(s).decode()}")
+        self.h = h
+
+    def check(self, s: int, what: str):
+        if s:
+            raise DmapError(s, f"{what}: {lib().dmap_status_string(s).decode()}: "
+                               f"{lib().dmap_last_error(self.h).decode()}")
+
+    @property
+    def kernel_launches(self) -> int:
+        return lib().dmap_kernel_launches(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dmap_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_DT = {np.dtype(np.float32): F32, np.dtype(np.float16): F16, np.dtype(np.float64): F64}
+CHANNELS = ("h0", "gu", "gv", "r", "ru", "rv", "h_min", "h_max")
+
+
+class Asset:
+    """HeightGrid + TaylorPyramid of one node grid on the device."""
+
+    def __init__(self, ctx: Context, nodes: np.ndarray, scale: float = 1.0, offset: float = 0.0,
+                 repeat: bool = False, keep_f64: bool = False):
+        v = np.ascontiguousarray(nodes)
+        if v.dtype not in _DT:
+            v = v.astype(np.float64)
+        if v.ndim != 2 or v.shape[0] != v.shape[1]:
+            raise ValueError("the node grid must be square")
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(lib().dmap_asset_create(ctx.h, v.ctypes.data, _DT[v.dtype], v.shape[0], scale, offset, int(repeat),
+                                          KEEP_F64 if keep_f64 else 0, C.byref(h)), "dmap_asset_create")
+        self.h = h
+        self.nodes = v.shape[0]
+        self.n_leaf = v.shape[0] - 1
+
+    @property
+    def n_levels(self) -> int:
+        return lib().dmap_asset_levels(self.h)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().dmap_asset_bytes(self.h)
+
+    def level(self, level: int, precision: str = "f64") -> dict:
+        m = self.n_leaf >> level
+        out = np.empty(8 * m * m)
+        self.ctx.check(lib().dmap_asset_pyramid_level(self.h, level, PRECISION[precision], out.ctypes.data),
+                       "dmap_asset_pyramid_level")
+        out = out.reshape(8, m, m)
+        return {k: out[c].copy() for c, k in enumerate(CHANNELS)}
+
+    def levels(self, precision: str = "f64"):
+        return [self.level(l, precision) for l in range(self.n_levels)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dmap_asset_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """ObjectIntersector over base triangles (n x 24 doubles: p0, p1, p2,
+    m0, m1, m2, t0, t1, t2), triangle k displaced by assets[tri_asset[k]]."""
+
+    def __init__(self, ctx: Context, assets: Sequence[Asset], tris: np.ndarray, tri_asset: np.ndarray):
+        self.ctx = ctx
+        self.assets = list(assets)
+        t = np.ascontiguousarray(tris, np.float64).reshape(-1, 24)
+        ta = np.ascontiguousarray(tri_asset, np.int32)
+        arr = (C.c_void_p * len(self.assets))(*[a.h.value for a in self.assets])
+        h = C.c_void_p()
+        ctx.check(lib().dmap_scene_create(ctx.h, arr, len(self.assets), ta.ctypes.data, t.ctypes.data, len(t),
+                                          C.byref(h)), "dmap_scene_create")
+        self.h = h
+        self.n_tri = len(t)
+
+    @classmethod
+    def from_synthetic(cls, ctx: Context, scene, keep_f64: bool = False):
+        """A dmap_b200.scenes.Scene on the device."""
+        assets = [Asset(ctx, a.nodes, a.scale, a.offset, a.repeat, keep_f64) for a in scene.assets]
+        return cls(ctx, assets, scene.tris, scene.tri_asset)
+
+    def triangle_info(self, tri: int) -> np.ndarray:
+        out = np.empty(11)
+        self.ctx.check(lib().dmap_scene_triangle_info(self.h, tri, out.ctypes.data), "dmap_scene_triangle_info")
+        return out
+
+    def intersect(self, rays: np.ndarray, options: Optional[TraversalOptions] = None, hit_dtype=np.float64,
+                  stats: bool = False):
+        """Host batch query: rays (n, 8) float32/float64 -> structured hits
+        (HIT32 or HIT64) and, when asked, (n, 8) int64 counters."""
+        opt = (options or TraversalOptions()).c()
+        r = np.ascontiguousarray(rays)
+        if r.dtype not in (np.float32, np.float64):
+            r = r.astype(np.float64)
+        n = len(r)
+        hd = HIT64 if np.dtype(hit_dtype) == np.float64 else HIT32
+        hits = np.empty(n, hd)
+        st = np.zeros((n, 8), np.int64) if stats else None
+        self.ctx.check(lib().dmap_intersect_host(self.h, r.ctypes.data, _DT[r.dtype], n, C.byref(opt),
+                                                 hits.ctypes.data, F64 if hd is HIT64 else F32,
+                                                 st.ctypes.data if stats else None), "dmap_intersect_host")
+        return (hits, st) if stats else hits
+
+    def intersect_device(self, rays_ptr: int, ray_dtype: int, n: int, hits_ptr: int, hit_dtype: int,
+                         options: Optional[TraversalOptions] = None, stats_ptr: int = 0, stream: int = 0):
+        """Device batch query on raw device pointers (asynchronous)."""
+        opt = (options or TraversalOptions()).c()
+        self.ctx.check(lib().dmap_intersect(self.h, rays_ptr, ray_dtype, n, C.byref(opt), hits_ptr, hit_dtype,
+                                            stats_ptr or None, stream or None), "dmap_intersect")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dmap_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

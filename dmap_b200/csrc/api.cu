@@ -1,0 +1,541 @@
+// The C ABI of include/dmap_b200.h: contexts, assets (node grid + device
+// pyramid), scenes (per-triangle setup) and the query entry points. Host
+// C++ over the CUDA runtime; kernels live in pyramid.cu, setup.cu,
+// walk64.cu and walk32.cu.
+#include "dmap_b200.h"
+
+#include "device_types.cuh"
+#include "launch.h"
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using dmapdev::AssetDev;
+using dmapdev::TriDev;
+using dmapdev::TriDev32;
+
+static_assert(sizeof(dmap_hit32) == sizeof(dmapdev::Hit32), "hit32 layout");
+static_assert(sizeof(dmap_hit64) == sizeof(dmapdev::Hit64), "hit64 layout");
+static_assert(DMAP_ST_COUNT == DMAP_ST_N, "stats layout");
+
+struct dmap_context
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    unsigned *status_dev = nullptr; // device status word
+    std::atomic<int64_t> launches{0};
+    std::string error;
+    // device staging for dmap_intersect_host
+    void *rays_dev = nullptr, *hits_dev = nullptr;
+    int64_t *stats_dev = nullptr;
+    size_t rays_cap = 0, hits_cap = 0, stats_cap = 0;
+};
+
+struct dmap_asset
+{
+    dmap_context *ctx = nullptr;
+    AssetDev dev{};
+    void *nodes = nullptr;
+    double *pyr64 = nullptr;
+    float *pyr32 = nullptr;
+    size_t bytes = 0;
+    int64_t cells = 0;
+};
+
+struct dmap_scene
+{
+    dmap_context *ctx = nullptr;
+    int n_tri = 0;
+    std::vector<dmap_asset *> assets;
+    AssetDev *assets_dev = nullptr;
+    TriDev *tris_dev = nullptr;
+    TriDev32 *tris32_dev = nullptr;
+    std::vector<TriDev> tris_host;
+    bool all_f64 = true;
+};
+
+namespace
+{
+
+dmap_status fail(dmap_context *ctx, dmap_status s, const std::string &msg)
+{
+    if (ctx)
+        ctx->error = msg;
+    return s;
+}
+
+dmap_status cuda_fail(dmap_context *ctx, cudaError_t e, const char *what)
+{
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation)
+        return fail(ctx, DMAP_ERR_OOM, msg);
+    return fail(ctx, DMAP_ERR_CUDA, msg);
+}
+
+#define DMAP_CUDA(ctx, call)                                                                                         \
+    do {                                                                                                              \
+        cudaError_t e_ = (call);                                                                                      \
+        if (e_ != cudaSuccess)                                                                                        \
+            return cuda_fail(ctx, e_, #call);                                                                         \
+    } while (0)
+
+size_t dtype_size(dmap_dtype t) { return t == DMAP_F64 ? 8 : t == DMAP_F16 ? 2 : 4; }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+dmap_status sync_and_check(dmap_context *ctx, const char *what)
+{
+    DMAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned st = 0;
+    DMAP_CUDA(ctx, cudaMemcpy(&st, ctx->status_dev, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st) {
+        DMAP_CUDA(ctx, cudaMemset(ctx->status_dev, 0, sizeof(unsigned)));
+        if (st & dmapdev::kStatusBadInput)
+            return fail(ctx, DMAP_ERR_DEGENERATE, std::string(what) + ": degenerate input");
+        return fail(ctx, DMAP_ERR_LIMIT, std::string(what) + ": a device iteration cap ran out");
+    }
+    return DMAP_OK;
+}
+
+template <typename T>
+dmap_status grow(dmap_context *ctx, T **p, size_t *cap, size_t bytes)
+{
+    if (*cap >= bytes)
+        return DMAP_OK;
+    if (*p)
+        cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    DMAP_CUDA(ctx, cudaMalloc((void **)p, bytes));
+    *cap = bytes;
+    return DMAP_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *dmap_status_string(dmap_status s)
+{
+    switch (s) {
+    case DMAP_OK: return "ok";
+    case DMAP_ERR_INVALID: return "invalid argument";
+    case DMAP_ERR_CUDA: return "CUDA error";
+    case DMAP_ERR_OOM: return "out of device memory";
+    case DMAP_ERR_DEGENERATE: return "degenerate base triangle";
+    case DMAP_ERR_BUDGET: return "over the memory budget";
+    case DMAP_ERR_LIMIT: return "device iteration cap reached";
+    case DMAP_ERR_NOT_READY: return "not ready";
+    case DMAP_ERR_UNSUPPORTED: return "unsupported options";
+    case DMAP_ERR_CANCELLED: return "cancelled";
+    }
+    return "unknown status";
+}
+
+dmap_status dmap_create(int device, dmap_context **out)
+{
+    if (!out)
+        return DMAP_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+        return DMAP_ERR_CUDA;
+    auto *ctx = new dmap_context;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) ||
+        cudaMalloc(&ctx->status_dev, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(ctx->status_dev, 0, sizeof(unsigned)) != cudaSuccess) {
+        delete ctx;
+        return DMAP_ERR_CUDA;
+    }
+    *out = ctx;
+    return DMAP_OK;
+}
+
+void dmap_destroy(dmap_context *ctx)
+{
+    if (!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->rays_dev);
+    cudaFree(ctx->hits_dev);
+    cudaFree(ctx->stats_dev);
+    cudaFree(ctx->status_dev);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *dmap_last_error(const dmap_context *ctx) { return ctx ? ctx->error.c_str() : ""; }
+int64_t dmap_kernel_launches(const dmap_context *ctx) { return ctx ? ctx->launches.load() : 0; }
+
+void dmap_options_default(dmap_options *opt)
+{
+    if (!opt)
+        return;
+    opt->bound = DMAP_BOUND_BOTH;
+    opt->slab_max_level = 1;
+    opt->leaf = DMAP_LEAF_NEWTON;
+    opt->precision = DMAP_PRECISION_F32;
+    opt->mode = DMAP_MODE_CLOSEST;
+    opt->polish_cond = 1e4;
+}
+
+// ---- assets ---------------------------------------------------------------
+
+dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_dtype dtype, int nodes, double scale,
+                              double offset, int repeat, unsigned flags, dmap_asset **out)
+{
+    if (!ctx || !values_host || !out)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: null argument");
+    *out = nullptr;
+    int n = nodes - 1;
+    if (nodes < 2 || (n & (n - 1)) != 0 || n > (1 << 16))
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: the node grid must be (2^L + 1)^2 with 2^L <= 65536");
+    if (dtype != DMAP_F32 && dtype != DMAP_F16 && dtype != DMAP_F64)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: dtype must be F32, F16 or F64");
+    if (!std::isfinite(scale) || !std::isfinite(offset))
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: scale and offset must be finite");
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    auto *a = new dmap_asset;
+    a->ctx = ctx;
+    size_t es = dtype_size(dtype);
+    size_t per16 = 16 / es;
+    int pitch = (int)(((size_t)nodes + per16 - 1) / per16 * per16);
+    AssetDev &d = a->dev;
+    d.dtype = dtype == DMAP_F32 ? 0 : dtype == DMAP_F16 ? 1 : 2;
+    d.W = nodes;
+    d.pitch = pitch;
+    d.n_leaf = n;
+    d.n_levels = 1;
+    while ((1 << d.n_levels) <= n)
+        ++d.n_levels;
+    d.repeat = repeat ? 1 : 0;
+    d.scale = scale;
+    d.offset = offset;
+    int64_t cells = 0;
+    for (int l = 0; l < d.n_levels; ++l) {
+        d.level_off[l] = cells;
+        int64_t m = n >> l;
+        cells += m * m;
+    }
+    a->cells = cells;
+    auto cleanup = [&](dmap_status s) {
+        cudaFree(a->nodes);
+        cudaFree(a->pyr64);
+        cudaFree(a->pyr32);
+        delete a;
+        return s;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&a->nodes, (size_t)pitch * nodes * es)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&a->pyr64, (size_t)cells * 64)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&a->pyr32, (size_t)cells * 32)) != cudaSuccess)
+        return cleanup(cuda_fail(ctx, e, "dmap_asset_create: cudaMalloc"));
+    if ((e = cudaMemcpy2DAsync(a->nodes, (size_t)pitch * es, values_host, (size_t)nodes * es, (size_t)nodes * es,
+                               nodes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+        return cleanup(cuda_fail(ctx, e, "dmap_asset_create: upload"));
+    d.nodes = a->nodes;
+    d.pyr64 = a->pyr64;
+    d.pyr32 = a->pyr32;
+
+    // TMA descriptor over the node grid: a (T+1) x box_w tile per CTA.
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc)
+        return cleanup(fail(ctx, DMAP_ERR_CUDA, "dmap_asset_create: cuTensorMapEncodeTiled unavailable"));
+    int T = n < 16 ? n : 16;
+    cuuint32_t box_w = (cuuint32_t)(((T + 1) * es + 15) / 16 * 16 / es);
+    CUtensorMap tmap;
+    cuuint64_t dims[2] = {(cuuint64_t)nodes, (cuuint64_t)nodes};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * es};
+    cuuint32_t box[2] = {box_w, (cuuint32_t)(T + 1)};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMapDataType tdt = dtype == DMAP_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                              : dtype == DMAP_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUresult cr = enc(&tmap, tdt, 2, a->nodes, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS)
+        return cleanup(fail(ctx, DMAP_ERR_CUDA, "dmap_asset_create: cuTensorMapEncodeTiled failed"));
+    if ((e = dmapk::launch_pyramid(&tmap, d, T, a->pyr64, a->pyr32, ctx->status_dev, ctx->stream)) != cudaSuccess)
+        return cleanup(cuda_fail(ctx, e, "dmap_asset_create: pyramid launch"));
+    {
+        // one leaf launch plus one fold launch per five levels above the tile
+        int level = 0, t = T, launches = 1;
+        while ((1 << level) * t < n) {
+            level += __builtin_ctz((unsigned)t);
+            int m = n >> level;
+            t = m < 16 ? m : 16;
+            ++launches;
+        }
+        ctx->launches += launches;
+    }
+    dmap_status s = sync_and_check(ctx, "dmap_asset_create");
+    if (s != DMAP_OK)
+        return cleanup(s);
+    if (!(flags & DMAP_ASSET_KEEP_F64)) {
+        cudaFree(a->pyr64);
+        a->pyr64 = nullptr;
+        d.pyr64 = nullptr;
+    }
+    a->bytes = (size_t)pitch * nodes * es + (size_t)cells * 32 + (a->pyr64 ? (size_t)cells * 64 : 0);
+    *out = a;
+    return DMAP_OK;
+}
+
+void dmap_asset_destroy(dmap_asset *a)
+{
+    if (!a)
+        return;
+    cudaSetDevice(a->ctx->device);
+    cudaStreamSynchronize(a->ctx->stream);
+    cudaFree(a->nodes);
+    cudaFree(a->pyr64);
+    cudaFree(a->pyr32);
+    delete a;
+}
+
+int dmap_asset_levels(const dmap_asset *a) { return a ? a->dev.n_levels : 0; }
+size_t dmap_asset_bytes(const dmap_asset *a) { return a ? a->bytes : 0; }
+
+dmap_status dmap_asset_pyramid_level(const dmap_asset *a, int level, int precision, double *out)
+{
+    if (!a || !out || level < 0 || level >= a->dev.n_levels)
+        return fail(a ? a->ctx : nullptr, DMAP_ERR_INVALID, "dmap_asset_pyramid_level: bad argument");
+    dmap_context *ctx = a->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    int64_t m = a->dev.n_leaf >> level, cells = m * m;
+    int64_t off = a->dev.level_off[level];
+    std::vector<double> aos((size_t)cells * 8);
+    if (precision == DMAP_PRECISION_F64) {
+        if (!a->pyr64)
+            return fail(ctx, DMAP_ERR_UNSUPPORTED, "dmap_asset_pyramid_level: the FP64 pyramid was not kept");
+        DMAP_CUDA(ctx, cudaMemcpy(aos.data(), a->pyr64 + 8 * off, (size_t)cells * 64, cudaMemcpyDeviceToHost));
+        if (a->dev.offset != 0.0)
+            for (int64_t k = 0; k < cells; ++k) {
+                aos[8 * k + 0] += a->dev.offset;
+                aos[8 * k + 6] += a->dev.offset;
+                aos[8 * k + 7] += a->dev.offset;
+            }
+    } else {
+        std::vector<float> f((size_t)cells * 8);
+        DMAP_CUDA(ctx, cudaMemcpy(f.data(), a->pyr32 + 8 * off, (size_t)cells * 32, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < f.size(); ++k)
+            aos[k] = f[k];
+    }
+    for (int c = 0; c < 8; ++c)
+        for (int64_t k = 0; k < cells; ++k)
+            out[c * cells + k] = aos[8 * k + c];
+    return DMAP_OK;
+}
+
+// ---- scenes ----------------------------------------------------------------
+
+dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset,
+                              const double *tris, int n_tri, dmap_scene **out)
+{
+    if (!ctx || !assets || n_assets <= 0 || !tri_asset || !tris || n_tri <= 0 || !out)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: bad argument");
+    *out = nullptr;
+    for (int k = 0; k < n_assets; ++k)
+        if (!assets[k] || assets[k]->ctx != ctx)
+            return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: asset of another context");
+    for (int k = 0; k < n_tri; ++k) {
+        if (tri_asset[k] < 0 || tri_asset[k] >= n_assets)
+            return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: triangle asset index out of range");
+        for (int q = 0; q < 24; ++q)
+            if (!std::isfinite(tris[24 * (size_t)k + q]))
+                return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: non-finite triangle data");
+    }
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    auto *s = new dmap_scene;
+    s->ctx = ctx;
+    s->n_tri = n_tri;
+    s->assets.assign(assets, assets + n_assets);
+    std::vector<AssetDev> ad(n_assets);
+    for (int k = 0; k < n_assets; ++k) {
+        ad[k] = assets[k]->dev;
+        s->all_f64 = s->all_f64 && assets[k]->pyr64 != nullptr;
+    }
+    double *tris_dev = nullptr;
+    int *ta_dev = nullptr;
+    auto cleanup = [&](dmap_status st) {
+        cudaFree(tris_dev);
+        cudaFree(ta_dev);
+        cudaFree(s->assets_dev);
+        cudaFree(s->tris_dev);
+        cudaFree(s->tris32_dev);
+        delete s;
+        return st;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc((void **)&s->assets_dev, sizeof(AssetDev) * n_assets)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&s->tris_dev, sizeof(TriDev) * n_tri)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&s->tris32_dev, sizeof(TriDev32) * n_tri)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&tris_dev, sizeof(double) * 24 * n_tri)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&ta_dev, sizeof(int) * n_tri)) != cudaSuccess)
+        return cleanup(cuda_fail(ctx, e, "dmap_scene_create: cudaMalloc"));
+    if ((e = cudaMemcpy(s->assets_dev, ad.data(), sizeof(AssetDev) * n_assets, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(tris_dev, tris, sizeof(double) * 24 * n_tri, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(ta_dev, tri_asset, sizeof(int) * n_tri, cudaMemcpyHostToDevice)))
+        return cleanup(cuda_fail(ctx, e, "dmap_scene_create: upload"));
+    if ((e = dmapk::launch_setup(tris_dev, ta_dev, s->assets_dev, n_tri, s->tris_dev, s->tris32_dev, ctx->status_dev,
+                                 ctx->stream)) != cudaSuccess)
+        return cleanup(cuda_fail(ctx, e, "dmap_scene_create: setup launch"));
+    ctx->launches += 1;
+    dmap_status st = sync_and_check(ctx, "dmap_scene_create");
+    if (st != DMAP_OK)
+        return cleanup(st);
+    s->tris_host.resize(n_tri);
+    if ((e = cudaMemcpy(s->tris_host.data(), s->tris_dev, sizeof(TriDev) * n_tri, cudaMemcpyDeviceToHost)))
+        return cleanup(cuda_fail(ctx, e, "dmap_scene_create: readback"));
+    cudaFree(tris_dev);
+    cudaFree(ta_dev);
+    tris_dev = nullptr;
+    ta_dev = nullptr;
+    *out = s;
+    return DMAP_OK;
+}
+
+void dmap_scene_destroy(dmap_scene *s)
+{
+    if (!s)
+        return;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    cudaFree(s->assets_dev);
+    cudaFree(s->tris_dev);
+    cudaFree(s->tris32_dev);
+    delete s;
+}
+
+int dmap_scene_triangle_count(const dmap_scene *s) { return s ? s->n_tri : 0; }
+
+dmap_status dmap_scene_triangle_info(const dmap_scene *s, int tri, double *out)
+{
+    if (!s || !out || tri < 0 || tri >= s->n_tri)
+        return DMAP_ERR_INVALID;
+    const TriDev &T = s->tris_host[tri];
+    double v[11] = {(double)T.root_level, (double)T.n_roots, T.residual_tol, T.box_lo[0], T.box_lo[1], T.box_lo[2],
+                    T.box_hi[0], T.box_hi[1], T.box_hi[2], T.h_min, T.h_max};
+    std::memcpy(out, v, sizeof(v));
+    return DMAP_OK;
+}
+
+// ---- queries ---------------------------------------------------------------
+
+static dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, const dmap_options *opt,
+                               dmap_dtype hit_dtype, dmapk::QueryOpts &q)
+{
+    dmap_options o;
+    dmap_options_default(&o);
+    if (opt)
+        o = *opt;
+    dmap_context *ctx = s->ctx;
+    if (n < 0 || (ray_dtype != DMAP_F32 && ray_dtype != DMAP_F64) || (hit_dtype != DMAP_F32 && hit_dtype != DMAP_F64))
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: rays and hits are F32 or F64");
+    if (o.bound < 0 || o.bound > 2 || o.leaf < 0 || o.leaf > 1 || o.mode < 0 || o.mode > 1 || o.precision < 0 ||
+        o.precision > 1)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad options");
+    if (o.precision == DMAP_PRECISION_F64 && !s->all_f64)
+        return fail(ctx, DMAP_ERR_UNSUPPORTED, "dmap_intersect: FP64 precision needs assets with DMAP_ASSET_KEEP_F64");
+    if (o.precision == DMAP_PRECISION_F32 && o.leaf != DMAP_LEAF_NEWTON)
+        return fail(ctx, DMAP_ERR_UNSUPPORTED, "dmap_intersect: the FP32 path has the Newton leaf only");
+    q.bound = o.bound;
+    q.slab_max_level = o.slab_max_level;
+    q.leaf = o.leaf;
+    q.mode = o.mode;
+    q.polish_cond = o.polish_cond;
+    q.ray_dtype = ray_dtype == DMAP_F64 ? 2 : 0;
+    q.hit_dtype = hit_dtype == DMAP_F64 ? 2 : 0;
+    q.precision = o.precision;
+    return DMAP_OK;
+}
+
+static dmap_status run_query(dmap_scene *s, const void *rays, int64_t n, const dmapk::QueryOpts &q, void *hits,
+                             int64_t *stats, cudaStream_t stream)
+{
+    dmap_context *ctx = s->ctx;
+    cudaError_t e;
+    if (q.precision == DMAP_PRECISION_F64)
+        e = dmapk::launch_walk64(s->tris_dev, s->n_tri, s->assets_dev, rays, n, q, hits, stats, ctx->status_dev,
+                                 stream);
+    else
+        e = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, rays, n, q, hits, stats,
+                                 ctx->status_dev, stream);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "dmap_intersect: launch");
+    if (n > 0)
+        ctx->launches += 1;
+    return DMAP_OK;
+}
+
+dmap_status dmap_intersect(dmap_scene *s, const void *rays_dev, dmap_dtype ray_dtype, int64_t n,
+                           const dmap_options *opt, void *hits_dev, dmap_dtype hit_dtype, int64_t *stats_dev,
+                           void *stream)
+{
+    if (!s || (n > 0 && (!rays_dev || !hits_dev)))
+        return fail(s ? s->ctx : nullptr, DMAP_ERR_INVALID, "dmap_intersect: null argument");
+    dmapk::QueryOpts q;
+    dmap_status st = check_query(s, ray_dtype, n, opt, hit_dtype, q);
+    if (st != DMAP_OK)
+        return st;
+    DMAP_CUDA(s->ctx, cudaSetDevice(s->ctx->device));
+    return run_query(s, rays_dev, n, q, hits_dev, stats_dev, stream ? (cudaStream_t)stream : s->ctx->stream);
+}
+
+dmap_status dmap_intersect_host(dmap_scene *s, const void *rays_host, dmap_dtype ray_dtype, int64_t n,
+                                const dmap_options *opt, void *hits_host, dmap_dtype hit_dtype, int64_t *stats_host)
+{
+    if (!s || (n > 0 && (!rays_host || !hits_host)))
+        return fail(s ? s->ctx : nullptr, DMAP_ERR_INVALID, "dmap_intersect_host: null argument");
+    dmapk::QueryOpts q;
+    dmap_status st = check_query(s, ray_dtype, n, opt, hit_dtype, q);
+    if (st != DMAP_OK || n == 0)
+        return st;
+    dmap_context *ctx = s->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    size_t rb = (size_t)n * 8 * dtype_size(ray_dtype);
+    size_t hb = (size_t)n * (hit_dtype == DMAP_F64 ? sizeof(dmap_hit64) : sizeof(dmap_hit32));
+    size_t sb = stats_host ? (size_t)n * DMAP_ST_COUNT * sizeof(int64_t) : 0;
+    if ((st = grow(ctx, &ctx->rays_dev, &ctx->rays_cap, rb)) != DMAP_OK ||
+        (st = grow(ctx, &ctx->hits_dev, &ctx->hits_cap, hb)) != DMAP_OK ||
+        (sb && (st = grow(ctx, &ctx->stats_dev, &ctx->stats_cap, sb)) != DMAP_OK))
+        return st;
+    DMAP_CUDA(ctx, cudaMemcpyAsync(ctx->rays_dev, rays_host, rb, cudaMemcpyHostToDevice, ctx->stream));
+    if ((st = run_query(s, ctx->rays_dev, n, q, ctx->hits_dev, sb ? ctx->stats_dev : nullptr, ctx->stream)) !=
+        DMAP_OK)
+        return st;
+    DMAP_CUDA(ctx, cudaMemcpyAsync(hits_host, ctx->hits_dev, hb, cudaMemcpyDeviceToHost, ctx->stream));
+    if (sb)
+        DMAP_CUDA(ctx, cudaMemcpyAsync(stats_host, ctx->stats_dev, sb, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_and_check(ctx, "dmap_intersect_host");
+}
+
+} // extern "C"

@@ -1,0 +1,42 @@
+// Host-side launchers of the device kernels (one per translation unit), called
+// by the C-ABI layer in api.cu.
+#pragma once
+#include "device_types.cuh"
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace dmapk
+{
+
+// Per-query options as the kernels read them.
+struct QueryOpts
+{
+    int bound, slab_max_level, leaf, mode;
+    double polish_cond;
+    int ray_dtype, hit_dtype; // 0 f32, 2 f64
+    int precision;            // DMAP_PRECISION_*
+};
+
+// Pyramid build (pyramid.cu). `tmap` is an encoded CUtensorMap over the node
+// grid (128 bytes), `tile` the leaf cells per CTA side. Writes the FP64
+// levels without the offset into pyr64 and the outward-rounded FP32 levels
+// with it into pyr32.
+cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int tile, double *pyr64, float *pyr32,
+                           unsigned *status, cudaStream_t stream);
+
+// Per-triangle setup (setup.cu).
+cudaError_t launch_setup(const double *tris_dev, const int *tri_asset_dev, const dmapdev::AssetDev *assets_dev,
+                         int n_tri, dmapdev::TriDev *out, dmapdev::TriDev32 *out32, unsigned *status,
+                         cudaStream_t stream);
+
+// The FP64 walk, one thread per ray over every triangle (walk64.cu).
+cudaError_t launch_walk64(const dmapdev::TriDev *tris, int n_tri, const dmapdev::AssetDev *assets, const void *rays,
+                          int64_t n, const QueryOpts &opt, void *hits, int64_t *stats, unsigned *status,
+                          cudaStream_t stream);
+
+// The FP32 walk (walk32.cu).
+cudaError_t launch_walk32(const dmapdev::TriDev32 *tris32, const dmapdev::TriDev *tris64, int n_tri,
+                          const dmapdev::AssetDev *assets, const void *rays, int64_t n, const QueryOpts &opt,
+                          void *hits, int64_t *stats, unsigned *status, cudaStream_t stream);
+
+} // namespace dmapk

@@ -1,0 +1,305 @@
+// K1: the Taylor bound pyramid on the device (taylor_pyramid.cpp:154-247,
+// leaf_level and fold, the reference's default Fold build).
+//
+// One CTA per tile of T x T leaf cells (T = min(16, 2^L)), one thread per
+// cell in Morton order, so that the four children of every parent are four
+// consecutive threads. The (T+1)^2 node tile is staged in shared memory by
+// one TMA 2-D tiled load (cp.async.bulk.tensor, no multicast); each thread
+// builds its leaf node in double, then the CTA folds 4 -> 1 with warp
+// shuffles (max/min/hull reductions over the four children) until its tile
+// is one cell, writing every level as it goes. Upper levels above the tile
+// are folded by further launches of the fold kernel over the stored FP64
+// level. Compiled with -fmad=false: every double operation is the
+// reference's, so the FP64 levels equal the reference bit for bit.
+//
+// Outputs per cell: 8 doubles (no offset; added on read) and 8 floats
+// (offset added, rounded outward: h0, gu, gv to nearest with r, ru, rv
+// widened by the rounding error, h_min down, h_max up).
+#include "device_types.cuh"
+#include "launch.h"
+#include <cuda.h>
+#include <cuda_fp16.h>
+
+namespace
+{
+using dmapdev::AssetDev;
+
+constexpr int kMaxTile = 16;  // 256 threads per CTA: the FP64 fold keeps its registers
+constexpr int kTilePitch = 24; // staged row pitch bound in elements (>= 17, TMA box inner extent rounded to 16 B)
+
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
+
+// Morton decode of a tile-local cell index: even bits -> x (u, i), odd -> y (v, j).
+__device__ __forceinline__ unsigned compact1by1(unsigned x)
+{
+    x &= 0x55555555u;
+    x = (x ^ (x >> 1)) & 0x33333333u;
+    x = (x ^ (x >> 2)) & 0x0f0f0f0fu;
+    x = (x ^ (x >> 4)) & 0x00ff00ffu;
+    x = (x ^ (x >> 8)) & 0x0000ffffu;
+    return x;
+}
+
+struct Node8 { double h0, gu, gv, r, ru, rv, mn, mx; };
+
+__device__ __forceinline__ double shfl(double v, int lane_mask)
+{
+    return __shfl_xor_sync(0xffffffffu, v, lane_mask);
+}
+
+// Fold four children held by lanes {L, L^1, L^2, L^3} of one warp into
+// their parent (taylor_pyramid.cpp:186-247). `b` is the lane's child u bit,
+// `a` its v bit; s is the parent half-extent. Every lane returns the parent.
+__device__ __forceinline__ Node8 fold4(const Node8 &c, int a, int b, double s)
+{
+    double gu_hi = c.gu + c.ru, gu_lo = c.gu - c.ru, gv_hi = c.gv + c.rv, gv_lo = c.gv - c.rv;
+    double mn = c.mn, mx = c.mx;
+#pragma unroll
+    for (int m = 1; m <= 2; m <<= 1) {
+        gu_hi = dmax(gu_hi, shfl(gu_hi, m));
+        gu_lo = dmin(gu_lo, shfl(gu_lo, m));
+        gv_hi = dmax(gv_hi, shfl(gv_hi, m));
+        gv_lo = dmin(gv_lo, shfl(gv_lo, m));
+        mn = dmin(mn, shfl(mn, m));
+        mx = dmax(mx, shfl(mx, m));
+    }
+    Node8 p;
+    double gu_p = 0.5 * (gu_hi + gu_lo);
+    double gv_p = 0.5 * (gv_hi + gv_lo);
+    p.gu = gu_p;
+    p.ru = 0.5 * (gu_hi - gu_lo);
+    p.gv = gv_p;
+    p.rv = 0.5 * (gv_hi - gv_lo);
+    p.mn = mn;
+    p.mx = mx;
+    const double off0 = -0.5 * s, off1 = 0.5 * s;
+    double dx = b ? off1 : off0, dy = a ? off1 : off0;
+    double du_g = c.gu - gu_p;
+    double dv_g = c.gv - gv_p;
+    double base = (c.h0 - c.gu * dx) - c.gv * dy;
+    double upper = -INFINITY, lower = INFINITY;
+#pragma unroll
+    for (int cu = 0; cu < 2; ++cu) {
+#pragma unroll
+        for (int cv = 0; cv < 2; ++cv) {
+            double corner = (base + du_g * (dx + (cu ? off1 : off0))) + dv_g * (dy + (cv ? off1 : off0));
+            upper = dmax(upper, corner + c.r);
+            lower = dmin(lower, corner - c.r);
+        }
+    }
+#pragma unroll
+    for (int m = 1; m <= 2; m <<= 1) {
+        upper = dmax(upper, shfl(upper, m));
+        lower = dmin(lower, shfl(lower, m));
+    }
+    p.h0 = 0.5 * (upper + lower);
+    p.r = 0.5 * (upper - lower);
+    return p;
+}
+
+__device__ __forceinline__ void store_node(const Node8 &n, double offset, size_t k, double *pyr64, float *pyr32)
+{
+    double2 *p = reinterpret_cast<double2 *>(pyr64 + 8 * k);
+    p[0] = make_double2(n.h0, n.gu);
+    p[1] = make_double2(n.gv, n.r);
+    p[2] = make_double2(n.ru, n.rv);
+    p[3] = make_double2(n.mn, n.mx);
+    double h0 = n.h0, mn = n.mn, mx = n.mx;
+    if (offset != 0.0) {
+        h0 += offset;
+        mn += offset;
+        mx += offset;
+    }
+    float h0f = __double2float_rn(h0), guf = __double2float_rn(n.gu), gvf = __double2float_rn(n.gv);
+    float rf = __double2float_ru(__dadd_ru(n.r, fabs(h0 - (double)h0f)));
+    float ruf = __double2float_ru(__dadd_ru(n.ru, fabs(n.gu - (double)guf)));
+    float rvf = __double2float_ru(__dadd_ru(n.rv, fabs(n.gv - (double)gvf)));
+    float4 *q = reinterpret_cast<float4 *>(pyr32 + 8 * k);
+    q[0] = make_float4(h0f, guf, gvf, rf);
+    q[1] = make_float4(ruf, rvf, __double2float_rd(mn), __double2float_ru(mx));
+}
+
+// Folds the CTA's cells (count = T*T held one per thread, Morton order) up
+// to one cell, storing each level. `level0` is the level of the held cells,
+// (tx, ty) the tile's position in units of T cells at level0.
+__device__ void fold_tile(Node8 v, int T, int level0, int tx, int ty, const AssetDev &a, double *pyr64,
+                          float *pyr32, Node8 *smem)
+{
+    int t = threadIdx.x;
+    int count = T * T;
+    int level = level0;
+    int side = T;
+    while (count > 1) {
+        int lvl = level + 1;
+        int m = a.n_leaf >> lvl;       // cells per side at the parent level
+        double s = 0.5 / m;            // parent half-extent
+        Node8 p;
+        if (t < ((count + 31) & ~31)) { // whole warps only, inactive lanes hold copies
+            p = fold4(v, (t >> 1) & 1, t & 1, s);
+        }
+        if (t < count && (t & 3) == 0) {
+            int pc = t >> 2;
+            smem[pc] = p;
+            int x = (int)compact1by1((unsigned)pc), y = (int)compact1by1((unsigned)pc >> 1);
+            int ps = side >> 1;
+            size_t k = (size_t)a.level_off[lvl] + (size_t)(ty * ps + y) * m + (tx * ps + x);
+            store_node(p, a.offset, k, pyr64, pyr32);
+        }
+        __syncthreads();
+        count >>= 2;
+        side >>= 1;
+        level = lvl;
+        if (t < count)
+            v = smem[t];
+        else if (count > 0)
+            v = smem[0];
+        __syncthreads();
+    }
+}
+
+template <typename In>
+__device__ __forceinline__ double to_d(In x);
+template <>
+__device__ __forceinline__ double to_d<float>(float x) { return (double)x; }
+template <>
+__device__ __forceinline__ double to_d<__half>(__half x) { return (double)__half2float(x); }
+template <>
+__device__ __forceinline__ double to_d<double>(double x) { return x; }
+
+__device__ __forceinline__ bool mbar_wait(unsigned bar_addr, unsigned phase)
+{
+    // Bounded wait on the TMA transaction barrier.
+    for (int it = 0; it < (1 << 24); ++it) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(bar_addr), "r"(phase)
+                     : "memory");
+        if (done)
+            return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+// Leaf level + in-tile folds. Block: T*T threads. Grid: (n_leaf/T)^2 tiles.
+template <typename In>
+__global__ void __launch_bounds__(256) pyramid_leaf_kernel(const __grid_constant__ CUtensorMap tmap, AssetDev a,
+                                                            int T, double *pyr64, float *pyr32, unsigned *status)
+{
+    __shared__ alignas(128) In tile[(kMaxTile + 1) * kTilePitch];
+    __shared__ alignas(8) unsigned long long bar;
+    __shared__ Node8 smem[kMaxTile * kMaxTile / 4];
+    int tiles_x = a.n_leaf / T;
+    int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
+    unsigned bar_addr = (unsigned)__cvta_generic_to_shared(&bar);
+    unsigned tile_addr = (unsigned)__cvta_generic_to_shared(tile);
+    const int box_w = ((T + 1) * (int)sizeof(In) + 15) / 16 * 16 / (int)sizeof(In);
+    const unsigned bytes = (unsigned)(box_w * (T + 1) * sizeof(In));
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_addr) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int x0 = tx * T, y0 = ty * T; // x0 * sizeof(In) is a multiple of 16 for T = 16 and 0 otherwise
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_addr), "r"(bytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                     " [%0], [%1, {%2, %3}], [%4];" ::"r"(tile_addr),
+                     "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(x0), "r"(y0), "r"(bar_addr)
+                     : "memory");
+    }
+    bool ok = mbar_wait(bar_addr, 0);
+    if (!ok) {
+        if (threadIdx.x == 0)
+            atomicOr(status, dmapdev::kStatusCapped);
+        return;
+    }
+    int t = threadIdx.x;
+    bool active = t < T * T; // a 1-, 2- or 4-cell tile still runs one full warp
+    int x = active ? (int)compact1by1((unsigned)t) : 0, y = active ? (int)compact1by1((unsigned)t >> 1) : 0;
+    // leaf_level (taylor_pyramid.cpp:154-176) on V = values * scale
+    double v00 = to_d(tile[y * box_w + x]) * a.scale, v10 = to_d(tile[y * box_w + x + 1]) * a.scale;
+    double v01 = to_d(tile[(y + 1) * box_w + x]) * a.scale, v11 = to_d(tile[(y + 1) * box_w + x + 1]) * a.scale;
+    double w = 1.0 / a.n_leaf;
+    double s = 0.5 * w;
+    Node8 n;
+    n.h0 = 0.25 * (((v00 + v10) + v01) + v11);
+    n.gu = 0.5 * ((v10 - v00) + (v11 - v01)) / w;
+    n.gv = 0.5 * ((v01 - v00) + (v11 - v10)) / w;
+    double c3 = (((v00 - v10) - v01) + v11) / (w * w);
+    n.r = fabs(c3) * s * s;
+    n.ru = fabs(c3) * s;
+    n.rv = fabs(c3) * s;
+    n.mn = dmin(dmin(v00, v10), dmin(v01, v11));
+    n.mx = dmax(dmax(v00, v10), dmax(v01, v11));
+    size_t k = (size_t)(ty * T + y) * a.n_leaf + (tx * T + x);
+    if (active)
+        store_node(n, a.offset, k, pyr64, pyr32);
+    fold_tile(n, T, 0, tx, ty, a, pyr64, pyr32, smem);
+}
+
+// Folds level `level0` (m0 x m0 cells, FP64 without offset) upward.
+// Block: T*T threads, grid: (m0/T)^2.
+__global__ void __launch_bounds__(256) pyramid_fold_kernel(AssetDev a, int level0, int T, double *pyr64,
+                                                            float *pyr32)
+{
+    __shared__ Node8 smem[kMaxTile * kMaxTile / 4];
+    int m0 = a.n_leaf >> level0;
+    int tiles_x = m0 / T;
+    int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
+    int t = threadIdx.x;
+    bool active = t < T * T;
+    int x = active ? (int)compact1by1((unsigned)t) : 0, y = active ? (int)compact1by1((unsigned)t >> 1) : 0;
+    size_t k = (size_t)a.level_off[level0] + (size_t)(ty * T + y) * m0 + (tx * T + x);
+    const double2 *p = reinterpret_cast<const double2 *>(pyr64 + 8 * k);
+    double2 q0 = p[0], q1 = p[1], q2 = p[2], q3 = p[3];
+    Node8 n = {q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y};
+    fold_tile(n, T, level0, tx, ty, a, pyr64, pyr32, smem);
+}
+
+template <typename In>
+cudaError_t launch_leaf(const void *tmap, const AssetDev &a, int T, double *pyr64, float *pyr32, unsigned *status,
+                        cudaStream_t stream)
+{
+    int tiles = (a.n_leaf / T) * (a.n_leaf / T);
+    int threads = T * T < 32 ? 32 : T * T;
+    pyramid_leaf_kernel<In><<<tiles, threads, 0, stream>>>(*reinterpret_cast<const CUtensorMap *>(tmap), a, T,
+                                                           pyr64, pyr32, status);
+    return cudaGetLastError();
+}
+
+} // namespace
+
+namespace dmapk
+{
+cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int tile, double *pyr64, float *pyr32,
+                           unsigned *status, cudaStream_t stream)
+{
+    cudaError_t e;
+    if (a.dtype == 0)
+        e = launch_leaf<float>(tmap, a, tile, pyr64, pyr32, status, stream);
+    else if (a.dtype == 1)
+        e = launch_leaf<__half>(tmap, a, tile, pyr64, pyr32, status, stream);
+    else
+        e = launch_leaf<double>(tmap, a, tile, pyr64, pyr32, status, stream);
+    if (e != cudaSuccess)
+        return e;
+    // levels above the first tile fold
+    int level = 0, T = tile;
+    while ((1 << level) * T < a.n_leaf) {
+        level += __builtin_ctz((unsigned)T); // the tile fold produced levels up to level + log2(T)
+        int m = a.n_leaf >> level;
+        T = m < kMaxTile ? m : kMaxTile;
+        int threads = T * T < 32 ? 32 : T * T;
+        pyramid_fold_kernel<<<(m / T) * (m / T), threads, 0, stream>>>(a, level, T, pyr64, pyr32);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+} // namespace dmapk

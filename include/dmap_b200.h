@@ -1,0 +1,185 @@
+/*
+ * dmap_b200: the ray vs displaced-surface query of MangoSister/dmap on NVIDIA
+ * B200 (sm_100a). Plain C ABI: opaque handles, plain pointers and sizes,
+ * integer status codes (never abort), no CUDA or C++ types in signatures
+ * (streams are passed as `void *` holding a cudaStream_t).
+ *
+ * Each entry point names the reference interface it replaces
+ * (code/cpp/src in the reference, file:line).
+ *
+ * Threading: one context per device. Calls on one context are serialized by
+ * the caller; different contexts may be used from different threads.
+ * Buffers passed as "device" must be device memory of the context's GPU;
+ * "host" buffers may be pageable or pinned.
+ */
+#ifndef DMAP_B200_H
+#define DMAP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum dmap_status {
+    DMAP_OK = 0,
+    DMAP_ERR_INVALID = 1,     /* bad argument (the reference ASSERTs instead) */
+    DMAP_ERR_CUDA = 2,        /* a CUDA call failed; dmap_last_error() has the text */
+    DMAP_ERR_OOM = 3,         /* device allocation failed */
+    DMAP_ERR_DEGENERATE = 4,  /* a base triangle is degenerate in texture space (displaced_surface.cpp:419) */
+    DMAP_ERR_BUDGET = 5,      /* the request does not fit the server's memory budget */
+    DMAP_ERR_LIMIT = 6,       /* an iteration cap ran out on the device; results are flagged */
+    DMAP_ERR_NOT_READY = 7,   /* a served request has not finished */
+    DMAP_ERR_UNSUPPORTED = 8, /* combination of options the build does not offer */
+    DMAP_ERR_CANCELLED = 9    /* a served request was cancelled */
+} dmap_status;
+
+typedef enum dmap_dtype { DMAP_F32 = 0, DMAP_F16 = 1, DMAP_F64 = 2 } dmap_dtype;
+
+typedef struct dmap_context dmap_context;
+typedef struct dmap_asset dmap_asset;
+typedef struct dmap_scene dmap_scene;
+typedef struct dmap_server dmap_server;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Binds a device and creates the library's streams and pinned staging. */
+dmap_status dmap_create(int device, dmap_context **out);
+void dmap_destroy(dmap_context *ctx);
+const char *dmap_status_string(dmap_status s);
+/* Text of the last error on this context (empty when none). */
+const char *dmap_last_error(const dmap_context *ctx);
+/* Number of the library's kernels launched on this context so far. */
+int64_t dmap_kernel_launches(const dmap_context *ctx);
+
+/* ---- displacement assets: HeightGrid + TaylorPyramid ------------------- */
+
+/* Asset flags. */
+#define DMAP_ASSET_KEEP_F64 1u /* keep the FP64 pyramid resident (needed by DMAP_PRECISION_F64) */
+
+/*
+ * Uploads a (nodes x nodes) node grid, nodes = 2^L + 1, row major with
+ * values[j * nodes + i] at (u, v) = (i, j) / (nodes - 1), and builds its
+ * Taylor bound pyramid on the device: h = scale * value + offset, texture
+ * coordinates wrapping when `repeat`, clamping otherwise.
+ * Replaces DisplacementAsset's grid + TaylorPyramid(const HeightGrid &, PyramidBuild::Fold)
+ * (displacement_asset.cpp:16-35, taylor_pyramid.h:89-92, taylor_pyramid.cpp:324-366).
+ * `values_host` is host memory of `dtype` (F32, F16 or F64).
+ */
+dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_dtype dtype, int nodes, double scale,
+                              double offset, int repeat, unsigned flags, dmap_asset **out);
+void dmap_asset_destroy(dmap_asset *asset);
+int dmap_asset_levels(const dmap_asset *asset);
+/* Device bytes the asset holds. */
+size_t dmap_asset_bytes(const dmap_asset *asset);
+/*
+ * Copies pyramid level `level` to the host as 8 channel planes (h0, gu, gv, r,
+ * ru, rv, h_min, h_max), each m*m doubles with m = 2^L >> level, [j*m + i]
+ * (the TaylorLevel layout, taylor_pyramid.h:52-61). precision selects the
+ * FP64 pyramid (DMAP_PRECISION_F64, needs KEEP_F64) or the outward-rounded
+ * FP32 one widened to double (DMAP_PRECISION_F32).
+ */
+dmap_status dmap_asset_pyramid_level(const dmap_asset *asset, int level, int precision, double *out_host);
+
+/* ---- scenes: ObjectIntersector over base triangles --------------------- */
+
+/*
+ * Per-triangle setup on the device: the base triangle and its chart, the
+ * tangent frame, the footprint roots, the height range and the object-space
+ * AABB. tris_host: n_tri x 24 doubles (p0, p1, p2, m0, m1, m2 as xyz; t0,
+ * t1, t2 as texture uv), tri_asset[k] indexes `assets`.
+ * Replaces ObjectIntersector(const std::vector<BaseTriangle> &, const TaylorPyramid &,
+ * const HeightGrid &) (displaced_intersector.h:183-184, displaced_intersector.cpp:666-679)
+ * with the BaseTriangle general-chart constructor (displaced_surface.h:296-298).
+ * A scene borrows its assets: destroy the scene first.
+ */
+dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset_host,
+                              const double *tris_host, int n_tri, dmap_scene **out);
+void dmap_scene_destroy(dmap_scene *scene);
+int dmap_scene_triangle_count(const dmap_scene *scene);
+/*
+ * Per-triangle setup results (11 doubles: root_level, n_roots,
+ * residual_tolerance, aabb lo xyz, aabb hi xyz, h_min, h_max), the fields
+ * DisplacedIntersector's constructor and triangle_aabb produce
+ * (displaced_intersector.cpp:335-351, node_bounds.cpp:347-378).
+ */
+dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *out11);
+
+/* ---- queries ------------------------------------------------------------ */
+
+/* TraversalOptions (traversal_options.h:600-608) plus the device choices. */
+#define DMAP_BOUND_BOX 0
+#define DMAP_BOUND_SLAB 1
+#define DMAP_BOUND_BOTH 2
+#define DMAP_LEAF_NEWTON 0
+#define DMAP_LEAF_TWO_TRIANGLE 1
+#define DMAP_PRECISION_F64 0 /* the reference's double arithmetic, operation for operation */
+#define DMAP_PRECISION_F32 1 /* FP32 walk and leaf, bounds widened outward, FP64 Newton polish */
+#define DMAP_MODE_CLOSEST 0  /* closest hit in (t_min, t_max): rtcIntersect1 / intersect_callback */
+#define DMAP_MODE_OCCLUDED 1 /* any hit in (t_min, t_max): rtcOccluded1 / occluded_callback */
+
+typedef struct dmap_options {
+    int bound;          /* DMAP_BOUND_*, default BOTH */
+    int slab_max_level; /* default 1 */
+    int leaf;           /* DMAP_LEAF_*, default NEWTON */
+    int precision;      /* DMAP_PRECISION_*, default F32 */
+    int mode;           /* DMAP_MODE_*, default CLOSEST */
+    double polish_cond; /* FP32 path: FP64 Newton polish when cond(J) exceeds this (default 1e4; 0 = always) */
+} dmap_options;
+
+/* Fills the defaults above. */
+void dmap_options_default(dmap_options *opt);
+
+/*
+ * Rays: n records of 8 values of `ray_dtype` (F32 or F64): o.xyz, d.xyz,
+ * t_min, t_max. Hits: n records of `hit_dtype` (F32: struct dmap_hit32, F64:
+ * struct dmap_hit64). Misses have tri = -1 and t = +inf. In OCCLUDED mode
+ * only `tri` (>= 0 when occluded) and `t` of some occluder are meaningful.
+ */
+typedef struct dmap_hit32 {
+    float t, st[2], bary[2], ng[3];
+    int32_t tri, i, j, flags;
+} dmap_hit32;
+typedef struct dmap_hit64 {
+    double t, st[2], bary[2], ng[3];
+    int32_t tri, i, j, flags;
+} dmap_hit64;
+/* dmap_hit*.flags bits */
+#define DMAP_HIT_POLISHED 1 /* FP32 path: the hit went through the FP64 Newton polish */
+#define DMAP_HIT_CAPPED 2   /* a device iteration cap ran out for this ray */
+
+/* Per-ray counters (TraversalStats, displaced_intersector.h:89-105), 8 int64 per ray. */
+#define DMAP_ST_TRIANGLE_TESTS 0
+#define DMAP_ST_NODE_TESTS 1
+#define DMAP_ST_LEAF_TESTS 2
+#define DMAP_ST_SUB_SQUARES 3
+#define DMAP_ST_NEWTON_ITERS 4
+#define DMAP_ST_NODE_AFTER_HIT 5
+#define DMAP_ST_LEAF_AFTER_HIT 6
+#define DMAP_ST_COUNT 8
+
+/*
+ * Batched query on device buffers, asynchronous on `stream` (a
+ * cudaStream_t, NULL = the context's stream). `stats_dev` may be NULL.
+ * Replaces, per ray, ObjectIntersector::intersect (displaced_intersector.h:193-194)
+ * and the embree callbacks intersect_callback / occluded_callback
+ * (displaced_geometry.cpp:49-106) for a scene of displaced objects.
+ */
+dmap_status dmap_intersect(dmap_scene *scene, const void *rays_dev, dmap_dtype ray_dtype, int64_t n,
+                           const dmap_options *opt, void *hits_dev, dmap_dtype hit_dtype, int64_t *stats_dev,
+                           void *stream);
+
+/*
+ * The same query on host buffers: copies the rays in, runs, copies the hits
+ * back, and returns when they are on the host (synchronous). This is the
+ * drop-in call a CPU-side scene makes per batch, and the single-ray
+ * ObjectIntersector::intersect when n = 1.
+ */
+dmap_status dmap_intersect_host(dmap_scene *scene, const void *rays_host, dmap_dtype ray_dtype, int64_t n,
+                                const dmap_options *opt, void *hits_host, dmap_dtype hit_dtype, int64_t *stats_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
