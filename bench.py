@@ -1,0 +1,370 @@
+"""Benchmark of the ray vs displaced-surface query (Mrays/s).
+
+Default workload (N=1): the GPU-scale plain-method scene, a radius-1 cube
+sphere of 96 displaced patches (6 faces x 4 x 4, two base triangles each),
+each patch its own 2048 x 2048 FP32 height map (seeded sines + value noise,
+amplitude 0.08); one step intersects 1920 x 1080 jittered primary rays and
+one cosine-weighted bounce ray per primary hit (closest hit, t/u/v/normal).
+Inputs are seeded synthetic data of the reference benchmark's shape.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dmap|reference]
+                  [--config sphere|quad] [--precision f32|f64]
+
+--impl reference times the reference's own CPU implementation of the query
+(oracle/_ref: the reference sources compiled here; else the C oracle port)
+on every host core over a bounded sample of the same workload.
+Under torchrun (N > 1) each rank intersects its own share of the rays with
+a replicated scene (no collective on the data path); value = all rays / max
+rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from dmap_b200 import scenes  # noqa: E402
+
+METRIC = "Mrays/s displaced-surface hits"
+FLOP = {"node": 450, "leaf": 290, "sub": 285, "newton": 215}   # per-unit FLOPs of the reference algorithm
+BYTES = {"ray": 32, "hit": 48, "node": 32, "leaf": 16}          # per-unit algorithmic bytes (FP32 records)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def build_scene(config: str, small: bool):
+    if config == "quad":
+        return scenes.quad_scene(128 if small else 512), scenes.quad_camera_rays(*(64, 64) if small else (256, 256))
+    n = 256 if small else 2048
+    k = 4
+    # parallel map generation: 96 independent seeded maps
+    def one(pid):
+        return scenes.sine_noise_heights(n, scenes.SEED + pid, 0.08, octaves=4)
+    with cf.ThreadPoolExecutor(min(16, os.cpu_count() or 4)) as ex:
+        maps = list(ex.map(one, range(6 * k * k)))
+    sc = scenes.cube_sphere_scene(1, k)   # geometry only, tiny maps replaced below
+    for pid, a in enumerate(sc.assets):
+        a.nodes = scenes.close_tile(maps[pid], repeat=False).astype(np.float32)
+    w, h = (480, 270) if small else (1920, 1080)
+    return sc, scenes.sphere_camera_rays(w, h)
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def work_per_ray(stats):
+    s = stats.astype(np.float64).sum(axis=0)
+    n = len(stats)
+    flops = (FLOP["node"] * s[1] + FLOP["leaf"] * s[2] + FLOP["sub"] * s[3] + FLOP["newton"] * s[4]) / n
+    byts = BYTES["ray"] + BYTES["hit"] + (BYTES["node"] * s[1] + BYTES["leaf"] * s[2]) / n
+    return flops, byts, {k: float(s[i] / n) for i, k in enumerate(["triangle_tests", "node_tests", "leaf_tests",
+                                                                      "sub_squares", "newton_iters"])}
+
+
+def cpu_sample(sc, rays, hits_t, budget_s: float, use_ref: bool):
+    """Times the CPU reference on a bounded sample: a block of primary rays
+    around the image centre and their bounce rays, over only the patches
+    whose boxes those rays reach (the flat loop's result is unchanged by
+    dropping triangles a ray's box test rejects)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import py_oracle
+    lib = py_oracle.Reference() if use_ref and py_oracle.Reference.available() else py_oracle.Oracle()
+    kind = "reference" if isinstance(lib, py_oracle.Reference) else "port"
+    W, H = (1920, 1080) if len(rays) == 1920 * 1080 else (480, 270) if len(rays) == 480 * 270 else (None, None)
+    if W:
+        jj, ii = np.mgrid[H // 2 - 32:H // 2 + 32, W // 2 - 32:W // 2 + 32]
+        idx = (jj * W + ii).ravel()
+    else:
+        idx = np.arange(min(len(rays), 4096))
+    sample = rays[idx]
+    ok = np.isfinite(hits_t[idx])
+    # object set: patches whose triangle boxes any sample ray meets
+    tris = sc.tris
+    keep_assets = sorted(set(sc.tri_asset.tolist())) if len(sc.assets) <= 4 else None
+    sub = sc
+    if keep_assets is None:
+        from dmap_b200 import Scene  # noqa
+        lo = np.minimum(np.minimum(tris[:, 0:3], tris[:, 3:6]), tris[:, 6:9]) - 0.2
+        hi = np.maximum(np.maximum(tris[:, 0:3], tris[:, 3:6]), tris[:, 6:9]) + 0.2
+        o, d = sample[:, 0:3].astype(np.float64), sample[:, 3:6].astype(np.float64)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv = 1.0 / d
+            t0 = (lo[None] - o[:, None]) * inv[:, None]
+            t1 = (hi[None] - o[:, None]) * inv[:, None]
+        tn = np.nanmax(np.minimum(t0, t1), axis=2)
+        tf = np.nanmin(np.maximum(t0, t1), axis=2)
+        touched = np.any((tn <= tf) & (tf >= 0), axis=0)
+        keep_assets = sorted(set(sc.tri_asset[touched].tolist()))
+        sub = scenes.Scene([sc.assets[a] for a in keep_assets],
+                           np.concatenate([sc.tris[sc.tri_asset == a] for a in keep_assets]),
+                           np.concatenate([np.full((sc.tri_asset == a).sum(), k, np.int32)
+                                           for k, a in enumerate(keep_assets)]))
+    cpu = py_oracle.CpuScene(lib, sub)
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    h, _ = cpu.intersect(sample, threads=threads)
+    dt = time.perf_counter() - t
+    # the bounce rays of the sample's hits
+    hit = np.isfinite(h[:, 0])
+    b = scenes.bounce_rays(sample[hit], h[hit, 0], h[hit, 5:8])
+    allr = np.concatenate([sample, b])
+    reps = max(1, int(budget_s / max(dt * len(allr) / len(sample), 1e-3)))
+    reps = min(reps, 64)
+    return cpu, allr, kind, threads, len(keep_assets), reps
+
+
+def run_cpu(args, rank, world):
+    sc, rays = build_scene(args.config, args.small)
+    # primary hits for the bounce rays: the CPU sample takes its own from the oracle
+    cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, rays, np.zeros(len(rays)), 10.0, True)
+    times = []
+    for s in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        cpu.intersect(allr, threads=threads)
+        dt = time.perf_counter() - t
+        if s >= args.warmup:
+            times.append(dt)
+    ms = 1e3 * float(np.mean(times))
+    v = len(allr) / (ms * 1e-3) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(args), "sample_rays": len(allr), "sample_objects": n_obj},
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": kind,
+                             "sample": f"{len(allr)} rays (64x64 primary block at the image centre + bounces) "
+                                       f"over the {n_obj} patches they reach"},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(args):
+    if args.config == "quad":
+        return "quad 512^2 FP32, 256x256 camera rays" if not args.small else "quad 128^2 (small)"
+    return ("cube sphere 96 patches x 2048^2 FP32, 1920x1080 jittered primary + 1 diffuse bounce per hit"
+            if not args.small else "cube sphere 96 patches x 256^2 (small)")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
+    ap.add_argument("--config", default="sphere", choices=["sphere", "quad"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_cpu(args, rank, world)
+        return
+
+    import torch
+    import dmap_b200 as dm
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    t_setup = time.perf_counter()
+    sc, prim = build_scene(args.config, args.small)
+    ctx = dm.Context(local)
+    keep64 = args.precision == "f64" or True   # the FP64 path counts the reference algorithm's work
+    dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=keep64)
+    opt = dm.TraversalOptions(precision=args.precision)
+    ref_opt = dm.TraversalOptions(precision="f64")
+    # bounce rays from the FP64 (reference-arithmetic) hits, frozen
+    h0 = dev.intersect(prim, ref_opt, np.float64)
+    hit = h0["tri"] >= 0
+    bounce = scenes.bounce_rays(prim[hit], h0["t"][hit], h0["ng"][hit])
+    rays_all = np.concatenate([prim, bounce]).astype(np.float32)
+    # this rank's share
+    n_all = len(rays_all)
+    lo, hi = rank * n_all // world, (rank + 1) * n_all // world
+    my = np.ascontiguousarray(rays_all[lo:hi])
+    n = len(my)
+    # algorithmic work of the reference algorithm on these rays (FP64 path counters)
+    _, st = dev.intersect(my, ref_opt, np.float64, stats=True)
+    flops_ray, bytes_ray, counts = work_per_ray(st)
+    setup_s = time.perf_counter() - t_setup
+
+    rays_d = torch.from_numpy(my).cuda()
+    hits_d = torch.empty((n, 12), dtype=torch.int32, device="cuda")   # 48 B hit32 records
+    # one explicit stream for the kernels, the L2 flush and the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        dev.intersect_device(rays_d.data_ptr(), dm.F32, n, hits_d.data_ptr(), dm.F32, opt,
+                             stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for e0, e1 in evs:
+            flush.fill_(1.0)          # L2 flush between steps, outside the events
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    launches = ctx.kernel_launches - launches0
+    ms = float(np.sum([a.elapsed_time(b) for a, b in evs])) / args.steps
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = n_all / (ms_max * 1e-3) / 1e6
+
+    # end to end through the public host API: pinned host rays in, hits out, per step
+    rays_h = torch.from_numpy(my).pin_memory()
+    hits_h = torch.empty((n, 12), dtype=torch.int32).pin_memory()
+    optc = opt.c()
+    import ctypes
+    L = dm.lib()
+
+    def e2e_step():
+        ctx.check(L.dmap_intersect_host(dev.h, rays_h.data_ptr(), dm.F32, n, ctypes.byref(optc),
+                                        hits_h.data_ptr(), dm.F32, None), "dmap_intersect_host")
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = n_all / e2e_s / 1e6
+
+    hbm, peak_src = peaks()
+    launch_ms = ms / max(1, launches // args.steps)
+    achieved_gbs = bytes_ray * n / (launch_ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+            "config": {"workload": workload_name(args), "rays_per_step": n_all, "precision": args.precision,
+                       "l2": "flushed between steps (256 MB write); pyramids 17 GB exceed L2",
+                       "parallelism": f"replicated scene, rays split over {world} rank(s)"},
+            "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": int(my.nbytes),
+                    "d2h_bytes_per_step": int(n * 48)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm, "traffic": None, "peak_source": peak_src,
+                         "kernel": "walk", "bytes_per_ray": bytes_ray},
+            "roofline_fp32": {"achieved": flops_ray * n / (launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                              "flops_per_ray": flops_ray, "nominal_peak": 74.4,
+                              "note": "FP32 CUDA-core issue is the path's bound; no measured FP32 peak on file"},
+            "work_per_ray": counts, "setup_s": setup_s}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, rays_all, np.where(hit, 1.0, np.inf), 10.0, True)
+            t = time.perf_counter()
+            for _ in range(reps):
+                cpu.intersect(allr, threads=threads)
+            dt = (time.perf_counter() - t) / reps
+            line["cpu_baseline"] = {"value": len(allr) / dt / 1e6, "unit": "Mrays/s", "cores": threads,
+                                    "kind": kind, "sample": f"{len(allr)} rays (64x64 primary block at the image "
+                                                            f"centre + bounces) over the {n_obj} patches they reach"}
+        except Exception as e:  # the baseline is reported, not required
+            line["cpu_baseline"] = {"error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

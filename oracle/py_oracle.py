@@ -77,7 +77,7 @@ class _Lib:
             self._param = f("triangle_param", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp)
         else:
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
-                               _dp, _lp)
+                               _dp, _lp, C.c_int)
 
     # -- pyramid --------------------------------------------------------
     def pyramid(self, values, scale=1.0, offset=0.0, build="fold"):
@@ -151,7 +151,7 @@ class CpuScene:
                                _ptr(st, _lp), None, threads)
         else:
             self.lib._sc_isect(self.h, _ptr(r), n, BOUND[bound], slab_max_level, LEAF[leaf], _ptr(hits),
-                               _ptr(st, _lp))
+                               _ptr(st, _lp), threads)
         return hits, st
 
     def triangle_info(self, tri):

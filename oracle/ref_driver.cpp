@@ -10,7 +10,10 @@
 
 #include <cmath>
 #include <cstring>
+#include <algorithm>
+#include <atomic>
 #include <memory>
+#include <thread>
 #include <vector>
 
 using dmap::BaseTriangle;
@@ -171,13 +174,41 @@ static void fill_stats(int64_t *out, const dmap::TraversalStats &st)
     out[O_ST_LEAF_AFTER_HIT] = st.leaf_tests_after_hit;
 }
 
-// Single thread; the object loop carries t_max the way intersect_flat does.
+// The object loop carries t_max the way intersect_flat does. The reference's
+// intersect is const and re-entrant, so rays are split over `threads`
+// std::threads in chunks of 4096 (threads <= 0: every core).
+static int64_t intersect_range(const r_scene *s, const double *rays, int64_t b, int64_t e,
+                               const dmap::TraversalOptions &opt, double *hits, int64_t *stats);
+
 int64_t r_scene_intersect(const r_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
-                          double *hits, int64_t *stats)
+                          double *hits, int64_t *stats, int threads)
 {
     dmap::TraversalOptions opt = options_of(bound, slab_max_level, leaf);
+    if (threads <= 0)
+        threads = (int)std::thread::hardware_concurrency();
+    if (threads <= 1)
+        return intersect_range(s, rays, 0, n, opt, hits, stats);
+    std::atomic<int64_t> next{0}, n_hit{0};
+    std::vector<std::thread> pool;
+    for (int k = 0; k < threads; ++k)
+        pool.emplace_back([&] {
+            for (;;) {
+                int64_t b = next.fetch_add(4096);
+                if (b >= n)
+                    break;
+                n_hit += intersect_range(s, rays, b, std::min<int64_t>(n, b + 4096), opt, hits, stats);
+            }
+        });
+    for (auto &t : pool)
+        t.join();
+    return n_hit.load();
+}
+
+static int64_t intersect_range(const r_scene *s, const double *rays, int64_t b, int64_t e,
+                               const dmap::TraversalOptions &opt, double *hits, int64_t *stats)
+{
     int64_t n_hit = 0;
-    for (int64_t r = 0; r < n; ++r) {
+    for (int64_t r = b; r < e; ++r) {
         const double *q = rays + 8 * r;
         vec3d o(q[0], q[1], q[2]), d(q[3], q[4], q[5]);
         double t_min = q[6], t_max = q[7];

@@ -1,0 +1,81 @@
+"""The FP32 path against the oracle: the walk's node tests are FP32 and
+widened outward, the leaves are the reference's FP64 leaf, so the hit set
+must equal the oracle's and every reported root must be the oracle's root
+(|dt| <= 4 residual tolerances; in practice identical), with never fewer node
+tests admitted than the FP64 walk (conservative bounds)."""
+import numpy as np
+import pytest
+
+import dmap_b200 as dm
+import py_oracle
+import helpers
+from dmap_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return dm.Context(0)
+
+
+def _check(cpu, dev, rays, bound="both", k=1):
+    ho, so = cpu.intersect(rays, bound, k, stats=True)
+    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, precision="f32"), np.float64, stats=True)
+    assert np.array_equal(hd["tri"] >= 0, ho[:, 10] >= 0), "hit/miss set differs"
+    hit = ho[:, 10] >= 0
+    tol = np.array([cpu.triangle_info(t)[2] for t in range(cpu.n_tri)])
+    dt = np.abs(hd["t"][hit] - ho[hit, 0])
+    assert (dt <= 4 * tol[ho[hit, 10].astype(int)] + 1e-12).all()
+    # leaves visited by the FP64 walk are visited by the FP32 walk too
+    assert (sd[:, 2] >= so[:, 2]).all()
+    return hit.sum(), float((sd[:, 1].sum() / max(so[:, 1].sum(), 1)))
+
+
+@pytest.mark.parametrize("bound,k", [("both", 1), ("box", 1), ("slab", 6)])
+def test_f32_quad(ctx, oracle, bound, k):
+    sc = scenes.quad_scene(64)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = np.concatenate([scenes.quad_camera_rays(64, 64), helpers.near_surface_rays(cpu, 2000),
+                           helpers.aimed_rays(cpu, 2000)[0]])
+    n, ratio = _check(cpu, dev, rays, bound, k)
+    assert n > 1000 and ratio < 1.5
+
+
+def test_f32_sphere(ctx, oracle):
+    sc = helpers.small_sphere(32)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 2000),
+                           helpers.aimed_rays(cpu, 2000)[0]])
+    n, ratio = _check(cpu, dev, rays)
+    assert n > 1000 and ratio < 1.5
+
+
+def test_f32_f16_texels_and_offset(ctx, oracle):
+    """FP16 texels (the precision variant): the oracle sees them widened to double."""
+    sc = helpers.small_sphere(64, patches=(0, 1, 2, 17))
+    for a in sc.assets:
+        a.nodes = a.nodes.astype(np.float16)
+        a.scale, a.offset = 0.9, 0.01
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = np.concatenate([helpers.near_surface_rays(cpu, 2000), helpers.aimed_rays(cpu, 2000)[0]])
+    _check(cpu, dev, rays)
+
+
+def test_f32_never_miss(ctx, oracle):
+    sc = helpers.small_sphere(32)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays, t_s, miss_dist, _ = helpers.aimed_rays(cpu, 4000, seed=91)
+    h = dev.intersect(rays, dm.TraversalOptions(precision="f32"))
+    ok = miss_dist < 1e-6
+    assert (h["tri"][ok] >= 0).all()
+
+
+def test_f32_occluded(ctx, oracle):
+    sc = helpers.small_sphere(32)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = helpers.near_surface_rays(cpu, 3000)
+    rays[:, 7] = np.where(np.arange(len(rays)) % 2 == 0, 1.0, np.inf)
+    ho, _ = cpu.intersect(rays)
+    h = dev.intersect(rays, dm.TraversalOptions(precision="f32", mode="occluded"))
+    assert np.array_equal(h["tri"] >= 0, ho[:, 10] >= 0)
