@@ -221,6 +221,9 @@ def main():
     ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
     ap.add_argument("--config", default="sphere", choices=["sphere", "quad"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--schedule", default="persistent", choices=["persistent", "simple"])
+    ap.add_argument("--leaf-batch", type=int, default=16)
+    ap.add_argument("--blocks-per-sm", type=int, default=4)
     ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     args = ap.parse_args()
@@ -247,7 +250,8 @@ def main():
     ctx = dm.Context(local)
     keep64 = args.precision == "f64" or True   # the FP64 path counts the reference algorithm's work
     dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=keep64)
-    opt = dm.TraversalOptions(precision=args.precision)
+    opt = dm.TraversalOptions(precision=args.precision, schedule=args.schedule, leaf_batch=args.leaf_batch,
+                              blocks_per_sm=args.blocks_per_sm)
     ref_opt = dm.TraversalOptions(precision="f64")
     # bounce rays from the FP64 (reference-arithmetic) hits, frozen
     h0 = dev.intersect(prim, ref_opt, np.float64)

@@ -34,6 +34,7 @@ BOUND = {"box": 0, "slab": 1, "both": 2}
 LEAF = {"newton": 0, "two_triangle": 1}
 PRECISION = {"f64": 0, "f32": 1}
 MODE = {"closest": 0, "occluded": 1}
+SCHEDULE = {"persistent": 0, "simple": 1}
 KEEP_F64 = 1
 
 HIT32 = np.dtype([("t", "<f4"), ("st", "<f4", 2), ("bary", "<f4", 2), ("ng", "<f4", 3), ("tri", "<i4"),
@@ -53,7 +54,8 @@ class DmapError(RuntimeError):
 
 class _Options(C.Structure):
     _fields_ = [("bound", C.c_int), ("slab_max_level", C.c_int), ("leaf", C.c_int), ("precision", C.c_int),
-                ("mode", C.c_int), ("polish_cond", C.c_double)]
+                ("mode", C.c_int), ("polish_cond", C.c_double), ("schedule", C.c_int), ("leaf_batch", C.c_int),
+                ("blocks_per_sm", C.c_int)]
 
 
 _lib = None
@@ -109,10 +111,14 @@ class TraversalOptions:
     precision: str = "f32"
     mode: str = "closest"
     polish_cond: float = 1e4
+    schedule: str = "persistent"
+    leaf_batch: int = 16
+    blocks_per_sm: int = 4
 
     def c(self) -> _Options:
         return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],
-                        MODE[self.mode], self.polish_cond)
+                        MODE[self.mode], self.polish_cond, SCHEDULE[self.schedule], self.leaf_batch,
+                        self.blocks_per_sm)
 
 
 class Context:

@@ -32,6 +32,7 @@ struct dmap_context
     int device = 0;
     cudaStream_t stream = nullptr;
     unsigned *status_dev = nullptr; // device status word
+    unsigned long long *counter_dev = nullptr; // ray counter of the persistent walk (scratch)
     std::atomic<int64_t> launches{0};
     std::string error;
     // device staging for dmap_intersect_host
@@ -169,6 +170,7 @@ dmap_status dmap_create(int device, dmap_context **out)
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) ||
         cudaMalloc(&ctx->status_dev, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&ctx->counter_dev, sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemset(ctx->status_dev, 0, sizeof(unsigned)) != cudaSuccess) {
         delete ctx;
         return DMAP_ERR_CUDA;
@@ -187,6 +189,7 @@ void dmap_destroy(dmap_context *ctx)
     cudaFree(ctx->hits_dev);
     cudaFree(ctx->stats_dev);
     cudaFree(ctx->status_dev);
+    cudaFree(ctx->counter_dev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -204,6 +207,9 @@ void dmap_options_default(dmap_options *opt)
     opt->precision = DMAP_PRECISION_F32;
     opt->mode = DMAP_MODE_CLOSEST;
     opt->polish_cond = 1e4;
+    opt->schedule = DMAP_SCHEDULE_PERSISTENT;
+    opt->leaf_batch = 16;
+    opt->blocks_per_sm = 4;
 }
 
 // ---- assets ---------------------------------------------------------------
@@ -475,6 +481,12 @@ static dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.ray_dtype = ray_dtype == DMAP_F64 ? 2 : 0;
     q.hit_dtype = hit_dtype == DMAP_F64 ? 2 : 0;
     q.precision = o.precision;
+    if (o.schedule < 0 || o.schedule > 1 || o.leaf_batch < 0 || o.leaf_batch > 32 || o.blocks_per_sm < 0 ||
+        o.blocks_per_sm > 16)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad schedule options");
+    q.schedule = o.schedule;
+    q.leaf_batch = o.leaf_batch;
+    q.blocks_per_sm = o.blocks_per_sm;
     return DMAP_OK;
 }
 
@@ -488,7 +500,7 @@ static dmap_status run_query(dmap_scene *s, const void *rays, int64_t n, const d
                                  stream);
     else
         e = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, rays, n, q, hits, stats,
-                                 ctx->status_dev, stream);
+                                 ctx->status_dev, ctx->counter_dev, stream);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "dmap_intersect: launch");
     if (n > 0)

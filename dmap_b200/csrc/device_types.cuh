@@ -70,6 +70,12 @@ struct TriDev32
     int roots_i[4], roots_j[4];
     double A[3][3];        // to_tangent in double for the ray transform
     double q0[3];
+    // The interpolated normal in tangent space, A N(s,t) = a0 + s au + t av,
+    // and |N(s,t)|^2 = qc + 2 s q1 + 2 t q2 + s^2 q11 + 2 s t q12 + t^2 q22,
+    // rounded from double; rowsum[i] = sum_j |A_ij| bounds |A n| for a unit n.
+    float a0[3], au[3], av[3];
+    float qc, q1, q2, q11, q12, q22;
+    float rowsum[3];
 };
 
 // Device status word bits (written with atomicOr).

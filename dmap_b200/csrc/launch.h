@@ -15,6 +15,9 @@ struct QueryOpts
     double polish_cond;
     int ray_dtype, hit_dtype; // 0 f32, 2 f64
     int precision;            // DMAP_PRECISION_*
+    int schedule;             // DMAP_SCHEDULE_*
+    int leaf_batch;           // persistent walk: run the deferred leaves once this many lanes of 32 wait
+    int blocks_per_sm;        // persistent walk: resident CTAs per SM (0 = occupancy maximum)
 };
 
 // Pyramid build (pyramid.cu). `tmap` is an encoded CUtensorMap over the node
@@ -34,9 +37,12 @@ cudaError_t launch_walk64(const dmapdev::TriDev *tris, int n_tri, const dmapdev:
                           int64_t n, const QueryOpts &opt, void *hits, int64_t *stats, unsigned *status,
                           cudaStream_t stream);
 
-// The FP32 walk (walk32.cu).
+// The FP32 walk (walk32.cu). `counter` is the persistent schedule's ray
+// counter (device scratch, one unsigned long long); the launcher zeroes it on
+// `stream` before the kernel.
 cudaError_t launch_walk32(const dmapdev::TriDev32 *tris32, const dmapdev::TriDev *tris64, int n_tri,
                           const dmapdev::AssetDev *assets, const void *rays, int64_t n, const QueryOpts &opt,
-                          void *hits, int64_t *stats, unsigned *status, cudaStream_t stream);
+                          void *hits, int64_t *stats, unsigned *status, unsigned long long *counter,
+                          cudaStream_t stream);
 
 } // namespace dmapk

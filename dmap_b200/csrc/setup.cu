@@ -236,6 +236,20 @@ __device__ void derive32(const TriDev &T, TriDev32 &S)
         S.roots_i[k] = T.roots_i[k];
         S.roots_j[k] = T.roots_j[k];
     }
+    v3 m0 = L3(T.m0), Mu = L3(T.Mu), Mv = L3(T.Mv);
+    v3 a0 = mat3mul(T.A, m0), au = mat3mul(T.A, Mu), av = mat3mul(T.A, Mv);
+    for (int a = 0; a < 3; ++a) {
+        S.a0[a] = (float)comp(a0, a);
+        S.au[a] = (float)comp(au, a);
+        S.av[a] = (float)comp(av, a);
+        S.rowsum[a] = fup((fabs(T.A[a][0]) + fabs(T.A[a][1])) + fabs(T.A[a][2]));
+    }
+    S.qc = (float)dot3(m0, m0);
+    S.q1 = (float)dot3(m0, Mu);
+    S.q2 = (float)dot3(m0, Mv);
+    S.q11 = (float)dot3(Mu, Mu);
+    S.q12 = (float)dot3(Mu, Mv);
+    S.q22 = (float)dot3(Mv, Mv);
 }
 
 __global__ void setup_kernel(const double *__restrict__ tris, const int *__restrict__ tri_asset,
