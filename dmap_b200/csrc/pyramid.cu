@@ -15,8 +15,11 @@
 // Outputs per cell: 8 doubles (no offset; added on read) and 8 floats
 // (offset added, rounded outward: h0, gu, gv to nearest with r, ru, rv
 // widened by the rounding error, h_min down, h_max up).
+#include "dmap_b200.h"
 #include "device_types.cuh"
 #include "launch.h"
+#include <cmath>
+#include <cstdint>
 #include <cuda.h>
 #include <cuda_fp16.h>
 
@@ -303,3 +306,133 @@ cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int til
     return cudaSuccess;
 }
 } // namespace dmapk
+
+// ---------------------------------------------------------------------------
+// dmap_pyramid_build_noalloc: the pyramid build for callers that cannot
+// allocate device memory.
+//
+// The regular build (dmap_asset_create) allocates its FP64 working levels,
+// and its node grid and output, with cudaMalloc. Callers that own every byte
+// of device memory through their own pool, or that must not allocate while
+// a frame is in flight, cannot let the library do that. For them this entry
+// point takes the node grid and the FP32 output pyramid as device buffers
+// they already hold, and keeps the FP64 working levels in the fixed array
+// below instead of allocating. The array is file-scope device memory: every
+// GPU that loads the library holds it (22.4 MB) until the process exits, and
+// it bounds the map size this entry point accepts to 512 x 512 texels.
+// Every call reuses the same array, so calls whose kernels overlap on the
+// GPU (two streams, or two host threads) race on it: serialize them.
+// ---------------------------------------------------------------------------
+
+namespace
+{
+constexpr int kNoallocMaxLeaf = 512;                    // texels per side
+constexpr size_t kNoallocCells = (size_t)349525;        // cells of a 512^2 pyramid: (4^10 - 1) / 3
+constexpr size_t kNoallocHead = 32;                     // doubles ahead of the levels: the status word
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocHead + 8 * kNoallocCells];
+
+typedef CUresult (*NoallocEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                    CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                    CUtensorMapFloatOOBfill);
+
+// The device address of the scratch array on the current device, looked up
+// once per device with that device current (the host-side symbol is only a
+// stand-in and must never reach a kernel).
+double *noalloc_scratch(int device, cudaError_t &err)
+{
+    static double *addr[64] = {};
+    err = cudaSuccess;
+    if (device < 0 || device >= 64)
+        return nullptr;
+    if (!addr[device]) {
+        double *p = nullptr;
+        err = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        if (err != cudaSuccess)
+            return nullptr;
+        addr[device] = p;
+    }
+    return addr[device];
+}
+} // namespace
+
+extern "C" dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dtype dtype, int nodes, int pitch,
+                                                  double scale, double offset, int repeat, float *pyr32_dev,
+                                                  void *stream)
+{
+    int n = nodes - 1;
+    if (!nodes_dev || !pyr32_dev)
+        return DMAP_ERR_INVALID;
+    if (nodes < 2 || (n & (n - 1)) != 0)
+        return DMAP_ERR_INVALID;
+    if (n > kNoallocMaxLeaf)
+        return DMAP_ERR_INVALID; // beyond the fixed scratch: use dmap_asset_create
+    if (dtype != DMAP_F32 && dtype != DMAP_F16 && dtype != DMAP_F64)
+        return DMAP_ERR_INVALID;
+    size_t es = dtype == DMAP_F64 ? 8 : dtype == DMAP_F16 ? 2 : 4;
+    if (pitch < nodes || ((size_t)pitch * es) % 16 != 0 || ((uintptr_t)nodes_dev & 15) != 0 ||
+        ((uintptr_t)pyr32_dev & 15) != 0 || !std::isfinite(scale) || !std::isfinite(offset))
+        return DMAP_ERR_INVALID;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess)
+        return DMAP_ERR_CUDA;
+    cudaError_t err;
+    double *scratch = noalloc_scratch(device, err);
+    if (!scratch)
+        return DMAP_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+
+    AssetDev a{};
+    a.nodes = nodes_dev;
+    a.dtype = dtype == DMAP_F32 ? 0 : dtype == DMAP_F16 ? 1 : 2;
+    a.W = nodes;
+    a.pitch = pitch;
+    a.n_leaf = n;
+    a.n_levels = 1;
+    while ((1 << a.n_levels) <= n)
+        ++a.n_levels;
+    a.repeat = repeat ? 1 : 0;
+    a.scale = scale;
+    a.offset = offset;
+    int64_t cells = 0;
+    for (int l = 0; l < a.n_levels; ++l) {
+        a.level_off[l] = cells;
+        int64_t m = n >> l;
+        cells += m * m;
+    }
+    double *levels = scratch + kNoallocHead;
+    unsigned *status = reinterpret_cast<unsigned *>(scratch);
+    a.pyr64 = levels;
+    a.pyr32 = pyr32_dev;
+
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+        return DMAP_ERR_CUDA;
+    int T = n < kMaxTile ? n : kMaxTile;
+    cuuint32_t box_w = (cuuint32_t)(((T + 1) * es + 15) / 16 * 16 / es);
+    CUtensorMap tmap;
+    cuuint64_t dims[2] = {(cuuint64_t)nodes, (cuuint64_t)nodes};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * es};
+    cuuint32_t box[2] = {box_w, (cuuint32_t)(T + 1)};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMapDataType tdt = dtype == DMAP_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                              : dtype == DMAP_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if (reinterpret_cast<NoallocEncodeFn>(fn)(&tmap, tdt, 2, const_cast<void *>(nodes_dev), dims, strides, box, estr,
+                                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return DMAP_ERR_CUDA;
+    // the status word must start at zero; the levels are overwritten whole
+    if (cudaMemsetAsync(status, 0, sizeof(unsigned), s) != cudaSuccess)
+        return DMAP_ERR_CUDA;
+    if (dmapk::launch_pyramid(&tmap, a, T, levels, pyr32_dev, status, s) != cudaSuccess)
+        return DMAP_ERR_CUDA;
+    unsigned st = 0;
+    if (cudaMemcpyAsync(&st, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return DMAP_ERR_CUDA;
+    return st ? DMAP_ERR_LIMIT : DMAP_OK;
+}

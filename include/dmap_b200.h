@@ -82,6 +82,29 @@ size_t dmap_asset_bytes(const dmap_asset *asset);
  */
 dmap_status dmap_asset_pyramid_level(const dmap_asset *asset, int level, int precision, double *out_host);
 
+/*
+ * The pyramid build without any device allocation. No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc (a host
+ * application that owns all device memory through its own pool, or that must
+ * not allocate while frames are in flight), which dmap_asset_create cannot
+ * serve because it allocates the node grid, the FP64 working levels and the
+ * output.
+ * The caller passes the node grid already on the device (`nodes` x `nodes`
+ * values of `dtype`, rows `pitch` elements apart, pitch * element size a
+ * multiple of 16 bytes, 16-byte aligned) and a device buffer for the FP32
+ * pyramid: sum over levels l = 0..L of (2^L >> l)^2 cells of 8 floats, laid
+ * out as the asset's FP32 pyramid (dmap_asset_pyramid_level, DMAP_PRECISION_F32).
+ * The FP64 working levels live in a fixed device array of the library (22.4
+ * MB per GPU that loads it, held until exit), so maps are limited to
+ * 2^L <= 512 texels per side; larger ones return DMAP_ERR_INVALID. The first
+ * call on each device looks up that array's device address; make it before
+ * any stream capture. Runs on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream) and returns when the pyramid is written. Calls share the
+ * array: calls that overlap on the GPU race, so serialize them.
+ */
+dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dtype dtype, int nodes, int pitch, double scale,
+                                       double offset, int repeat, float *pyr32_dev, void *stream);
+
 /* ---- scenes: ObjectIntersector over base triangles --------------------- */
 
 /*
