@@ -221,8 +221,8 @@ def main():
     ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
     ap.add_argument("--config", default="sphere", choices=["sphere", "quad"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
-    ap.add_argument("--schedule", default="persistent", choices=["persistent", "simple"])
-    ap.add_argument("--leaf-batch", type=int, default=16)
+    ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
+    ap.add_argument("--rounds", type=int, default=6)
     ap.add_argument("--blocks-per-sm", type=int, default=4)
     ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
@@ -250,7 +250,7 @@ def main():
     ctx = dm.Context(local)
     keep64 = args.precision == "f64" or True   # the FP64 path counts the reference algorithm's work
     dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=keep64)
-    opt = dm.TraversalOptions(precision=args.precision, schedule=args.schedule, leaf_batch=args.leaf_batch,
+    opt = dm.TraversalOptions(precision=args.precision, schedule=args.schedule, rounds=args.rounds,
                               blocks_per_sm=args.blocks_per_sm)
     ref_opt = dm.TraversalOptions(precision="f64")
     # bounce rays from the FP64 (reference-arithmetic) hits, frozen
@@ -266,6 +266,9 @@ def main():
     # algorithmic work of the reference algorithm on these rays (FP64 path counters)
     _, st = dev.intersect(my, ref_opt, np.float64, stats=True)
     flops_ray, bytes_ray, counts = work_per_ray(st)
+    # the measured path's own counters (its bounds are wider: more cells may pass)
+    _, st_path = dev.intersect(my, opt, np.float64, stats=True)
+    counts_path = work_per_ray(st_path)[2]
     setup_s = time.perf_counter() - t_setup
 
     rays_d = torch.from_numpy(my).cuda()
@@ -348,7 +351,7 @@ def main():
             "roofline_fp32": {"achieved": flops_ray * n / (launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                               "flops_per_ray": flops_ray, "nominal_peak": 74.4,
                               "note": "FP32 CUDA-core issue is the path's bound; no measured FP32 peak on file"},
-            "work_per_ray": counts, "setup_s": setup_s}
+            "work_per_ray": counts, "work_per_ray_path": counts_path, "setup_s": setup_s}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s

@@ -34,7 +34,7 @@ BOUND = {"box": 0, "slab": 1, "both": 2}
 LEAF = {"newton": 0, "two_triangle": 1}
 PRECISION = {"f64": 0, "f32": 1}
 MODE = {"closest": 0, "occluded": 1}
-SCHEDULE = {"persistent": 0, "simple": 1}
+SCHEDULE = {"wavefront": 0, "simple": 1}
 KEEP_F64 = 1
 
 HIT32 = np.dtype([("t", "<f4"), ("st", "<f4", 2), ("bary", "<f4", 2), ("ng", "<f4", 3), ("tri", "<i4"),
@@ -54,7 +54,7 @@ class DmapError(RuntimeError):
 
 class _Options(C.Structure):
     _fields_ = [("bound", C.c_int), ("slab_max_level", C.c_int), ("leaf", C.c_int), ("precision", C.c_int),
-                ("mode", C.c_int), ("polish_cond", C.c_double), ("schedule", C.c_int), ("leaf_batch", C.c_int),
+                ("mode", C.c_int), ("polish_cond", C.c_double), ("schedule", C.c_int), ("rounds", C.c_int),
                 ("blocks_per_sm", C.c_int)]
 
 
@@ -111,13 +111,13 @@ class TraversalOptions:
     precision: str = "f32"
     mode: str = "closest"
     polish_cond: float = 1e4
-    schedule: str = "persistent"
-    leaf_batch: int = 16
+    schedule: str = "wavefront"
+    rounds: int = 6
     blocks_per_sm: int = 4
 
     def c(self) -> _Options:
         return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],
-                        MODE[self.mode], self.polish_cond, SCHEDULE[self.schedule], self.leaf_batch,
+                        MODE[self.mode], self.polish_cond, SCHEDULE[self.schedule], self.rounds,
                         self.blocks_per_sm)
 
 

@@ -32,7 +32,7 @@ struct dmap_context
     int device = 0;
     cudaStream_t stream = nullptr;
     unsigned *status_dev = nullptr; // device status word
-    unsigned long long *counter_dev = nullptr; // ray counter of the persistent walk (scratch)
+    dmapk::WaveScratch wave; // the wavefront schedule's scratch, grown to the largest batch
     std::atomic<int64_t> launches{0};
     std::string error;
     // device staging for dmap_intersect_host
@@ -170,7 +170,6 @@ dmap_status dmap_create(int device, dmap_context **out)
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) ||
         cudaMalloc(&ctx->status_dev, sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&ctx->counter_dev, sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemset(ctx->status_dev, 0, sizeof(unsigned)) != cudaSuccess) {
         delete ctx;
         return DMAP_ERR_CUDA;
@@ -189,7 +188,11 @@ void dmap_destroy(dmap_context *ctx)
     cudaFree(ctx->hits_dev);
     cudaFree(ctx->stats_dev);
     cudaFree(ctx->status_dev);
-    cudaFree(ctx->counter_dev);
+    cudaFree(ctx->wave.state);
+    cudaFree(ctx->wave.queue[0]);
+    cudaFree(ctx->wave.queue[1]);
+    cudaFree(ctx->wave.leaves);
+    cudaFree(ctx->wave.counters);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -207,8 +210,8 @@ void dmap_options_default(dmap_options *opt)
     opt->precision = DMAP_PRECISION_F32;
     opt->mode = DMAP_MODE_CLOSEST;
     opt->polish_cond = 1e4;
-    opt->schedule = DMAP_SCHEDULE_PERSISTENT;
-    opt->leaf_batch = 16;
+    opt->schedule = DMAP_SCHEDULE_WAVEFRONT;
+    opt->rounds = 6;
     opt->blocks_per_sm = 4;
 }
 
@@ -481,11 +484,11 @@ static dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.ray_dtype = ray_dtype == DMAP_F64 ? 2 : 0;
     q.hit_dtype = hit_dtype == DMAP_F64 ? 2 : 0;
     q.precision = o.precision;
-    if (o.schedule < 0 || o.schedule > 1 || o.leaf_batch < 0 || o.leaf_batch > 32 || o.blocks_per_sm < 0 ||
+    if (o.schedule < 0 || o.schedule > 1 || o.rounds < 0 || o.rounds > dmapk::kMaxRounds || o.blocks_per_sm < 0 ||
         o.blocks_per_sm > 16)
         return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad schedule options");
     q.schedule = o.schedule;
-    q.leaf_batch = o.leaf_batch;
+    q.rounds = o.rounds;
     q.blocks_per_sm = o.blocks_per_sm;
     return DMAP_OK;
 }
@@ -495,16 +498,37 @@ static dmap_status run_query(dmap_scene *s, const void *rays, int64_t n, const d
 {
     dmap_context *ctx = s->ctx;
     cudaError_t e;
-    if (q.precision == DMAP_PRECISION_F64)
+    if (q.precision == DMAP_PRECISION_F64) {
         e = dmapk::launch_walk64(s->tris_dev, s->n_tri, s->assets_dev, rays, n, q, hits, stats, ctx->status_dev,
                                  stream);
-    else
+    } else {
+        if (q.schedule == DMAP_SCHEDULE_WAVEFRONT && n > ctx->wave.capacity) {
+            // grow the wavefront scratch to this batch (the previous one is idle:
+            // calls on a context are serialized)
+            dmapk::WaveScratch &w = ctx->wave;
+            DMAP_CUDA(ctx, cudaStreamSynchronize(stream));
+            cudaFree(w.state);
+            cudaFree(w.queue[0]);
+            cudaFree(w.queue[1]);
+            cudaFree(w.leaves);
+            cudaFree(w.counters);
+            w = dmapk::WaveScratch{};
+            if ((e = cudaMalloc(&w.state, dmapk::wave_state_bytes() * n)) != cudaSuccess ||
+                (e = cudaMalloc((void **)&w.queue[0], sizeof(int) * n)) != cudaSuccess ||
+                (e = cudaMalloc((void **)&w.queue[1], sizeof(int) * n)) != cudaSuccess ||
+                (e = cudaMalloc(&w.leaves, dmapk::wave_leaf_bytes() * n)) != cudaSuccess ||
+                (e = cudaMalloc((void **)&w.counters, sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1))) !=
+                    cudaSuccess)
+                return cuda_fail(ctx, e, "dmap_intersect: wavefront scratch");
+            w.capacity = n;
+        }
         e = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, rays, n, q, hits, stats,
-                                 ctx->status_dev, ctx->counter_dev, stream);
+                                 ctx->status_dev, ctx->wave, stream);
+    }
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "dmap_intersect: launch");
     if (n > 0)
-        ctx->launches += 1;
+        ctx->launches += q.precision == DMAP_PRECISION_F64 ? 1 : dmapk::walk32_launches(q);
     return DMAP_OK;
 }
 

@@ -16,9 +16,27 @@ struct QueryOpts
     int ray_dtype, hit_dtype; // 0 f32, 2 f64
     int precision;            // DMAP_PRECISION_*
     int schedule;             // DMAP_SCHEDULE_*
-    int leaf_batch;           // persistent walk: run the deferred leaves once this many lanes of 32 wait
-    int blocks_per_sm;        // persistent walk: resident CTAs per SM (0 = occupancy maximum)
+    int rounds;               // wavefront: walk/leaf rounds before the inline-leaf drain
+    int blocks_per_sm;        // wavefront walk: resident 128-thread CTAs per SM
 };
+
+constexpr int kMaxRounds = 32;
+
+// Device scratch of the wavefront schedule for up to `capacity` rays: the
+// parked walk states, two ray queues (resume in / resume out), the leaf
+// jobs, and 4 counters per round (kMaxRounds + 1 rounds).
+struct WaveScratch
+{
+    void *state = nullptr;
+    int *queue[2] = {nullptr, nullptr};
+    void *leaves = nullptr;
+    unsigned long long *counters = nullptr;
+    int64_t capacity = 0;
+};
+size_t wave_state_bytes();
+size_t wave_leaf_bytes();
+// Kernel launches one FP32 query makes under these options.
+int walk32_launches(const QueryOpts &opt);
 
 // Pyramid build (pyramid.cu). `tmap` is an encoded CUtensorMap over the node
 // grid (128 bytes), `tile` the leaf cells per CTA side. Writes the FP64
@@ -37,12 +55,10 @@ cudaError_t launch_walk64(const dmapdev::TriDev *tris, int n_tri, const dmapdev:
                           int64_t n, const QueryOpts &opt, void *hits, int64_t *stats, unsigned *status,
                           cudaStream_t stream);
 
-// The FP32 walk (walk32.cu). `counter` is the persistent schedule's ray
-// counter (device scratch, one unsigned long long); the launcher zeroes it on
-// `stream` before the kernel.
+// The FP32 walk (walk32.cu). The wavefront schedule needs `ws` sized for n
+// rays; the launcher zeroes its counters (and `stats`) on `stream`.
 cudaError_t launch_walk32(const dmapdev::TriDev32 *tris32, const dmapdev::TriDev *tris64, int n_tri,
                           const dmapdev::AssetDev *assets, const void *rays, int64_t n, const QueryOpts &opt,
-                          void *hits, int64_t *stats, unsigned *status, unsigned long long *counter,
-                          cudaStream_t stream);
+                          void *hits, int64_t *stats, unsigned *status, const WaveScratch &ws, cudaStream_t stream);
 
 } // namespace dmapk

@@ -4,28 +4,32 @@
 // leaves run the reference's certified Newton leaf in double (f64_leaf.cuh),
 // which makes every reported hit the reference's own FP64 root.
 //
-// Conservative FP32 affine arithmetic. A form is c + a eu + b ev + rho with
+// Conservative FP32 arithmetic. A form is c + a eu + b ev + rho with
 // |rho| <= k; c, a, b are rounded to nearest and k is an upper bound kept
 // with round-up operations. Every operation adds to k a bound on the
 // rounding of the coefficients it produced: G * (sum of the magnitudes of
 // the terms that entered them), G = 2^-20 (16 units in the last place, more
 // than the few roundings of each step), and every input rounded from double
 // (the triangle's frame, normals, pyramid nodes) carries its own rounding
-// into k the same way. The Min-Range reciprocal square root is bounded with
-// directed rounding around rsqrtf's documented 2-ulp error. The box of a cell
-// is the outward interval hull; the tangent-space ray (transformed in double,
-// then rounded) is covered by widening every box by the ray's own rounding
-// error over the triangle's t range. Slab tests use directed-rounding
-// interval arithmetic throughout.
+// into k the same way. The reciprocal norm is bounded with directed rounding
+// around rsqrtf's documented 2-ulp error. The box of a cell is the outward
+// interval hull; the tangent-space ray (transformed in double, then rounded)
+// is covered by widening every box by the ray's own rounding error over the
+// triangle's t range. Slab tests use directed-rounding interval arithmetic.
 //
 // Two schedules:
-//  - simple: one thread per ray, one launch (the plain per-request kernel);
-//  - persistent (default): one resident grid; every lane owns a ray and
-//    fetches the next from a global counter when it finishes, and lanes that
-//    reach a leaf wait until `leaf_batch` lanes of the warp wait too, so the
-//    ~30k-instruction FP64 leaf runs for many lanes at once instead of one
-//    lane at a time (measured: the simple kernel issues 1.7 active threads
-//    per warp instruction on the cube-sphere workload).
+//  - simple: one thread per ray, one launch (the plain per-request kernel).
+//    Its lanes serialize on divergence: each lane walks its own triangles
+//    while the others wait (measured 1.6 active threads per warp
+//    instruction on the cube-sphere workload).
+//  - wavefront (default): rounds of two persistent kernels. The walk kernel
+//    keeps every lane on a node test each step: a lane whose ray reaches a
+//    leaf writes a leaf job, parks the ray's walk state and takes the next
+//    ray; the leaf kernel runs the parked leaves, 32 per warp, and queues
+//    their rays to resume. After `rounds` rounds a last walk runs the few
+//    remaining rays with their leaves inline. Every ray still visits its
+//    cells in the reference's order with the reference's t_max, so its hit
+//    is the one the simple schedule finds.
 //
 // This translation unit is compiled with -fmad=false (the FP64 leaf must
 // round like the reference); FP32 code uses explicit fmaf where it wants one.
@@ -38,7 +42,8 @@ using dmapdev::AssetDev;
 using dmapdev::TriDev;
 using dmapdev::TriDev32;
 
-constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the warp-cooperative box pass
+constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the object-box candidate mask
+constexpr unsigned FULL = 0xffffffffu;
 
 // The triangle's object box, widened, against the float ray (rounded from
 // the caller's): where the exact ray is inside the box, |t d| <= |o| + |box|,
@@ -70,17 +75,24 @@ __device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, c
 __device__ __forceinline__ void tangent_ray(const TriDev32 &T, const double *o, const double *d, float t_far,
                                             Ray32 &r)
 {
+    float ro[3], rd[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         double x = (o[0] - T.q0[0]) * T.A[a][0];
         x = __fma_rn(T.A[a][1], o[1] - T.q0[1], x);
         x = __fma_rn(T.A[a][2], o[2] - T.q0[2], x);
         double y = __fma_rn(T.A[a][2], d[2], __fma_rn(T.A[a][1], d[1], T.A[a][0] * d[0]));
-        r.o[a] = (float)x;
-        r.d[a] = (float)y;
-        r.inv[a] = r.d[a] != 0.0f ? __frcp_rn(r.d[a]) : 0.0f;
-        r.E[a] = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.o[a]), ru_mul(t_far, fabsf(r.d[a]))), 1.0f));
+        ro[a] = (float)x;
+        rd[a] = (float)y;
     }
+    r.ox = ro[0], r.oy = ro[1], r.oz = ro[2];
+    r.dx = rd[0], r.dy = rd[1], r.dz = rd[2];
+    r.ix = r.dx != 0.0f ? __frcp_rn(r.dx) : 0.0f;
+    r.iy = r.dy != 0.0f ? __frcp_rn(r.dy) : 0.0f;
+    r.iz = r.dz != 0.0f ? __frcp_rn(r.dz) : 0.0f;
+    r.ex = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.ox), ru_mul(t_far, fabsf(r.dx))), 1.0f));
+    r.ey = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.oy), ru_mul(t_far, fabsf(r.dy))), 1.0f));
+    r.ez = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.oz), ru_mul(t_far, fabsf(r.dz))), 1.0f));
 }
 
 __device__ __forceinline__ float far_bound(float t1) { return ru_add(ru_mul(t1, 1.0f + 4.0f * G), G); }
@@ -94,11 +106,11 @@ __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const Asse
 {
     Ray32 r;
     tangent_ray(T, o, d, t_far, r);
-    int si = r.d[0] < 0.0f, sj = r.d[1] < 0.0f;
+    int si = r.dx < 0.0f, sj = r.dy < 0.0f;
     float tmin_f = __double2float_rd(t_min);
     bool found = false;
     int64_t nah = 0, lah = 0;
-    const float inv_n = 1.0f / (float)g.n_leaf;
+    const int log2n = __ffs(g.n_leaf) - 1;
     for (int q = 0; q < T.n_roots; ++q) {
         Cell32 cur = {T.root_level, T.roots_i[q], T.roots_j[q]}, end = cur;
         cell_next(end, si, sj, T.root_level);
@@ -108,7 +120,7 @@ __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const Asse
                 atomicOr(status, dmapdev::kStatusCapped);
                 break;
             }
-            float w = ldexpf(inv_n, cur.level);
+            float w = pow2f(cur.level - log2n);
             if (!square_meets_domain(T, ((float)cur.i + 0.5f) * w, ((float)cur.j + 0.5f) * w, 0.5f * w)) {
                 cell_next(cur, si, sj, T.root_level);
                 continue;
@@ -198,7 +210,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
             stats[DMAP_ST_N * k + q] = st[q];
 }
 
-// ---- persistent schedule ----------------------------------------------------
+// ---- wavefront schedule ---------------------------------------------------------
 
 // The certified leaf of d64::intersect_newton (displaced_intersector.cpp:239-323)
 // for every lane of `batch` at once, stepped so that each heavy block (one
@@ -253,6 +265,7 @@ __device__ __noinline__ bool leaf64_sync(unsigned batch, const TriDev &T, const 
                         leafent ch[4];
                         int n = 0;
                         double r = 0.5 * rho;
+#pragma unroll 1
                         for (int q = 0; q < 4; ++q) {
                             double ca = e.a + ((q & 1) ? r : -r), cb = e.b + ((q & 2) ? r : -r), t_lo;
                             ++subs;
@@ -289,103 +302,155 @@ __device__ __noinline__ bool leaf64_sync(unsigned batch, const TriDev &T, const 
     return found;
 }
 
-template <bool ST, int MINB, typename R, typename H, typename Fp>
-__global__ void __launch_bounds__(128, MINB)
-    walk32_persistent(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
-                      const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n,
-                      dmapk::QueryOpts opt, H *__restrict__ hits, int64_t *__restrict__ stats,
-                      unsigned long long *__restrict__ counter, unsigned *status)
+// A parked walk: the ray's position in ObjectIntersector's triangle loop and
+// in DisplacedIntersector's walk, its current t_max and result, its
+// candidate mask and the counters of the triangle in progress.
+struct RayState
 {
-    constexpr unsigned FULL = 0xffffffffu;
-    enum : int { NEED = 0, TOP = 1, WALK = 2, LEAF = 3, DONE = 4 };
+    double t_max;
+    int tri, root, best_tri, flags;
+    int cl, ci, cj, el, ei, ej;
+    int nah, lah;
+    unsigned mask[kMaskWords];
+};
+struct LeafJob
+{
+    int ray, tri, i, j;
+};
+// RayState.flags
+constexpr int kFoundInTri = 1; // a hit was taken in the triangle in progress
+constexpr int kInWalk = 2;     // parked inside a triangle's walk (at a leaf)
+
+// Counter slots of one round: the walk's fetch counter, the leaf queue's
+// length, the leaf kernel's fetch counter, the resume queue's length.
+__device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, int round, int k)
+{
+    return c + 4 * round + k;
+}
+
+// One lane's walk from its parked or fresh state to the next leaf (parked,
+// job written) or to the end of the ray. Every lane of the warp executes one
+// node test per step; lanes that finish take another ray.
+template <bool ST, bool INLINE_LEAF, typename R, typename H, typename Fp>
+__global__ void __launch_bounds__(128, 4)
+    wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
+              const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
+              H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
+              const int *__restrict__ q_in, int round, LeafJob *__restrict__ q_leaf, unsigned long long *ctr,
+              unsigned *status)
+{
+    enum : int { NEED = 0, TOP = 1, WALK = 2, DONE = 3 };
     const int lane = threadIdx.x & 31;
+    const bool use_mask = n_tri <= 32 * kMaskWords;
+    // items of this round: every ray in round 0, else the resume queue
+    const unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
+    unsigned long long *fetch = round_ctr(ctr, round, 0);
     int phase = NEED;
-    int64_t ray = 0;
+    int ray = 0;
     double o[3], d[3], t_min = 0.0, t_max = 0.0;
-    float of[3], df[3], invf[3];
-    int tri = 0, best_tri = -1, root = 0, si = 0, sj = 0, guard = 0;
+    float of[3], df[3], invf[3], tmin_f = 0.0f;
+    int tri = 0, best_tri = -1, root = 0, si = 0, sj = 0, nah = 0, lah = 0, flags = 0, guard = 0;
     Ray32 r;
     Cell32 cur = {0, 0, 0}, end = {0, 0, 0};
-    float tmin_f = 0.0f;
-    int64_t st[DMAP_ST_N];
-    int nah = 0, lah = 0;
-    bool tri_found = false;
-    int waited = 0;
-    const int batch = opt.leaf_batch > 0 ? opt.leaf_batch : 16;
-    // Object-box candidates of the lane's ray, one bit per triangle, found
-    // by the whole warp at fetch time (32 boxes per ballot) instead of one
-    // lane scanning every box while the others wait.
-    constexpr int MW = kMaskWords;
-    const bool use_mask = n_tri <= 32 * MW;
-    unsigned mask[MW];
+    unsigned mask[kMaskWords];
 #pragma unroll
-    for (int w = 0; w < MW; ++w)
+    for (int w = 0; w < kMaskWords; ++w)
         mask[w] = 0u;
+    int64_t stl[DMAP_ST_N];
 
-    auto finish = [&]() {
-        if (best_tri < 0) {
-            d64::hit64 none;
-            store_hit<H, Fp>(hits, ray, false, none, -1, 0);
-        }
+    auto flush_stats = [&]() {
         if (ST)
             for (int q = 0; q < DMAP_ST_N; ++q)
-                stats[DMAP_ST_N * ray + q] = st[q];
-        phase = NEED;
+                stats[DMAP_ST_N * (int64_t)ray + q] += stl[q];
     };
 
     for (;;) {
-        // 1. lanes without a ray take the next ones, one atomic per warp
+        // 1. lanes without work take the next items, one atomic per warp
         unsigned need = __ballot_sync(FULL, phase == NEED);
         bool fresh = false;
         if (need) {
             int leader = __ffs(need) - 1;
             unsigned long long base = 0;
             if (lane == leader)
-                base = atomicAdd(counter, (unsigned long long)__popc(need));
+                base = atomicAdd(fetch, (unsigned long long)__popc(need));
             base = __shfl_sync(FULL, base, leader);
             if (phase == NEED) {
-                ray = (int64_t)(base + (unsigned long long)__popc(need & ((1u << lane) - 1u)));
-                if (ray >= n) {
+                unsigned long long item = base + (unsigned long long)__popc(need & ((1u << lane) - 1u));
+                if (item >= count) {
                     phase = DONE;
                 } else {
+                    ray = round == 0 ? (int)item : q_in[item];
                     load_ray(rays, ray, o, d, t_min, t_max);
+#pragma unroll
                     for (int a = 0; a < 3; ++a) {
                         of[a] = (float)o[a];
                         df[a] = (float)d[a];
                         invf[a] = df[a] != 0.0f ? __frcp_rn(df[a]) : 0.0f;
                     }
                     tmin_f = __double2float_rd(t_min);
-                    tri = 0;
-                    best_tri = -1;
                     if (ST)
                         for (int q = 0; q < DMAP_ST_N; ++q)
-                            st[q] = 0;
-                    phase = TOP;
-                    fresh = true;
+                            stl[q] = 0;
+                    if (round == 0) {
+                        tri = 0;
+                        best_tri = -1;
+                        flags = 0;
+                        nah = lah = 0;
+                        fresh = true;
+                        phase = TOP;
+                    } else {
+                        const RayState &s = states[ray];
+                        t_max = s.t_max;
+                        tri = s.tri;
+                        root = s.root;
+                        best_tri = s.best_tri;
+                        flags = s.flags;
+                        nah = s.nah;
+                        lah = s.lah;
+#pragma unroll
+                        for (int w = 0; w < kMaskWords; ++w)
+                            mask[w] = s.mask[w];
+                        // back into the walk just after the leaf (displaced_intersector.cpp:229)
+                        const TriDev32 &T = tris32[tri];
+                        float t1 = __double2float_ru(t_max);
+                        object_box(T, of, df, invf, tmin_f, t1);
+                        tangent_ray(T, o, d, far_bound(fmaxf(t1, tmin_f)), r);
+                        si = r.dx < 0.0f;
+                        sj = r.dy < 0.0f;
+                        cur = {s.cl, s.ci, s.cj};
+                        end = {s.el, s.ei, s.ej};
+                        cell_next(cur, si, sj, T.root_level);
+                        guard = 0;
+                        phase = WALK;
+                    }
                 }
             }
-            if (use_mask) {
-                unsigned todo = __ballot_sync(FULL, fresh);
-                while (todo) {
-                    int src = __ffs(todo) - 1;
-                    todo &= todo - 1;
-                    float so[3], sd[3], si3[3];
+        }
+        // round 0: the warp finds the fresh rays' candidate triangles together, 32 boxes per ballot
+        if (use_mask) {
+            unsigned todo = __ballot_sync(FULL, fresh);
+            while (todo) {
+                int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                float so[3], sd[3], sv[3];
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        so[a] = __shfl_sync(FULL, of[a], src);
-                        sd[a] = __shfl_sync(FULL, df[a], src);
-                        si3[a] = __shfl_sync(FULL, invf[a], src);
-                    }
-                    float s_tmin = __shfl_sync(FULL, tmin_f, src);
-                    float s_tmax = __shfl_sync(FULL, __double2float_ru(t_max), src);
+                for (int a = 0; a < 3; ++a) {
+                    so[a] = __shfl_sync(FULL, of[a], src);
+                    sd[a] = __shfl_sync(FULL, df[a], src);
+                    sv[a] = __shfl_sync(FULL, invf[a], src);
+                }
+                float s_tmin = __shfl_sync(FULL, tmin_f, src);
+                float s_tmax = __shfl_sync(FULL, __double2float_ru(t_max), src);
+#pragma unroll 1
+                for (int w = 0; w < kMaskWords; ++w) {
+                    int t = 32 * w + lane;
+                    float t1 = s_tmax;
+                    bool pass = t < n_tri && object_box(tris32[t], so, sd, sv, s_tmin, t1);
+                    unsigned bits = __ballot_sync(FULL, pass);
+                    if (lane == src) {
 #pragma unroll
-                    for (int w = 0; w < MW; ++w) {
-                        int t = 32 * w + lane;
-                        float t1 = s_tmax;
-                        bool pass = t < n_tri && object_box(tris32[t], so, sd, si3, s_tmin, t1);
-                        unsigned bits = __ballot_sync(FULL, pass);
-                        if (lane == src)
-                            mask[w] = bits;
+                        for (int q = 0; q < kMaskWords; ++q)
+                            mask[q] = q == w ? bits : mask[q];
                     }
                 }
             }
@@ -393,7 +458,7 @@ __global__ void __launch_bounds__(128, MINB)
         if (__all_sync(FULL, phase == DONE))
             break;
 
-        // 2. the next triangle whose object box the ray meets
+        // 2. the next triangle whose object box the ray meets (intersect_flat's loop)
         if (phase == TOP) {
             float t1 = 0.0f;
             bool hit_box = false;
@@ -402,7 +467,7 @@ __global__ void __launch_bounds__(128, MINB)
                     int w = tri >> 5;
                     unsigned bits = mask[0];
 #pragma unroll
-                    for (int q = 1; q < MW; ++q)
+                    for (int q = 1; q < kMaskWords; ++q)
                         bits = w == q ? mask[q] : bits;
                     bits &= ~0u << (tri & 31);
                     if (!bits) {
@@ -427,21 +492,26 @@ __global__ void __launch_bounds__(128, MINB)
                 }
             }
             if (!hit_box) {
-                finish();
+                if (best_tri < 0) {
+                    d64::hit64 none;
+                    store_hit<H, Fp>(hits, ray, false, none, -1, 0);
+                }
+                flush_stats();
+                phase = NEED;
             } else {
                 const TriDev32 &T = tris32[tri];
                 tangent_ray(T, o, d, far_bound(t1), r);
-                si = r.d[0] < 0.0f;
-                sj = r.d[1] < 0.0f;
+                si = r.dx < 0.0f;
+                sj = r.dy < 0.0f;
                 root = 0;
                 cur = {T.root_level, T.roots_i[0], T.roots_j[0]};
                 end = cur;
                 cell_next(end, si, sj, T.root_level);
                 guard = 0;
-                tri_found = false;
+                flags &= ~kFoundInTri;
                 nah = lah = 0;
                 if (ST)
-                    ++st[DMAP_ST_TRI];
+                    ++stl[DMAP_ST_TRI];
                 phase = WALK;
             }
         }
@@ -450,7 +520,7 @@ __global__ void __launch_bounds__(128, MINB)
         bool cand = false;
         if (phase == WALK) {
             const TriDev32 &T = tris32[tri];
-            const float inv_n = 1.0f / (float)assets[T.asset].n_leaf;
+            const int log2n = __ffs(assets[T.asset].n_leaf) - 1;
             for (;;) {
                 if (cur.level == end.level && cur.i == end.i && cur.j == end.j) {
                     if (++root < T.n_roots) {
@@ -459,9 +529,9 @@ __global__ void __launch_bounds__(128, MINB)
                         cell_next(end, si, sj, T.root_level);
                         continue;
                     }
-                    if (ST && tri_found) {
-                        st[DMAP_ST_NAH] += nah;
-                        st[DMAP_ST_LAH] += lah;
+                    if (ST && (flags & kFoundInTri)) {
+                        stl[DMAP_ST_NAH] += nah;
+                        stl[DMAP_ST_LAH] += lah;
                     }
                     ++tri;
                     phase = TOP;
@@ -473,7 +543,7 @@ __global__ void __launch_bounds__(128, MINB)
                     phase = TOP;
                     break;
                 }
-                float w = ldexpf(inv_n, cur.level);
+                float w = pow2f(cur.level - log2n);
                 if (!square_meets_domain(T, ((float)cur.i + 0.5f) * w, ((float)cur.j + 0.5f) * w, 0.5f * w)) {
                     cell_next(cur, si, sj, T.root_level);
                     continue;
@@ -488,7 +558,7 @@ __global__ void __launch_bounds__(128, MINB)
         if (cand) {
             const TriDev32 &T = tris32[tri];
             if (ST) {
-                ++st[DMAP_ST_NODE];
+                ++stl[DMAP_ST_NODE];
                 ++nah;
             }
             if (!node_test32(T, assets[T.asset], r, cur.level, cur.i, cur.j, tmin_f, __double2float_ru(t_max),
@@ -500,46 +570,119 @@ __global__ void __launch_bounds__(128, MINB)
                 cur.j = 2 * cur.j + sj;
             } else {
                 if (ST) {
-                    ++st[DMAP_ST_LEAF];
+                    ++stl[DMAP_ST_LEAF];
                     ++lah;
                 }
-                phase = LEAF;
-            }
-        }
-        __syncwarp();
-
-        // 4. deferred leaves: run them together once enough lanes wait
-        unsigned pend = __ballot_sync(FULL, phase == LEAF);
-        if (pend) {
-            unsigned live = __ballot_sync(FULL, phase != DONE);
-            int np = __popc(pend), nl = __popc(live);
-            if (np >= (batch < nl ? batch : nl) || ++waited >= 64) {
-                waited = 0;
-                if (phase == LEAF) {
-                    const TriDev32 &T = tris32[tri];
+                if (INLINE_LEAF) {
+                    // the last round: the few remaining rays finish here
                     d64::hit64 lh;
-                    if (leaf64_sync(pend, tris64[tri], assets[T.asset], o, d, t_min, t_max, cur.i, cur.j, lh,
-                                    ST ? st : nullptr) &&
+                    if (leaf64(tris64[tri], assets[T.asset], o, d, t_min, t_max, cur.i, cur.j, lh,
+                               ST ? stl : nullptr) &&
                         lh.t < t_max) {
                         t_max = lh.t;
                         best_tri = tri;
-                        tri_found = true;
+                        flags |= kFoundInTri;
                         nah = lah = 0;
                         store_hit<H, Fp>(hits, ray, true, lh, tri, DMAP_HIT_FP64_LEAF);
-                        if (opt.mode == 1)
-                            finish();
+                        if (opt.mode == 1) {
+                            flush_stats();
+                            phase = NEED;
+                        }
                     }
-                    if (phase == LEAF) {
+                    if (phase == WALK)
                         cell_next(cur, si, sj, T.root_level);
-                        phase = WALK;
-                    }
+                } else {
+                    // park at the leaf: a job for the leaf kernel, the walk state for the next round
+                    RayState &s = states[ray];
+                    s.t_max = t_max;
+                    s.tri = tri;
+                    s.root = root;
+                    s.best_tri = best_tri;
+                    s.flags = flags | kInWalk;
+                    s.cl = cur.level, s.ci = cur.i, s.cj = cur.j;
+                    s.el = end.level, s.ei = end.i, s.ej = end.j;
+                    s.nah = nah;
+                    s.lah = lah;
+#pragma unroll
+                    for (int w = 0; w < kMaskWords; ++w)
+                        s.mask[w] = mask[w];
+                    unsigned long long slot = atomicAdd(round_ctr(ctr, round, 1), 1ull);
+                    q_leaf[slot] = LeafJob{ray, tri, cur.i, cur.j};
+                    flush_stats();
+                    phase = NEED;
                 }
             }
         }
+        __syncwarp();
     }
 }
 
-int persistent_grid(int blocks_per_sm)
+// One parked leaf: the ray's current t_max, the certified leaf for the lanes
+// of `act` together, the result into the ray's state and hit record, and the
+// ray back to the resume queue unless an occlusion query is answered.
+template <bool ST, typename R, typename H, typename Fp>
+__device__ __forceinline__ void leaf_job(const TriDev *__restrict__ tris64, const AssetDev *__restrict__ assets,
+                                         const R *__restrict__ rays, const dmapk::QueryOpts &opt, H *hits,
+                                         int64_t *stats, RayState *states, LeafJob job, int round, int *q_out,
+                                         unsigned long long *ctr, unsigned act)
+{
+    double o[3], d[3], t_min, t_max;
+    load_ray(rays, job.ray, o, d, t_min, t_max);
+    RayState &s = states[job.ray];
+    t_max = s.t_max;
+    int64_t stl[DMAP_ST_N] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const TriDev &T = tris64[job.tri];
+    d64::hit64 lh;
+    bool done = false;
+    if (leaf64_sync(act, T, assets[T.asset], o, d, t_min, t_max, job.i, job.j, lh, ST ? stl : nullptr) &&
+        lh.t < t_max) {
+        s.t_max = lh.t;
+        s.best_tri = job.tri;
+        s.flags |= kFoundInTri;
+        s.nah = s.lah = 0;
+        store_hit<H, Fp>(hits, job.ray, true, lh, job.tri, DMAP_HIT_FP64_LEAF);
+        done = opt.mode == 1; // occlusion: any hit answers the query
+    }
+    if (ST) {
+        stats[DMAP_ST_N * (int64_t)job.ray + DMAP_ST_SUB] += stl[DMAP_ST_SUB];
+        stats[DMAP_ST_N * (int64_t)job.ray + DMAP_ST_NEWTON] += stl[DMAP_ST_NEWTON];
+    }
+    if (!done) {
+        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 3), 1ull);
+        q_out[slot] = job.ray;
+    }
+}
+
+// The parked leaves of a round, one per lane, 32 per warp in step (the
+// certified leaf, displaced_intersector.cpp:239-323); each ray whose walk
+// has cells left goes back to the resume queue.
+template <bool ST, typename R, typename H, typename Fp>
+__global__ void __launch_bounds__(128)
+    wave_leaf(const TriDev *__restrict__ tris64, const AssetDev *__restrict__ assets, const R *__restrict__ rays,
+              dmapk::QueryOpts opt, H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
+              const LeafJob *__restrict__ q_leaf, int round, int *__restrict__ q_out, unsigned long long *ctr)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned long long count = *round_ctr(ctr, round, 1);
+    unsigned long long *fetch = round_ctr(ctr, round, 2);
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0)
+            base = atomicAdd(fetch, 32ull);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= count)
+            break;
+        unsigned long long item = base + lane;
+        bool active = item < count;
+        unsigned act = __ballot_sync(FULL, active);
+        if (active)
+            leaf_job<ST, R, H, Fp>(tris64, assets, rays, opt, hits, stats, states, q_leaf[item], round, q_out, ctr,
+                                   act);
+        __syncwarp();
+    }
+}
+
+int sm_count()
 {
     static int sms = 0;
     if (!sms) {
@@ -547,13 +690,13 @@ int persistent_grid(int blocks_per_sm)
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    return sms * (blocks_per_sm > 0 ? blocks_per_sm : 4);
+    return sms;
 }
 
 template <typename R, typename H, typename Fp>
 cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const AssetDev *assets, const void *rays,
                    int64_t n, const dmapk::QueryOpts &opt, void *hits, int64_t *stats, unsigned *status,
-                   unsigned long long *counter, cudaStream_t stream)
+                   const dmapk::WaveScratch &ws, cudaStream_t stream)
 {
     const R *rr = static_cast<const R *>(rays);
     H *hh = static_cast<H *>(hits);
@@ -564,56 +707,97 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
                                                                            stats, status);
         return cudaGetLastError();
     }
-    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
-    if (e != cudaSuccess)
+    if (ws.capacity < n)
+        return cudaErrorInvalidValue;
+    cudaError_t e;
+    if (stats && (e = cudaMemsetAsync(stats, 0, sizeof(int64_t) * DMAP_ST_N * n, stream)) != cudaSuccess)
         return e;
+    int rounds = opt.rounds > 0 ? opt.rounds : 6;
+    if (rounds > dmapk::kMaxRounds)
+        rounds = dmapk::kMaxRounds;
+    if ((e = cudaMemsetAsync(ws.counters, 0, sizeof(unsigned long long) * 4 * (rounds + 1), stream)) != cudaSuccess)
+        return e;
+    int bps = opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4;
     int64_t need = (n + 127) / 128;
-    int grid = persistent_grid(opt.blocks_per_sm);
+    int grid = sm_count() * bps;
     if (need < grid)
         grid = (int)need;
-    // Up to two resident blocks per SM the kernel gets the full 255
-    // registers (no spills); from three on it is capped at 128.
-    bool wide = opt.blocks_per_sm > 0 && opt.blocks_per_sm <= 2;
-    if (stats) {
-        if (wide)
-            walk32_persistent<true, 2, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
-                                                                            stats, counter, status);
+    RayState *states = static_cast<RayState *>(ws.state);
+    LeafJob *leaves = static_cast<LeafJob *>(ws.leaves);
+    for (int rd = 0; rd <= rounds; ++rd) {
+        const int *q_in = ws.queue[(rd + 1) & 1];
+        int *q_out = ws.queue[rd & 1];
+        bool last = rd == rounds;
+        if (stats) {
+            if (last)
+                wave_walk<true, true, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
+                                                                          stats, states, q_in, rd, leaves,
+                                                                          ws.counters, status);
+            else
+                wave_walk<true, false, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
+                                                                           stats, states, q_in, rd, leaves,
+                                                                           ws.counters, status);
+        } else {
+            if (last)
+                wave_walk<false, true, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
+                                                                           nullptr, states, q_in, rd, leaves,
+                                                                           ws.counters, status);
+            else
+                wave_walk<false, false, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt,
+                                                                            hh, nullptr, states, q_in, rd, leaves,
+                                                                            ws.counters, status);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+        if (last)
+            break;
+        int lgrid = sm_count() * 4;
+        if (stats)
+            wave_leaf<true, R, H, Fp><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, hh, stats, states, leaves, rd,
+                                                                q_out, ws.counters);
         else
-            walk32_persistent<true, 4, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
-                                                                            stats, counter, status);
-    } else {
-        if (wide)
-            walk32_persistent<false, 2, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt,
-                                                                             hh, nullptr, counter, status);
-        else
-            walk32_persistent<false, 4, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt,
-                                                                             hh, nullptr, counter, status);
+            wave_leaf<false, R, H, Fp><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, hh, nullptr, states, leaves,
+                                                                 rd, q_out, ws.counters);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 } // namespace
 
 namespace dmapk
 {
+size_t wave_state_bytes() { return sizeof(RayState); }
+size_t wave_leaf_bytes() { return sizeof(LeafJob); }
+
+int walk32_launches(const QueryOpts &opt)
+{
+    if (opt.schedule == 1)
+        return 1;
+    int rounds = opt.rounds > 0 ? opt.rounds : 6;
+    if (rounds > kMaxRounds)
+        rounds = kMaxRounds;
+    return 2 * rounds + 1;
+}
+
 cudaError_t launch_walk32(const dmapdev::TriDev32 *t32, const dmapdev::TriDev *t64, int n_tri,
                           const dmapdev::AssetDev *assets, const void *rays, int64_t n, const QueryOpts &opt,
-                          void *hits, int64_t *stats, unsigned *status, unsigned long long *counter,
-                          cudaStream_t stream)
+                          void *hits, int64_t *stats, unsigned *status, const WaveScratch &ws, cudaStream_t stream)
 {
     if (n <= 0)
         return cudaSuccess;
     bool r64 = opt.ray_dtype == 2, h64 = opt.hit_dtype == 2;
     if (r64 && h64)
-        return launch<double, dmapdev::Hit64, double>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status,
-                                                      counter, stream);
+        return launch<double, dmapdev::Hit64, double>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status, ws,
+                                                      stream);
     if (r64)
-        return launch<double, dmapdev::Hit32, float>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status,
-                                                     counter, stream);
+        return launch<double, dmapdev::Hit32, float>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status, ws,
+                                                     stream);
     if (h64)
-        return launch<float, dmapdev::Hit64, double>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status,
-                                                     counter, stream);
-    return launch<float, dmapdev::Hit32, float>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status, counter,
+        return launch<float, dmapdev::Hit64, double>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status, ws,
+                                                     stream);
+    return launch<float, dmapdev::Hit32, float>(t32, t64, n_tri, assets, rays, n, opt, hits, stats, status, ws,
                                                 stream);
 }
 } // namespace dmapk

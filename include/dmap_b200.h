@@ -142,8 +142,8 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *o
 #define DMAP_MODE_CLOSEST 0  /* closest hit in (t_min, t_max): rtcIntersect1 / intersect_callback */
 #define DMAP_MODE_OCCLUDED 1 /* any hit in (t_min, t_max): rtcOccluded1 / occluded_callback */
 
-#define DMAP_SCHEDULE_PERSISTENT 0 /* resident grid, per-lane ray fetch, batched leaves (default) */
-#define DMAP_SCHEDULE_SIMPLE 1     /* one thread per ray, one launch: the plain per-request kernel */
+#define DMAP_SCHEDULE_WAVEFRONT 0 /* rounds of a persistent walk kernel and a leaf kernel (default) */
+#define DMAP_SCHEDULE_SIMPLE 1    /* one thread per ray, one launch: the plain per-request kernel */
 
 typedef struct dmap_options {
     int bound;          /* DMAP_BOUND_*, default BOTH */
@@ -152,9 +152,9 @@ typedef struct dmap_options {
     int precision;      /* DMAP_PRECISION_*, default F32 */
     int mode;           /* DMAP_MODE_*, default CLOSEST */
     double polish_cond; /* FP32 path: FP64 Newton polish when cond(J) exceeds this (default 1e4; 0 = always) */
-    int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default PERSISTENT */
-    int leaf_batch;     /* persistent: run deferred leaves once this many lanes of a warp wait (1..32, default 16) */
-    int blocks_per_sm;  /* persistent: resident 128-thread blocks per SM (default 4) */
+    int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
+    int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32, default 6) */
+    int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 4) */
 } dmap_options;
 
 /* Fills the defaults above. */

@@ -44,15 +44,30 @@ def test_f32_quad(ctx, oracle, bound, k):
     assert n > 1000 and ratio < 1.5
 
 
-@pytest.mark.parametrize("schedule,batch,bps", [("persistent", 16, 4), ("persistent", 1, 1), ("persistent", 32, 2),
-                                                ("simple", 16, 4)])
-def test_f32_sphere(ctx, oracle, schedule, batch, bps):
+@pytest.mark.parametrize("schedule,rounds,bps", [("wavefront", 6, 4), ("wavefront", 0, 1), ("wavefront", 1, 2),
+                                                 ("wavefront", 32, 4), ("simple", 6, 4)])
+def test_f32_sphere(ctx, oracle, schedule, rounds, bps):
+    """Every schedule gives the oracle's hits; rounds = 0 runs everything in
+    the inline-leaf walk, rounds = 1 parks each ray once."""
     sc = helpers.small_sphere(32)
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
     rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 2000),
                            helpers.aimed_rays(cpu, 2000)[0]])
-    n, ratio = _check(cpu, dev, rays, schedule=schedule, leaf_batch=batch, blocks_per_sm=bps)
+    n, ratio = _check(cpu, dev, rays, schedule=schedule, rounds=rounds, blocks_per_sm=bps)
     assert n > 1000 and ratio < 1.5
+
+
+def test_f32_schedules_agree_bitwise(ctx, oracle):
+    """The wavefront and the simple schedule return the same records."""
+    sc = helpers.small_sphere(32)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = np.concatenate([scenes.sphere_camera_rays(64, 36), helpers.near_surface_rays(cpu, 1500)])
+    a, sa = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront"), np.float64, stats=True)
+    b, sb = dev.intersect(rays, dm.TraversalOptions(schedule="simple"), np.float64, stats=True)
+    assert np.array_equal(a["tri"], b["tri"])
+    hit = a["tri"] >= 0
+    assert np.array_equal(a["t"][hit], b["t"][hit]) and np.array_equal(a["ng"][hit], b["ng"][hit])
+    assert np.array_equal(sa[:, 2], sb[:, 2]) and np.array_equal(sa[:, 3], sb[:, 3])
 
 
 def test_f32_f16_texels_and_offset(ctx, oracle):
