@@ -313,13 +313,21 @@ struct RayState
     int nah, lah;
     unsigned mask[kMaskWords];
 };
+// Up to kCollect consecutive leaves of one triangle's walk, in walk order.
+// The walk goes on past a leaf with the t_max it has (it cannot know the
+// leaf's result yet), so it may also reach leaves the reference prunes with
+// the smaller t_max of a hit; the leaf kernel runs them with that smaller
+// t_max, where they cannot report a nearer root than the one found, so the
+// ray's hit is unchanged.
+constexpr int kCollect = 4;
 struct LeafJob
 {
-    int ray, tri, i, j;
+    int ray, tri, n, pad;
+    int i[kCollect], j[kCollect];
 };
 // RayState.flags
 constexpr int kFoundInTri = 1; // a hit was taken in the triangle in progress
-constexpr int kInWalk = 2;     // parked inside a triangle's walk (at a leaf)
+constexpr int kAtEnd = 2;      // parked at the end of a triangle's walk: resume without cell_next
 
 // Counter slots of one round: the walk's fetch counter, the leaf queue's
 // length, the leaf kernel's fetch counter, the resume queue's length.
@@ -357,11 +365,41 @@ __global__ void __launch_bounds__(128, 4)
     for (int w = 0; w < kMaskWords; ++w)
         mask[w] = 0u;
     int64_t stl[DMAP_ST_N];
+    int nl = 0, li0 = 0, lj0 = 0, li1 = 0, lj1 = 0, li2 = 0, lj2 = 0, li3 = 0, lj3 = 0; // collected leaves
 
     auto flush_stats = [&]() {
         if (ST)
             for (int q = 0; q < DMAP_ST_N; ++q)
                 stats[DMAP_ST_N * (int64_t)ray + q] += stl[q];
+    };
+    // Park the ray: its collected leaves become one job, its walk state
+    // waits for the next round (at_end: the triangle's walk is over).
+    auto park = [&](bool at_end) {
+        RayState &s = states[ray];
+        s.t_max = t_max;
+        s.tri = tri;
+        s.root = root;
+        s.best_tri = best_tri;
+        s.flags = at_end ? (flags | kAtEnd) : (flags & ~kAtEnd);
+        s.cl = cur.level, s.ci = cur.i, s.cj = cur.j;
+        s.el = end.level, s.ei = end.i, s.ej = end.j;
+        s.nah = nah;
+        s.lah = lah;
+#pragma unroll
+        for (int w = 0; w < kMaskWords; ++w)
+            s.mask[w] = mask[w];
+        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 1), 1ull);
+        LeafJob job;
+        job.ray = ray;
+        job.tri = tri;
+        job.n = nl;
+        job.pad = 0;
+        job.i[0] = li0, job.j[0] = lj0, job.i[1] = li1, job.j[1] = lj1;
+        job.i[2] = li2, job.j[2] = lj2, job.i[3] = li3, job.j[3] = lj3;
+        q_leaf[slot] = job;
+        nl = 0;
+        flush_stats();
+        phase = NEED;
     };
 
     for (;;) {
@@ -419,8 +457,11 @@ __global__ void __launch_bounds__(128, 4)
                         sj = r.dy < 0.0f;
                         cur = {s.cl, s.ci, s.cj};
                         end = {s.el, s.ei, s.ej};
-                        cell_next(cur, si, sj, T.root_level);
+                        if (!(flags & kAtEnd))
+                            cell_next(cur, si, sj, T.root_level); // past the last leaf (displaced_intersector.cpp:229)
+                        flags &= ~kAtEnd;
                         guard = 0;
+                        nl = 0;
                         phase = WALK;
                     }
                 }
@@ -523,11 +564,17 @@ __global__ void __launch_bounds__(128, 4)
             const int log2n = __ffs(assets[T.asset].n_leaf) - 1;
             for (;;) {
                 if (cur.level == end.level && cur.i == end.i && cur.j == end.j) {
-                    if (++root < T.n_roots) {
+                    if (root + 1 < T.n_roots) {
+                        ++root;
                         cur = {T.root_level, T.roots_i[root], T.roots_j[root]};
                         end = cur;
                         cell_next(end, si, sj, T.root_level);
                         continue;
+                    }
+                    if (!INLINE_LEAF && nl > 0) {
+                        // the collected leaves decide this triangle's t_max before the next one
+                        park(true);
+                        break;
                     }
                     if (ST && (flags & kFoundInTri)) {
                         stl[DMAP_ST_NAH] += nah;
@@ -592,24 +639,19 @@ __global__ void __launch_bounds__(128, 4)
                     if (phase == WALK)
                         cell_next(cur, si, sj, T.root_level);
                 } else {
-                    // park at the leaf: a job for the leaf kernel, the walk state for the next round
-                    RayState &s = states[ray];
-                    s.t_max = t_max;
-                    s.tri = tri;
-                    s.root = root;
-                    s.best_tri = best_tri;
-                    s.flags = flags | kInWalk;
-                    s.cl = cur.level, s.ci = cur.i, s.cj = cur.j;
-                    s.el = end.level, s.ei = end.i, s.ej = end.j;
-                    s.nah = nah;
-                    s.lah = lah;
-#pragma unroll
-                    for (int w = 0; w < kMaskWords; ++w)
-                        s.mask[w] = mask[w];
-                    unsigned long long slot = atomicAdd(round_ctr(ctr, round, 1), 1ull);
-                    q_leaf[slot] = LeafJob{ray, tri, cur.i, cur.j};
-                    flush_stats();
-                    phase = NEED;
+                    // collect the leaf; park once kCollect are held
+                    li0 = nl == 0 ? cur.i : li0;
+                    lj0 = nl == 0 ? cur.j : lj0;
+                    li1 = nl == 1 ? cur.i : li1;
+                    lj1 = nl == 1 ? cur.j : lj1;
+                    li2 = nl == 2 ? cur.i : li2;
+                    lj2 = nl == 2 ? cur.j : lj2;
+                    li3 = nl == 3 ? cur.i : li3;
+                    lj3 = nl == 3 ? cur.j : lj3;
+                    if (++nl == kCollect)
+                        park(false);
+                    else
+                        cell_next(cur, si, sj, T.root_level);
                 }
             }
         }
@@ -632,16 +674,26 @@ __device__ __forceinline__ void leaf_job(const TriDev *__restrict__ tris64, cons
     t_max = s.t_max;
     int64_t stl[DMAP_ST_N] = {0, 0, 0, 0, 0, 0, 0, 0};
     const TriDev &T = tris64[job.tri];
-    d64::hit64 lh;
     bool done = false;
-    if (leaf64_sync(act, T, assets[T.asset], o, d, t_min, t_max, job.i, job.j, lh, ST ? stl : nullptr) &&
-        lh.t < t_max) {
-        s.t_max = lh.t;
-        s.best_tri = job.tri;
-        s.flags |= kFoundInTri;
-        s.nah = s.lah = 0;
-        store_hit<H, Fp>(hits, job.ray, true, lh, job.tri, DMAP_HIT_FP64_LEAF);
-        done = opt.mode == 1; // occlusion: any hit answers the query
+    // the ray's collected leaves in walk order, lanes of the warp together
+    for (int q = 0; q < kCollect; ++q) {
+        bool mine = q < job.n && !done;
+        unsigned batch = __ballot_sync(act, mine); // every lane of act takes part
+        if (!batch)
+            break;
+        if (!mine)
+            continue;
+        d64::hit64 lh;
+        if (leaf64_sync(batch, T, assets[T.asset], o, d, t_min, t_max, job.i[q], job.j[q], lh, ST ? stl : nullptr) &&
+            lh.t < t_max) {
+            t_max = lh.t;
+            s.t_max = lh.t;
+            s.best_tri = job.tri;
+            s.flags |= kFoundInTri;
+            s.nah = s.lah = 0;
+            store_hit<H, Fp>(hits, job.ray, true, lh, job.tri, DMAP_HIT_FP64_LEAF);
+            done = opt.mode == 1; // occlusion: any hit answers the query
+        }
     }
     if (ST) {
         stats[DMAP_ST_N * (int64_t)job.ray + DMAP_ST_SUB] += stl[DMAP_ST_SUB];
