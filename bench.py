@@ -61,10 +61,20 @@ def build_scene(config: str, small: bool):
     with cf.ThreadPoolExecutor(min(16, os.cpu_count() or 4)) as ex:
         maps = list(ex.map(one, range(6 * k * k)))
     sc = scenes.cube_sphere_scene(1, k)   # geometry only, tiny maps replaced below
+    texel = np.float16 if config == "sphere16" else np.float32
     for pid, a in enumerate(sc.assets):
-        a.nodes = scenes.close_tile(maps[pid], repeat=False).astype(np.float32)
+        a.nodes = scenes.close_tile(maps[pid], repeat=False).astype(texel)
     w, h = (480, 270) if small else (1920, 1080)
     return sc, scenes.sphere_camera_rays(w, h)
+
+
+def extra_rays(config: str, sc, small: bool):
+    """The precision variant's grazing rays: aimed at random base-surface
+    points from 0.1-5 deg above the tangent plane, origins backed off."""
+    if config != "sphere16":
+        return np.zeros((0, 8), np.float32)
+    p, m = scenes.base_points(sc, 100_000 if small else 1_000_000, seed=scenes.SEED + 7)
+    return scenes.grazing_rays(p, m, seed=scenes.SEED + 8)
 
 
 class Clocks:
@@ -119,6 +129,19 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profiled_traffic_per_ray(args):
+    """DRAM bytes per ray of one query, from the committed ncu summary of the
+    same schedule (a line `traffic_bytes_per_ray <schedule> <value>`), or None."""
+    p = ROOT / "profiles" / "traversal_sphere_dram.md"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        f = ln.strip().strip("`").split()
+        if len(f) == 3 and f[0] == "traffic_bytes_per_ray" and f[1] == args.schedule:
+            return float(f[2])
+    return None
 
 
 def work_per_ray(stats):
@@ -209,6 +232,10 @@ def run_cpu(args, rank, world):
 def workload_name(args):
     if args.config == "quad":
         return "quad 512^2 FP32, 256x256 camera rays" if not args.small else "quad 128^2 (small)"
+    if args.config == "sphere16":
+        return ("cube sphere 96 patches x 2048^2 FP16 texels, 1920x1080 jittered primary + 1 diffuse bounce "
+                "per hit + 1M grazing rays (0.1-5 deg)" if not args.small
+                else "cube sphere 96 patches x 256^2 FP16 + 100k grazing (small)")
     return ("cube sphere 96 patches x 2048^2 FP32, 1920x1080 jittered primary + 1 diffuse bounce per hit"
             if not args.small else "cube sphere 96 patches x 256^2 (small)")
 
@@ -219,7 +246,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
-    ap.add_argument("--config", default="sphere", choices=["sphere", "quad"])
+    ap.add_argument("--config", default="sphere", choices=["sphere", "sphere16", "quad"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
     ap.add_argument("--rounds", type=int, default=6)
@@ -257,7 +284,7 @@ def main():
     h0 = dev.intersect(prim, ref_opt, np.float64)
     hit = h0["tri"] >= 0
     bounce = scenes.bounce_rays(prim[hit], h0["t"][hit], h0["ng"][hit])
-    rays_all = np.concatenate([prim, bounce]).astype(np.float32)
+    rays_all = np.concatenate([prim, bounce, extra_rays(args.config, sc, args.small)]).astype(np.float32)
     # this rank's share
     n_all = len(rays_all)
     lo, hi = rank * n_all // world, (rank + 1) * n_all // world
@@ -334,8 +361,11 @@ def main():
     e2e = n_all / e2e_s / 1e6
 
     hbm, peak_src = peaks()
-    launch_ms = ms / max(1, launches // args.steps)
-    achieved_gbs = bytes_ray * n / (launch_ms * 1e-3) / 1e9
+    # the unit is one query: its walk and leaf kernels run back to back on one
+    # stream and the events bracket all of them
+    achieved_gbs = bytes_ray * n / (ms * 1e-3) / 1e9
+    traffic_ray = profiled_traffic_per_ray(args)
+    traffic = traffic_ray * n if traffic_ray else None
     line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
@@ -346,9 +376,10 @@ def main():
                     "d2h_bytes_per_step": int(n * 48)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved_gbs / hbm, "traffic": None, "peak_source": peak_src,
-                         "kernel": "walk", "bytes_per_ray": bytes_ray},
-            "roofline_fp32": {"achieved": flops_ray * n / (launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved_gbs / hbm, "traffic": traffic, "peak_source": peak_src,
+                         "kernel": f"one query: {launches // args.steps} launches of the walk and leaf kernels",
+                         "bytes_per_ray": bytes_ray, "traffic_per_ray": traffic_ray},
+            "roofline_fp32": {"achieved": flops_ray * n / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                               "flops_per_ray": flops_ray, "nominal_peak": 74.4,
                               "note": "FP32 CUDA-core issue is the path's bound; no measured FP32 peak on file"},
             "work_per_ray": counts, "work_per_ray_path": counts_path, "setup_s": setup_s}

@@ -20,6 +20,7 @@ entry point raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 from pathlib import Path
 from typing import Optional, Sequence
@@ -27,7 +28,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libdmap_b200.so"
+# DMAP_B200_LIB names another build of the library (tuning variants)
+LIB_PATH = Path(os.environ.get("DMAP_B200_LIB") or _PKG / "libdmap_b200.so")
 
 F32, F16, F64 = 0, 1, 2
 BOUND = {"box": 0, "slab": 1, "both": 2}

@@ -42,6 +42,15 @@ using dmapdev::AssetDev;
 using dmapdev::TriDev;
 using dmapdev::TriDev32;
 
+// Resident 128-thread CTAs per SM the walk and leaf kernels are compiled for
+// (register budget: 65536 / (128 x blocks) per thread).
+#ifndef DMAP_WALK_MIN_BLOCKS
+#define DMAP_WALK_MIN_BLOCKS 4
+#endif
+#ifndef DMAP_LEAF_MIN_BLOCKS
+#define DMAP_LEAF_MIN_BLOCKS 1
+#endif
+
 constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the object-box candidate mask
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -340,7 +349,7 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
 template <bool ST, bool INLINE_LEAF, typename R, typename H, typename Fp>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
               H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
@@ -709,7 +718,7 @@ __device__ __forceinline__ void leaf_job(const TriDev *__restrict__ tris64, cons
 // certified leaf, displaced_intersector.cpp:239-323); each ray whose walk
 // has cells left goes back to the resume queue.
 template <bool ST, typename R, typename H, typename Fp>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
     wave_leaf(const TriDev *__restrict__ tris64, const AssetDev *__restrict__ assets, const R *__restrict__ rays,
               dmapk::QueryOpts opt, H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
               const LeafJob *__restrict__ q_leaf, int round, int *__restrict__ q_out, unsigned long long *ctr)

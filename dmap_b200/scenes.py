@@ -299,6 +299,21 @@ def uniform_direction(rng, n):
     return np.stack([s * np.cos(phi), s * np.sin(phi), z], axis=1)
 
 
+def base_points(scene: Scene, n: int, seed: int = SEED):
+    """n random points on the scene's base triangles (uniform triangle,
+    uniform barycentrics) and their interpolated vertex normals."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k = rng.integers(0, len(scene.tris), n)
+    a, b = rng.random(n), rng.random(n)
+    flip = a + b > 1.0
+    a, b = np.where(flip, 1.0 - a, a), np.where(flip, 1.0 - b, b)
+    t = scene.tris[k]
+    w = np.stack([1.0 - a - b, a, b], 1)
+    p = w[:, 0:1] * t[:, 0:3] + w[:, 1:2] * t[:, 3:6] + w[:, 2:3] * t[:, 6:9]
+    m = w[:, 0:1] * t[:, 9:12] + w[:, 1:2] * t[:, 12:15] + w[:, 2:3] * t[:, 15:18]
+    return p, m / np.linalg.norm(m, axis=1, keepdims=True)
+
+
 def grazing_rays(points: np.ndarray, normals: np.ndarray, seed: int = SEED) -> np.ndarray:
     """Rays aimed at surface points from a tangent direction tilted
     0.1-5 deg (log-uniform) toward the surface, origin backed off 0.05-1."""

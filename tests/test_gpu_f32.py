@@ -1,8 +1,8 @@
 """The FP32 path against the oracle: the walk's node tests are FP32 and
 widened outward, the leaves are the reference's FP64 leaf, so the hit set
-must equal the oracle's and every reported root must be the oracle's root
-(|dt| <= 4 residual tolerances; in practice identical), with never fewer node
-tests admitted than the FP64 walk (conservative bounds)."""
+must equal the oracle's and every reported hit record (t, st, bary, ng, i, j)
+must be the oracle's, bit for bit; a ray the FP64 walk finds a root for
+reaches a leaf here too (conservative bounds)."""
 import numpy as np
 import pytest
 
@@ -24,9 +24,12 @@ def _check(cpu, dev, rays, bound="both", k=1, **kw):
     hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, precision="f32", **kw), np.float64, stats=True)
     assert np.array_equal(hd["tri"] >= 0, ho[:, 10] >= 0), "hit/miss set differs"
     hit = ho[:, 10] >= 0
-    tol = np.array([cpu.triangle_info(t)[2] for t in range(cpu.n_tri)])
-    dt = np.abs(hd["t"][hit] - ho[hit, 0])
-    assert (dt <= 4 * tol[ho[hit, 10].astype(int)] + 1e-12).all()
+    assert np.array_equal(hd["tri"][hit], ho[hit, 10].astype(np.int32))
+    assert np.array_equal(hd["t"][hit], ho[hit, 0]), "t differs from the oracle's FP64 root"
+    assert np.array_equal(hd["st"][hit], ho[hit, 1:3]) and np.array_equal(hd["bary"][hit], ho[hit, 3:5])
+    assert np.array_equal(hd["ng"][hit], ho[hit, 5:8])
+    assert np.array_equal(hd["i"][hit], ho[hit, 8].astype(np.int32))
+    assert np.array_equal(hd["j"][hit], ho[hit, 9].astype(np.int32))
     # the FP32 bounds enclose the surface: a ray whose FP64 walk finds a root
     # reaches that root's leaf here too
     got = hd["tri"] >= 0
