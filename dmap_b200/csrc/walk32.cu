@@ -25,8 +25,9 @@
 //  - wavefront (default): rounds of two persistent kernels. The walk kernel
 //    keeps every lane on a node test each step: a lane whose ray reaches a
 //    leaf writes a leaf job, parks the ray's walk state and takes the next
-//    ray; the leaf kernel runs the parked leaves, 32 per warp, and queues
-//    their rays to resume. After `rounds` rounds a last walk runs the few
+//    ray; the leaf kernel runs the parked leaves, one job per lane, each
+//    lane taking the next job when its own is done, and queues their rays
+//    to resume. After `rounds` rounds a last walk runs the few
 //    remaining rays with their leaves inline. Every ray still visits its
 //    cells in the reference's order with the reference's t_max, so its hit
 //    is the one the simple schedule finds.
@@ -220,96 +221,6 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
 }
 
 // ---- wavefront schedule ---------------------------------------------------------
-
-// The certified leaf of d64::intersect_newton (displaced_intersector.cpp:239-323)
-// for every lane of `batch` at once, stepped so that each heavy block (one
-// sub-square expansion: four bounds and the sort; one Newton run) executes
-// once per step for all lanes that need it, with the warp reconverged
-// between blocks. The arithmetic and the search order are the reference's:
-// each lane's result equals intersect_newton's bit for bit.
-__device__ __noinline__ bool leaf64_sync(unsigned batch, const TriDev &T, const AssetDev &g, const double *o,
-                                         const double *d, double t_min, double t_max, int i, int j, d64::hit64 &hit,
-                                         int64_t *st)
-{
-    using namespace d64;
-    constexpr int kDepth = 5; // subdivision_depth
-    v3 O = V3(o[0], o[1], o[2]), D = V3(d[0], d[1], d[2]);
-    leafbound L;
-    L.w = cell_width(g, 0);
-    L.lo = {i * L.w, j * L.w};
-    L.h00 = grid_h(g, L.lo.x, L.lo.y);
-    L.h10 = grid_h(g, L.lo.x + L.w, L.lo.y);
-    L.h01 = grid_h(g, L.lo.x, L.lo.y + L.w);
-    L.h11 = grid_h(g, L.lo.x + L.w, L.lo.y + L.w);
-    v2 c = add2(L.lo, V2(0.5 * L.w, 0.5 * L.w));
-    double hw = 0.5 * L.w;
-    L.N_hat = AF3(add3(add3(L3(T.m0), mul3(c.x, L3(T.Mu))), mul3(c.y, L3(T.Mv))), mul3(hw, L3(T.Mu)),
-                  mul3(hw, L3(T.Mv)));
-    normalize(L.N_hat);
-    L.o = O;
-    L.d_len = norm3(D);
-    L.dn = div3(D, L.d_len);
-    plane_basis(L.dn, L.d1, L.d2);
-
-    bool found = false;
-    int64_t subs = 0, iters = 0;
-    leafent stack[4 * kDepth + 4];
-    int sp = 0;
-    stack[sp++] = {0.5, 0.5, -INFINITY, 0};
-    bool first = true, alive = true;
-    while (__any_sync(batch, alive)) {
-        bool newton = false;
-        leafent e = {0.0, 0.0, 0.0, 0};
-        if (alive) {
-            if (sp == 0) {
-                alive = false;
-            } else {
-                e = stack[--sp];
-                if (first || e.t_lo < t_max) {
-                    first = false;
-                    if (e.depth == kDepth) {
-                        newton = true;
-                    } else {
-                        double rho = ldexp(0.5, -e.depth);
-                        leafent ch[4];
-                        int n = 0;
-                        double r = 0.5 * rho;
-#pragma unroll 1
-                        for (int q = 0; q < 4; ++q) {
-                            double ca = e.a + ((q & 1) ? r : -r), cb = e.b + ((q & 2) ? r : -r), t_lo;
-                            ++subs;
-                            if (sub_square_bound(T, L, ca, cb, r, t_min, t_max, t_lo))
-                                ch[n++] = {ca, cb, t_lo, e.depth + 1};
-                        }
-                        for (int p = 1; p < n; ++p)
-                            for (int q = p; q > 0 && ch[q].t_lo < ch[q - 1].t_lo; --q) {
-                                leafent x = ch[q];
-                                ch[q] = ch[q - 1];
-                                ch[q - 1] = x;
-                            }
-                        for (int q = n - 1; q >= 0; --q)
-                            stack[sp++] = ch[q];
-                    }
-                }
-            }
-        }
-        __syncwarp(batch);
-        if (newton) {
-            hit64 h;
-            if (newton_from(T, g, O, D, t_min, t_max, i, j, add2(L.lo, mul2(L.w, V2(e.a, e.b))), h, iters)) {
-                hit = h;
-                t_max = h.t;
-                found = true;
-            }
-        }
-        __syncwarp(batch);
-    }
-    if (st) {
-        st[DMAP_ST_SUB] += subs;
-        st[DMAP_ST_NEWTON] += iters;
-    }
-    return found;
-}
 
 // A parked walk: the ray's position in ObjectIntersector's triangle loop and
 // in DisplacedIntersector's walk, its current t_max and result, its
@@ -668,54 +579,14 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     }
 }
 
-// One parked leaf: the ray's current t_max, the certified leaf for the lanes
-// of `act` together, the result into the ray's state and hit record, and the
-// ray back to the resume queue unless an occlusion query is answered.
-template <bool ST, typename R, typename H, typename Fp>
-__device__ __forceinline__ void leaf_job(const TriDev *__restrict__ tris64, const AssetDev *__restrict__ assets,
-                                         const R *__restrict__ rays, const dmapk::QueryOpts &opt, H *hits,
-                                         int64_t *stats, RayState *states, LeafJob job, int round, int *q_out,
-                                         unsigned long long *ctr, unsigned act)
-{
-    double o[3], d[3], t_min, t_max;
-    load_ray(rays, job.ray, o, d, t_min, t_max);
-    RayState &s = states[job.ray];
-    t_max = s.t_max;
-    int64_t stl[DMAP_ST_N] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const TriDev &T = tris64[job.tri];
-    bool done = false;
-    // the ray's collected leaves in walk order, lanes of the warp together
-    for (int q = 0; q < kCollect; ++q) {
-        bool mine = q < job.n && !done;
-        unsigned batch = __ballot_sync(act, mine); // every lane of act takes part
-        if (!batch)
-            break;
-        if (!mine)
-            continue;
-        d64::hit64 lh;
-        if (leaf64_sync(batch, T, assets[T.asset], o, d, t_min, t_max, job.i[q], job.j[q], lh, ST ? stl : nullptr) &&
-            lh.t < t_max) {
-            t_max = lh.t;
-            s.t_max = lh.t;
-            s.best_tri = job.tri;
-            s.flags |= kFoundInTri;
-            s.nah = s.lah = 0;
-            store_hit<H, Fp>(hits, job.ray, true, lh, job.tri, DMAP_HIT_FP64_LEAF);
-            done = opt.mode == 1; // occlusion: any hit answers the query
-        }
-    }
-    if (ST) {
-        stats[DMAP_ST_N * (int64_t)job.ray + DMAP_ST_SUB] += stl[DMAP_ST_SUB];
-        stats[DMAP_ST_N * (int64_t)job.ray + DMAP_ST_NEWTON] += stl[DMAP_ST_NEWTON];
-    }
-    if (!done) {
-        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 3), 1ull);
-        q_out[slot] = job.ray;
-    }
-}
-
-// The parked leaves of a round, one per lane, 32 per warp in step (the
-// certified leaf, displaced_intersector.cpp:239-323); each ray whose walk
+// The parked leaves of a round (the certified leaf, d64::intersect_newton,
+// displaced_intersector.cpp:239-323). Each lane holds one job at a time and
+// takes the next one as soon as its own is done, so a warp's lanes stay busy
+// however long their leaves run. A step of the loop runs, for the lanes that
+// need it: the leaf setup, one sub-square expansion (four bounds, the sort,
+// the push) or one Newton run, with the warp reconverged between blocks.
+// Each lane's search is intersect_newton's, in the same order with the same
+// arithmetic, so each ray's result equals it bit for bit. A ray whose walk
 // has cells left goes back to the resume queue.
 template <bool ST, typename R, typename H, typename Fp>
 __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
@@ -723,22 +594,150 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
               dmapk::QueryOpts opt, H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
               const LeafJob *__restrict__ q_leaf, int round, int *__restrict__ q_out, unsigned long long *ctr)
 {
+    using namespace d64;
+    constexpr int kDepth = 5; // subdivision_depth
+    enum : int { NEED = 0, SETUP = 1, SEARCH = 2, DONE = 3 };
     const int lane = threadIdx.x & 31;
     const unsigned long long count = *round_ctr(ctr, round, 1);
     unsigned long long *fetch = round_ctr(ctr, round, 2);
+    int phase = NEED;
+    unsigned long long item = 0;
+    int ray = 0, tri = 0, n_leaves = 0, q = 0, li = 0, lj = 0, sp = 0;
+    bool first = false, answered = false;
+    double t_min = 0.0, t_max = 0.0;
+    v3 O = V3(0.0, 0.0, 0.0), D = O;
+    leafbound L;
+    leafent stack[4 * kDepth + 4];
+    int64_t subs = 0, iters = 0;
+
     for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0)
-            base = atomicAdd(fetch, 32ull);
-        base = __shfl_sync(FULL, base, 0);
-        if (base >= count)
+        // lanes without a job take the next ones, one atomic per warp
+        unsigned need = __ballot_sync(FULL, phase == NEED);
+        if (need) {
+            int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if (lane == leader)
+                base = atomicAdd(fetch, (unsigned long long)__popc(need));
+            base = __shfl_sync(FULL, base, leader);
+            if (phase == NEED) {
+                item = base + (unsigned long long)__popc(need & ((1u << lane) - 1u));
+                if (item >= count) {
+                    phase = DONE;
+                } else {
+                    const LeafJob &J = q_leaf[item];
+                    ray = J.ray;
+                    tri = J.tri;
+                    n_leaves = J.n;
+                    q = 0;
+                    double o[3], d[3];
+                    load_ray(rays, ray, o, d, t_min, t_max);
+                    O = V3(o[0], o[1], o[2]);
+                    D = V3(d[0], d[1], d[2]);
+                    t_max = states[ray].t_max;
+                    answered = false;
+                    subs = iters = 0;
+                    phase = SETUP;
+                }
+            }
+        }
+        if (__all_sync(FULL, phase == DONE))
             break;
-        unsigned long long item = base + lane;
-        bool active = item < count;
-        unsigned act = __ballot_sync(FULL, active);
-        if (active)
-            leaf_job<ST, R, H, Fp>(tris64, assets, rays, opt, hits, stats, states, q_leaf[item], round, q_out, ctr,
-                                   act);
+        const TriDev &T = tris64[tri];
+        const AssetDev &g = assets[T.asset];
+        // leaf q of the job: the texel's corners, its normal form, the ray's plane basis (:239-264)
+        if (phase == SETUP) {
+            li = q_leaf[item].i[q];
+            lj = q_leaf[item].j[q];
+            L.w = cell_width(g, 0);
+            L.lo = {li * L.w, lj * L.w};
+            L.h00 = grid_h(g, L.lo.x, L.lo.y);
+            L.h10 = grid_h(g, L.lo.x + L.w, L.lo.y);
+            L.h01 = grid_h(g, L.lo.x, L.lo.y + L.w);
+            L.h11 = grid_h(g, L.lo.x + L.w, L.lo.y + L.w);
+            v2 c = add2(L.lo, V2(0.5 * L.w, 0.5 * L.w));
+            double hw = 0.5 * L.w;
+            L.N_hat = AF3(add3(add3(L3(T.m0), mul3(c.x, L3(T.Mu))), mul3(c.y, L3(T.Mv))), mul3(hw, L3(T.Mu)),
+                          mul3(hw, L3(T.Mv)));
+            normalize(L.N_hat);
+            L.o = O;
+            L.d_len = norm3(D);
+            L.dn = div3(D, L.d_len);
+            plane_basis(L.dn, L.d1, L.d2);
+            sp = 0;
+            stack[sp++] = {0.5, 0.5, -INFINITY, 0};
+            first = true;
+            phase = SEARCH;
+        }
+        // the next live entry of the search (a pop is a call of search_leaf;
+        // an entry at or beyond t_max is the sorted loop's break)
+        bool expand = false, newton = false;
+        leafent e = {0.0, 0.0, 0.0, 0};
+        if (phase == SEARCH) {
+            while (sp > 0) {
+                e = stack[--sp];
+                if (first || e.t_lo < t_max) {
+                    first = false;
+                    newton = e.depth == kDepth;
+                    expand = !newton;
+                    break;
+                }
+            }
+            if (!expand && !newton) {
+                // the leaf is done; the next of the job, or the job is done
+                if (++q < n_leaves && !answered) {
+                    phase = SETUP;
+                } else {
+                    if (ST) {
+                        stats[DMAP_ST_N * (int64_t)ray + DMAP_ST_SUB] += subs;
+                        stats[DMAP_ST_N * (int64_t)ray + DMAP_ST_NEWTON] += iters;
+                    }
+                    if (!answered) {
+                        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 3), 1ull);
+                        q_out[slot] = ray;
+                    }
+                    phase = NEED;
+                }
+            }
+        }
+        __syncwarp();
+        if (expand) {
+            double r = 0.5 * ldexp(0.5, -e.depth);
+            leafent ch[4];
+            int n = 0;
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) {
+                double ca = e.a + ((k & 1) ? r : -r), cb = e.b + ((k & 2) ? r : -r), t_lo;
+                ++subs;
+                if (sub_square_bound(T, L, ca, cb, r, t_min, t_max, t_lo))
+                    ch[n++] = {ca, cb, t_lo, e.depth + 1};
+            }
+            for (int p = 1; p < n; ++p)
+                for (int k = p; k > 0 && ch[k].t_lo < ch[k - 1].t_lo; --k) {
+                    leafent x = ch[k];
+                    ch[k] = ch[k - 1];
+                    ch[k - 1] = x;
+                }
+            for (int k = n - 1; k >= 0; --k)
+                stack[sp++] = ch[k];
+        }
+        __syncwarp();
+        if (newton) {
+            hit64 h;
+            if (newton_from(T, g, O, D, t_min, t_max, li, lj, add2(L.lo, mul2(L.w, V2(e.a, e.b))), h, iters)) {
+                // a nearer root of this leaf (each later one is nearer still)
+                t_max = h.t;
+                RayState &s = states[ray];
+                s.t_max = h.t;
+                s.best_tri = tri;
+                s.flags |= kFoundInTri;
+                s.nah = s.lah = 0;
+                store_hit<H, Fp>(hits, ray, true, h, tri, DMAP_HIT_FP64_LEAF);
+                if (opt.mode == 1) { // occlusion: any hit answers the query
+                    answered = true;
+                    sp = 0;
+                }
+            }
+        }
         __syncwarp();
     }
 }
