@@ -60,6 +60,28 @@ class _Options(C.Structure):
                 ("blocks_per_sm", C.c_int)]
 
 
+class _Camera(C.Structure):
+    _fields_ = [("eye", C.c_double * 3), ("target", C.c_double * 3), ("up", C.c_double * 3), ("fov_deg", C.c_double),
+                ("width", C.c_int), ("height", C.c_int)]
+
+
+class _RenderDesc(C.Structure):
+    _fields_ = [("camera", _Camera), ("emitter_p0", C.c_double * 3), ("emitter_e1", C.c_double * 3),
+                ("emitter_e2", C.c_double * 3), ("radiance", C.c_double * 3), ("albedo", C.c_double * 3),
+                ("spp", C.c_int), ("max_depth", C.c_int), ("rr_depth", C.c_int), ("seed", C.c_uint64),
+                ("paths_per_batch", C.c_int64), ("use_graph", C.c_int)]
+
+
+class _RenderStats(C.Structure):
+    _fields_ = [("paths", C.c_int64), ("extension_rays", C.c_int64), ("shadow_rays", C.c_int64),
+                ("batches", C.c_int64), ("kernel_launches", C.c_int64), ("device_ms", C.c_double)]
+
+
+class _RayRecord(C.Structure):
+    _fields_ = [("capacity", C.c_int64), ("rays", C.c_void_p), ("kind", C.c_void_p), ("tri", C.c_void_p),
+                ("t", C.c_void_p), ("count", C.c_int64)]
+
+
 _lib = None
 
 
@@ -89,6 +111,8 @@ def lib() -> C.CDLL:
             "dmap_scene_triangle_info": (i32, [vp, i32, vp]),
             "dmap_intersect": (i32, [vp, vp, i32, i64, C.POINTER(_Options), vp, i32, vp, vp]),
             "dmap_intersect_host": (i32, [vp, vp, i32, i64, C.POINTER(_Options), vp, i32, vp]),
+            "dmap_render": (i32, [vp, C.POINTER(_RenderDesc), C.POINTER(_Options), vp, C.POINTER(_RenderStats),
+                                  C.POINTER(_RayRecord)]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -257,6 +281,37 @@ class Scene:
         opt = (options or TraversalOptions()).c()
         self.ctx.check(lib().dmap_intersect(self.h, rays_ptr, ray_dtype, n, C.byref(opt), hits_ptr, hit_dtype,
                                             stats_ptr or None, stream or None), "dmap_intersect")
+
+    def render(self, view: dict, emitter: np.ndarray, spp: int = 1, max_depth: int = 5, rr_depth: int = 3,
+               radiance=(10.0, 10.0, 10.0), albedo=(0.7, 0.7, 0.7), seed: int = 2027, paths_per_batch: int = 0,
+               use_graph: bool = True, options: Optional[TraversalOptions] = None, record: int = 0):
+        """The batched path tracer (dmap_render): view as scenes.path_tracer_view,
+        emitter as the (4, 3) corners p00, p10, p01, p11 of the light rectangle.
+        Returns (image (h, w, 3) float32, stats dict, record dict or None)."""
+        cam = _Camera((C.c_double * 3)(*view["eye"]), (C.c_double * 3)(*view["target"]),
+                      (C.c_double * 3)(*view["up"]), view["fov_deg"], view["width"], view["height"])
+        e = np.asarray(emitter, np.float64)
+        d = _RenderDesc(cam, (C.c_double * 3)(*e[0]), (C.c_double * 3)(*(e[1] - e[0])),
+                        (C.c_double * 3)(*(e[2] - e[0])), (C.c_double * 3)(*radiance), (C.c_double * 3)(*albedo),
+                        spp, max_depth, rr_depth, seed, paths_per_batch, int(use_graph))
+        img = np.empty((view["height"], view["width"], 3), np.float32)
+        st = _RenderStats()
+        rec = None
+        rp = None
+        if record > 0:
+            rec = {"rays": np.zeros((record, 8), np.float32), "kind": np.zeros(record, np.int32),
+                   "tri": np.zeros(record, np.int32), "t": np.zeros(record, np.float32)}
+            rp = _RayRecord(record, rec["rays"].ctypes.data, rec["kind"].ctypes.data, rec["tri"].ctypes.data,
+                            rec["t"].ctypes.data, 0)
+        opt = (options or TraversalOptions()).c()
+        self.ctx.check(lib().dmap_render(self.h, C.byref(d), C.byref(opt), img.ctypes.data, C.byref(st),
+                                         C.byref(rp) if rp is not None else None), "dmap_render")
+        if rec is not None:
+            m = min(rp.count, record)
+            rec = {k: v[:m] for k, v in rec.items()}
+            rec["count"] = rp.count
+        stats = {k: getattr(st, k) for k, _ in _RenderStats._fields_}
+        return img, stats, rec
 
     def close(self):
         if getattr(self, "h", None):

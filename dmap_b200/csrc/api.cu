@@ -2,142 +2,9 @@
 // pyramid), scenes (per-triangle setup) and the query entry points. Host
 // C++ over the CUDA runtime; kernels live in pyramid.cu, setup.cu,
 // walk64.cu and walk32.cu.
-#include "dmap_b200.h"
+#include "api_internal.h"
 
-#include "device_types.cuh"
-#include "launch.h"
-
-#include <cuda.h>
-#include <cuda_fp16.h>
-#include <cuda_runtime.h>
-
-#include <atomic>
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <mutex>
-#include <string>
-#include <vector>
-
-using dmapdev::AssetDev;
-using dmapdev::TriDev;
-using dmapdev::TriDev32;
-
-static_assert(sizeof(dmap_hit32) == sizeof(dmapdev::Hit32), "hit32 layout");
-static_assert(sizeof(dmap_hit64) == sizeof(dmapdev::Hit64), "hit64 layout");
-static_assert(DMAP_ST_COUNT == DMAP_ST_N, "stats layout");
-
-struct dmap_context
-{
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    unsigned *status_dev = nullptr; // device status word
-    dmapk::WaveScratch wave; // the wavefront schedule's scratch, grown to the largest batch
-    std::atomic<int64_t> launches{0};
-    std::string error;
-    // device staging for dmap_intersect_host
-    void *rays_dev = nullptr, *hits_dev = nullptr;
-    int64_t *stats_dev = nullptr;
-    size_t rays_cap = 0, hits_cap = 0, stats_cap = 0;
-};
-
-struct dmap_asset
-{
-    dmap_context *ctx = nullptr;
-    AssetDev dev{};
-    void *nodes = nullptr;
-    double *pyr64 = nullptr;
-    float *pyr32 = nullptr;
-    size_t bytes = 0;
-    int64_t cells = 0;
-};
-
-struct dmap_scene
-{
-    dmap_context *ctx = nullptr;
-    int n_tri = 0;
-    std::vector<dmap_asset *> assets;
-    AssetDev *assets_dev = nullptr;
-    TriDev *tris_dev = nullptr;
-    TriDev32 *tris32_dev = nullptr;
-    std::vector<TriDev> tris_host;
-    bool all_f64 = true;
-};
-
-namespace
-{
-
-dmap_status fail(dmap_context *ctx, dmap_status s, const std::string &msg)
-{
-    if (ctx)
-        ctx->error = msg;
-    return s;
-}
-
-dmap_status cuda_fail(dmap_context *ctx, cudaError_t e, const char *what)
-{
-    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
-    if (e == cudaErrorMemoryAllocation)
-        return fail(ctx, DMAP_ERR_OOM, msg);
-    return fail(ctx, DMAP_ERR_CUDA, msg);
-}
-
-#define DMAP_CUDA(ctx, call)                                                                                         \
-    do {                                                                                                              \
-        cudaError_t e_ = (call);                                                                                      \
-        if (e_ != cudaSuccess)                                                                                        \
-            return cuda_fail(ctx, e_, #call);                                                                         \
-    } while (0)
-
-size_t dtype_size(dmap_dtype t) { return t == DMAP_F64 ? 8 : t == DMAP_F16 ? 2 : 4; }
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled()
-{
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
-}
-
-dmap_status sync_and_check(dmap_context *ctx, const char *what)
-{
-    DMAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    unsigned st = 0;
-    DMAP_CUDA(ctx, cudaMemcpy(&st, ctx->status_dev, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (st) {
-        DMAP_CUDA(ctx, cudaMemset(ctx->status_dev, 0, sizeof(unsigned)));
-        if (st & dmapdev::kStatusBadInput)
-            return fail(ctx, DMAP_ERR_DEGENERATE, std::string(what) + ": degenerate input");
-        return fail(ctx, DMAP_ERR_LIMIT, std::string(what) + ": a device iteration cap ran out");
-    }
-    return DMAP_OK;
-}
-
-template <typename T>
-dmap_status grow(dmap_context *ctx, T **p, size_t *cap, size_t bytes)
-{
-    if (*cap >= bytes)
-        return DMAP_OK;
-    if (*p)
-        cudaFree(*p);
-    *p = nullptr;
-    *cap = 0;
-    DMAP_CUDA(ctx, cudaMalloc((void **)p, bytes));
-    *cap = bytes;
-    return DMAP_OK;
-}
-
-} // namespace
+using namespace dmapi;
 
 extern "C" {
 
@@ -188,11 +55,7 @@ void dmap_destroy(dmap_context *ctx)
     cudaFree(ctx->hits_dev);
     cudaFree(ctx->stats_dev);
     cudaFree(ctx->status_dev);
-    cudaFree(ctx->wave.state);
-    cudaFree(ctx->wave.queue[0]);
-    cudaFree(ctx->wave.queue[1]);
-    cudaFree(ctx->wave.leaves);
-    cudaFree(ctx->wave.counters);
+    wave_release(ctx->wave);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -459,7 +322,9 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *s, int tri, double *out)
 
 // ---- queries ---------------------------------------------------------------
 
-static dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, const dmap_options *opt,
+} // extern "C"
+
+dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, const dmap_options *opt,
                                dmap_dtype hit_dtype, dmapk::QueryOpts &q)
 {
     dmap_options o;
@@ -493,6 +358,8 @@ static dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     return DMAP_OK;
 }
 
+extern "C" {
+
 static dmap_status run_query(dmap_scene *s, const void *rays, int64_t n, const dmapk::QueryOpts &q, void *hits,
                              int64_t *stats, cudaStream_t stream)
 {
@@ -503,24 +370,12 @@ static dmap_status run_query(dmap_scene *s, const void *rays, int64_t n, const d
                                  stream);
     } else {
         if (q.schedule == DMAP_SCHEDULE_WAVEFRONT && n > ctx->wave.capacity) {
-            // grow the wavefront scratch to this batch (the previous one is idle:
-            // calls on a context are serialized)
-            dmapk::WaveScratch &w = ctx->wave;
+            // grow the wavefront scratch to this batch (the previous one is idle
+            // once the stream drains: calls on a context are serialized)
             DMAP_CUDA(ctx, cudaStreamSynchronize(stream));
-            cudaFree(w.state);
-            cudaFree(w.queue[0]);
-            cudaFree(w.queue[1]);
-            cudaFree(w.leaves);
-            cudaFree(w.counters);
-            w = dmapk::WaveScratch{};
-            if ((e = cudaMalloc(&w.state, dmapk::wave_state_bytes() * n)) != cudaSuccess ||
-                (e = cudaMalloc((void **)&w.queue[0], sizeof(int) * n)) != cudaSuccess ||
-                (e = cudaMalloc((void **)&w.queue[1], sizeof(int) * n)) != cudaSuccess ||
-                (e = cudaMalloc(&w.leaves, dmapk::wave_leaf_bytes() * n)) != cudaSuccess ||
-                (e = cudaMalloc((void **)&w.counters, sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1))) !=
-                    cudaSuccess)
-                return cuda_fail(ctx, e, "dmap_intersect: wavefront scratch");
-            w.capacity = n;
+            dmap_status ws = wave_reserve(ctx, ctx->wave, n);
+            if (ws != DMAP_OK)
+                return ws;
         }
         e = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, rays, n, q, hits, stats,
                                  ctx->status_dev, ctx->wave, stream);

@@ -1,0 +1,183 @@
+// Internal to the library: the handle structs behind the C ABI's opaque
+// types and the error helpers shared by the translation units of the host
+// side (api.cu, render.cu, server.cu).
+#pragma once
+#include "dmap_b200.h"
+
+#include "device_types.cuh"
+#include "launch.h"
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using dmapdev::AssetDev;
+using dmapdev::TriDev;
+using dmapdev::TriDev32;
+
+static_assert(sizeof(dmap_hit32) == sizeof(dmapdev::Hit32), "hit32 layout");
+static_assert(sizeof(dmap_hit64) == sizeof(dmapdev::Hit64), "hit64 layout");
+static_assert(DMAP_ST_COUNT == DMAP_ST_N, "stats layout");
+
+struct dmap_context
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    unsigned *status_dev = nullptr; // device status word
+    dmapk::WaveScratch wave; // the wavefront schedule's scratch, grown to the largest batch
+    std::atomic<int64_t> launches{0};
+    std::string error;
+    // device staging for dmap_intersect_host
+    void *rays_dev = nullptr, *hits_dev = nullptr;
+    int64_t *stats_dev = nullptr;
+    size_t rays_cap = 0, hits_cap = 0, stats_cap = 0;
+};
+
+struct dmap_asset
+{
+    dmap_context *ctx = nullptr;
+    AssetDev dev{};
+    void *nodes = nullptr;
+    double *pyr64 = nullptr;
+    float *pyr32 = nullptr;
+    size_t bytes = 0;
+    int64_t cells = 0;
+};
+
+struct dmap_scene
+{
+    dmap_context *ctx = nullptr;
+    int n_tri = 0;
+    std::vector<dmap_asset *> assets;
+    AssetDev *assets_dev = nullptr;
+    TriDev *tris_dev = nullptr;
+    TriDev32 *tris32_dev = nullptr;
+    std::vector<TriDev> tris_host;
+    bool all_f64 = true;
+};
+
+namespace dmapi
+{
+
+inline dmap_status fail(dmap_context *ctx, dmap_status s, const std::string &msg)
+{
+    if (ctx)
+        ctx->error = msg;
+    return s;
+}
+
+inline dmap_status cuda_fail(dmap_context *ctx, cudaError_t e, const char *what)
+{
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation)
+        return fail(ctx, DMAP_ERR_OOM, msg);
+    return fail(ctx, DMAP_ERR_CUDA, msg);
+}
+
+#define DMAP_CUDA(ctx, call)                                                                                         \
+    do {                                                                                                              \
+        cudaError_t e_ = (call);                                                                                      \
+        if (e_ != cudaSuccess)                                                                                        \
+            return cuda_fail(ctx, e_, #call);                                                                         \
+    } while (0)
+
+inline size_t dtype_size(dmap_dtype t) { return t == DMAP_F64 ? 8 : t == DMAP_F16 ? 2 : 4; }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+inline EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+inline dmap_status sync_and_check(dmap_context *ctx, const char *what)
+{
+    DMAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned st = 0;
+    DMAP_CUDA(ctx, cudaMemcpy(&st, ctx->status_dev, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st) {
+        DMAP_CUDA(ctx, cudaMemset(ctx->status_dev, 0, sizeof(unsigned)));
+        if (st & dmapdev::kStatusBadInput)
+            return fail(ctx, DMAP_ERR_DEGENERATE, std::string(what) + ": degenerate input");
+        return fail(ctx, DMAP_ERR_LIMIT, std::string(what) + ": a device iteration cap ran out");
+    }
+    return DMAP_OK;
+}
+
+template <typename T>
+dmap_status grow(dmap_context *ctx, T **p, size_t *cap, size_t bytes)
+{
+    if (*cap >= bytes)
+        return DMAP_OK;
+    if (*p)
+        cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    DMAP_CUDA(ctx, cudaMalloc((void **)p, bytes));
+    *cap = bytes;
+    return DMAP_OK;
+}
+
+inline void wave_release(dmapk::WaveScratch &w)
+{
+    cudaFree(w.state);
+    cudaFree(w.queue[0]);
+    cudaFree(w.queue[1]);
+    cudaFree(w.leaves);
+    cudaFree(w.counters);
+    w = dmapk::WaveScratch{};
+}
+
+// Grows a wavefront scratch to n rays. The caller makes sure that no kernel
+// using the old one is in flight.
+inline dmap_status wave_reserve(dmap_context *ctx, dmapk::WaveScratch &w, int64_t n)
+{
+    if (n <= w.capacity)
+        return DMAP_OK;
+    wave_release(w);
+    cudaError_t e;
+    if ((e = cudaMalloc(&w.state, dmapk::wave_state_bytes() * n)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&w.queue[0], sizeof(int) * n)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&w.queue[1], sizeof(int) * n)) != cudaSuccess ||
+        (e = cudaMalloc(&w.leaves, dmapk::wave_leaf_bytes() * n)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&w.counters, sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1))) !=
+            cudaSuccess) {
+        wave_release(w);
+        return cuda_fail(ctx, e, "wavefront scratch");
+    }
+    w.capacity = n;
+    return DMAP_OK;
+}
+
+// Device bytes of a wavefront scratch for n rays.
+inline size_t wave_bytes(int64_t n)
+{
+    return (dmapk::wave_state_bytes() + 2 * sizeof(int) + dmapk::wave_leaf_bytes()) * (size_t)n +
+           sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1);
+}
+
+// Validates dmap_options into the kernels' QueryOpts (api.cu).
+dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, const dmap_options *opt,
+                        dmap_dtype hit_dtype, dmapk::QueryOpts &q);
+
+} // namespace dmapi
+

@@ -18,6 +18,10 @@ struct QueryOpts
     int schedule;             // DMAP_SCHEDULE_*
     int rounds;               // wavefront: walk/leaf rounds before the inline-leaf drain
     int blocks_per_sm;        // wavefront walk: resident 128-thread CTAs per SM
+    // When set, the number of rays is read here on the device when the query
+    // runs (at most the n the launch is given, which sizes grids and scratch):
+    // stages of a device-driven pipeline pass counts they produced themselves.
+    const long long *n_dev = nullptr;
 };
 
 constexpr int kMaxRounds = 32;

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
                                                      int64_t *__restrict__ stats, unsigned *status)
 {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n)
+    if (k >= n || (opt.n_dev && k >= *opt.n_dev))
         return;
     double o[3], d[3], t_min, t_max;
     load_ray(rays, k, o, d, t_min, t_max);
@@ -271,7 +271,9 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     const int lane = threadIdx.x & 31;
     const bool use_mask = n_tri <= 32 * kMaskWords;
     // items of this round: every ray in round 0, else the resume queue
-    const unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
+    unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
+    if (round == 0 && opt.n_dev && (unsigned long long)*opt.n_dev < count)
+        count = *opt.n_dev < 0 ? 0ull : (unsigned long long)*opt.n_dev;
     unsigned long long *fetch = round_ctr(ctr, round, 0);
     int phase = NEED;
     int ray = 0;

@@ -207,7 +207,11 @@ def path_tracer_scene(n_sphere: int = 2048, n_ground: int = 4096, k: int = 4, se
     """The cube sphere plus a displaced ground plane (4 x 4 units at
     y = -1.3, normal +y, 2 triangles) and a 0.5 x 0.5 emitter rectangle
     above the sphere."""
-    sc = cube_sphere_scene(n_sphere, k, seed, dtype=dtype)
+    return with_ground_and_emitter(cube_sphere_scene(n_sphere, k, seed, dtype=dtype), n_ground, seed, dtype)
+
+
+def with_ground_and_emitter(sc: Scene, n_ground: int = 4096, seed: int = SEED, dtype=np.float32) -> Scene:
+    """A scene plus the path tracer's ground plane and emitter."""
     g = ground_plane_asset(n_ground, seed + 1000, dtype=dtype)
     y = -1.3
     up = np.array([0.0, 1.0, 0.0])
@@ -219,6 +223,13 @@ def path_tracer_scene(n_sphere: int = 2048, n_ground: int = 4096, k: int = 4, se
     tri_asset = np.concatenate([sc.tri_asset, np.full(2, len(assets) - 1, np.int32)])
     emitter = np.array([[-0.25, 2.0, -0.25], [0.25, 2.0, -0.25], [-0.25, 2.0, 0.25], [0.25, 2.0, 0.25]])
     return Scene(assets, tris, tri_asset, name="path_tracer", emitter=emitter, extent=float(np.linalg.norm([4, 3.5, 4])))
+
+
+def path_tracer_view(width: int = 1280, height: int = 720) -> dict:
+    """The path tracer's camera: in front of the sphere, slightly above it,
+    the ground plane and the emitter's light pool in view."""
+    return dict(eye=(0.0, 1.0, 4.6), target=(0.0, -0.3, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0,
+                width=width, height=height)
 
 
 # --------------------------------------------------------------------------

@@ -208,6 +208,76 @@ dmap_status dmap_intersect(dmap_scene *scene, const void *rays_dev, dmap_dtype r
 dmap_status dmap_intersect_host(dmap_scene *scene, const void *rays_host, dmap_dtype ray_dtype, int64_t n,
                                 const dmap_options *opt, void *hits_host, dmap_dtype hit_dtype, int64_t *stats_host);
 
+/* ---- batched path tracer ------------------------------------------------- */
+
+/*
+ * A wavefront path tracer over a scene of displaced triangles lit by one
+ * rectangular area emitter, every ray query going through the FP32 query
+ * path above: per bounce, one closest-hit query for the extension rays and
+ * one occlusion query for the emitter-sampled shadow rays. It replaces, for
+ * diffuse scenes, the render loop that issues those queries through the
+ * embree callbacks: ks's SmallPT driven by path_trace_render
+ * (path_trace.cpp:98-124), next-event estimation in direct_lighting
+ * (direct_lighting.cpp:198-217: light sample, shadow ray shortened by
+ * shadow_eps = 1e-4, spawn_ray<NextBounce> offsets) and the occlusion query
+ * behind Scene::occlude1 (occluded_callback, displaced_geometry.cpp:78-106).
+ *
+ * Shading (ours; ks's SmallPT is not part of the reference sources): every
+ * displaced surface is Lambertian with `albedo`; the emitter is the one-sided
+ * rectangle p0 + a e1 + b e2 (a, b in [0, 1]) emitting `radiance` on the side
+ * of e1 x e2 and sampled uniformly by area; camera rays that see the emitter
+ * add its radiance, later bounces that reach it end (next-event estimation
+ * only); missed rays see black. Paths have at most `max_depth` vertices and
+ * Russian roulette from vertex `rr_depth` on. Sample-major path order: path
+ * g is pixel g % (width * height) of sample g / (width * height); the random
+ * numbers of a path are a hash of (seed, g, vertex, dimension), so an image
+ * is the same for any batching.
+ */
+typedef struct dmap_camera {
+    double eye[3], target[3], up[3];
+    double fov_deg; /* vertical field of view */
+    int width, height;
+} dmap_camera;
+
+typedef struct dmap_render_desc {
+    dmap_camera camera;
+    double emitter_p0[3], emitter_e1[3], emitter_e2[3], radiance[3];
+    double albedo[3];
+    int spp, max_depth, rr_depth;
+    uint64_t seed;
+    int64_t paths_per_batch; /* paths in flight per wave: whole samples of the image (0 = 4M) */
+    int use_graph;           /* capture one batch's stages in a CUDA graph and replay it per batch */
+} dmap_render_desc;
+
+typedef struct dmap_render_stats {
+    int64_t paths, extension_rays, shadow_rays; /* queries issued */
+    int64_t batches, kernel_launches;
+    double device_ms;                           /* CUDA-event time of the whole render */
+} dmap_render_stats;
+
+/*
+ * Optional record of every query the render issues, in issue order within a
+ * stage (for ray replay against a CPU intersector): rays as issued (8 floats:
+ * o, d, t_min, t_max), kind (0 extension / closest hit, 1 shadow / occlusion),
+ * and the answer: the hit triangle (-1 for a miss / not occluded) and, for
+ * extension rays, t. `count` returns the number of queries issued; at most
+ * `capacity` are written.
+ */
+typedef struct dmap_ray_record {
+    int64_t capacity;
+    float *rays;
+    int32_t *kind;
+    int32_t *tri;
+    float *t;
+    int64_t count;
+} dmap_ray_record;
+
+/* Renders into rgb_host (height x width x 3 floats, the mean over spp, rows
+ * top to bottom). opt: the query options (FP32 precision; NULL = defaults);
+ * stats and record may be NULL. Synchronous. */
+dmap_status dmap_render(dmap_scene *scene, const dmap_render_desc *desc, const dmap_options *opt, float *rgb_host,
+                        dmap_render_stats *stats, dmap_ray_record *record);
+
 #ifdef __cplusplus
 }
 #endif

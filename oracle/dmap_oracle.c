@@ -1321,7 +1321,7 @@ static int isect_intersect(const o_isect *X, v3 o, v3 d, double t_min, double t_
 
 typedef struct {
     double *values;
-    o_grid grid;
+    o_grid *grid; /* heap: the triangles' intersectors point at it while obj[] grows */
     o_pyramid *pyr;
     int n_tri, first_tri;
     o_tri *tris;
@@ -1342,6 +1342,7 @@ void o_scene_free(o_scene *s)
         return;
     for (int k = 0; k < s->n_obj; ++k) {
         free(s->obj[k].values);
+        free(s->obj[k].grid);
         o_pyramid_free(s->obj[k].pyr);
         free(s->obj[k].tris);
         free(s->obj[k].isects);
@@ -1361,15 +1362,17 @@ int o_scene_add_object(o_scene *s, const double *values, int W, double scale, do
     memset(O, 0, sizeof(*O));
     O->values = (double *)malloc((size_t)W * W * sizeof(double));
     memcpy(O->values, values, (size_t)W * W * sizeof(double));
-    O->grid.W = W;
-    O->grid.H = W;
-    O->grid.scale = scale;
-    O->grid.values = O->values;
-    O->grid.offset = offset;
-    O->grid.repeat = repeat;
+    O->grid = (o_grid *)calloc(1, sizeof(o_grid));
+    O->grid->W = W;
+    O->grid->H = W;
+    O->grid->scale = scale;
+    O->grid->values = O->values;
+    O->grid->offset = offset;
+    O->grid->repeat = repeat;
     O->pyr = o_pyramid_build(O->values, W, scale, offset, build);
     if (!O->pyr) {
         free(O->values);
+        free(O->grid);
         return -1;
     }
     O->n_tri = n_tri;
@@ -1380,6 +1383,7 @@ int o_scene_add_object(o_scene *s, const double *values, int W, double scale, do
         if (!tri_init(&O->tris[k], tris + 24 * (size_t)k)) {
             o_pyramid_free(O->pyr);
             free(O->values);
+            free(O->grid);
             free(O->tris);
             free(O->isects);
             return -1;
@@ -1387,7 +1391,7 @@ int o_scene_add_object(o_scene *s, const double *values, int W, double scale, do
     }
     for (int k = 0; k < n_tri; ++k) { /* displaced_intersector.cpp:666-679 */
         o_isect *X = &O->isects[k];
-        isect_init(X, &O->tris[k], O->pyr, &O->grid);
+        isect_init(X, &O->tris[k], O->pyr, O->grid);
         triangle_height_range(&O->tris[k], O->pyr, &X->h_min, &X->h_max);
         X->box = triangle_aabb(&O->tris[k], X->h_min, X->h_max);
     }
