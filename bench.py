@@ -246,7 +246,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
-    ap.add_argument("--config", default="sphere", choices=["sphere", "sphere16", "quad", "pathtrace"])
+    ap.add_argument("--config", default="sphere", choices=["sphere", "sphere16", "quad", "pathtrace", "serve"])
+    ap.add_argument("--requests", type=int, default=4096, help="serve: requests in the arrival trace")
+    ap.add_argument("--interarrival-ms", type=float, default=15.0, help="serve: mean Poisson inter-arrival time")
+    ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-request comparison")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
     ap.add_argument("--rounds", type=int, default=6)
@@ -274,6 +277,9 @@ def main():
 
     if args.config == "pathtrace":
         run_pathtrace(args, rank, world, local, dist)
+        return
+    if args.config == "serve":
+        run_serve(args, rank, world, local, dist)
         return
 
     t_setup = time.perf_counter()
@@ -477,6 +483,173 @@ def run_pathtrace(args, rank, world, local, dist):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def serve_trace(n_req: int, interarrival_ms: float, seed: int, small: bool):
+    """The arrival trace: Poisson arrivals, a seeded scene id and a ray
+    count log-uniform in [1K, 4M] (4x smaller bounds with --small); mix 60%
+    primary (scene 0, 1 or 2), 30% path-traced (scene 2, 4 spp, depth 3,
+    ray count = camera samples), 10% shadow-only (scene 2)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = np.cumsum(rng.exponential(interarrival_ms * 1e-3, n_req))
+    t -= t[0]
+    hi = 1 << 20 if small else 4 << 20
+    n = np.exp(rng.uniform(np.log(1024), np.log(hi), n_req)).astype(np.int64)
+    u = rng.random(n_req)
+    kind = np.where(u < 0.6, 0, np.where(u < 0.9, 1, 2))          # primary, path-traced, shadow
+    scene = np.where(kind == 0, rng.integers(0, 3, n_req), 2)
+    return [dict(t=float(t[k]), n=int(n[k]), kind=int(kind[k]), scene=int(scene[k]), seed=seed + k,
+                 off=float(rng.random())) for k in range(n_req)]
+
+
+def run_serve(args, rank, world, local, dist):
+    """Serving: resident scenes (the quad, the cube sphere, the cube sphere +
+    ground + emitter sharing the sphere's assets), an open-loop Poisson trace
+    of requests, served by dmap_server (continuous batching, HBM-budget
+    admission) and, on the same arrival times, by the plain path: each
+    request alone, in arrival order, one launch per query (the simple
+    one-thread-per-ray schedule through dmap_intersect_host / dmap_render)."""
+    import torch
+    import dmap_b200 as dm
+    t_setup = time.perf_counter()
+    small = args.small
+    sph, _ = build_scene("sphere", small)
+    quad = scenes.quad_scene(128 if small else 512)
+    ctx = dm.Context(local)
+    d_quad = dm.Scene.from_synthetic(ctx, quad)
+    sph_assets = [dm.Asset(ctx, a.nodes) for a in sph.assets]
+    d_sph = dm.Scene(ctx, sph_assets, sph.tris, sph.tri_asset)
+    pt = scenes.with_ground_and_emitter(sph, 512 if small else 4096)
+    ground = dm.Asset(ctx, pt.assets[-1].nodes)
+    d_pt = dm.Scene(ctx, sph_assets + [ground], pt.tris, pt.tri_asset)   # shares the sphere's pyramids
+    devs = [d_quad, d_sph, d_pt]
+    resident = sum(a.device_bytes for a in sph_assets + [ground]) + sum(a.device_bytes for a in d_quad.assets)
+    view = scenes.path_tracer_view(1280, 720)
+    # ray pools in pinned memory: camera rays per scene, shadow rays toward the emitter
+    side = 1024 if small else 2048
+    pools = [scenes.quad_camera_rays(side, side),
+             scenes.sphere_camera_rays(side * 5 // 4, side * 4 // 5 if small else 1638),
+             scenes.pinhole_rays(view["eye"], view["target"], view["up"], view["fov_deg"], side * 5 // 4,
+                                 side * 4 // 5 if small else 1638, jitter_seed=scenes.SEED + 3)]
+    h = d_pt.intersect(pools[2], dm.TraversalOptions(), np.float32)
+    hit = h["tri"] >= 0
+    x = pools[2][hit, 0:3] + h["t"][hit, None] * pools[2][hit, 3:6]
+    ng = h["ng"][hit]
+    ng = np.where((np.sum(ng * pools[2][hit, 3:6], 1) > 0)[:, None], -ng, ng)
+    rng = np.random.Generator(np.random.PCG64(scenes.SEED + 4))
+    e = pt.emitter
+    y = e[0] + rng.random((len(x), 1)) * (e[1] - e[0]) + rng.random((len(x), 1)) * (e[2] - e[0])
+    xo = x + 1e-4 * ng
+    w = y - xo
+    dist_ = np.linalg.norm(w, axis=1)
+    shadow = np.zeros((len(x), 8), np.float32)
+    shadow[:, 0:3], shadow[:, 3:6], shadow[:, 7] = xo, w / dist_[:, None], dist_ - 1e-4
+    pools.append(shadow)
+    pinned = [torch.from_numpy(np.ascontiguousarray(p)).pin_memory() for p in pools]
+    trace = serve_trace(args.requests, args.interarrival_ms, scenes.SEED + 99, small)
+    ring_n = (16 << 20) if not small else (4 << 20)
+    ring = torch.empty(ring_n * 48, dtype=torch.uint8).pin_memory().numpy().view(dm.HIT32)
+    setup_s = time.perf_counter() - t_setup
+
+    def request_rays(r):
+        pool = pinned[3] if r["kind"] == 2 else pinned[r["scene"]]
+        n = min(r["n"], len(pool))
+        lo = int(r["off"] * (len(pool) - n))
+        return pool.numpy()[lo:lo + n]
+
+    def request_view(r):
+        px = max(64, r["n"] // 4)
+        wdt = max(8, int(round(math.sqrt(px * 16 / 9))))
+        v = dict(view)
+        v["width"], v["height"] = wdt, max(8, px // wdt)
+        return v
+
+    rkw = dict(spp=4, max_depth=3, rr_depth=3)
+    opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm)
+    # warm-up: every path once
+    srv = dm.Server(ctx, hbm_budget_bytes=120 * 10 ** 9, slots=2, options=opt)
+    for k in range(args.warmup):
+        ids = [srv.submit_rays(devs[k % 3], pools[k % 3][:50000])[0],
+               srv.submit_render(d_pt, request_view({"n": 40000}), pt.emitter, seed=k, **rkw)[0]]
+        srv.drain()
+    srv.close()
+
+    # served
+    srv = dm.Server(ctx, hbm_budget_bytes=120 * 10 ** 9, slots=2, options=opt)
+    ring_at, outstanding = 0, []
+    t0 = time.perf_counter()
+    with Clocks(local) as clk:
+        for r in trace:
+            now = time.perf_counter() - t0
+            if r["t"] > now:
+                time.sleep(r["t"] - now)
+            if r["kind"] == 1:
+                srv.submit_render(d_pt, request_view(r), pt.emitter, seed=r["seed"], **rkw)
+                continue
+            rays = request_rays(r)
+            n = len(rays)
+            if ring_at + n > ring_n:
+                ring_at = 0
+            # back-pressure: the ring slice must be free
+            while outstanding and any(a < ring_at + n and ring_at < b for a, b, _ in outstanding):
+                a, b, rid = outstanding.pop(0)
+                srv.wait(rid)
+            rid, _ = srv.submit_rays(devs[r["scene"]] if r["kind"] == 0 else d_pt, rays,
+                                     "occluded" if r["kind"] == 2 else "closest", hits=ring[ring_at:ring_at + n])
+            outstanding.append((ring_at, ring_at + n, rid))
+            ring_at += n
+        srv.drain()
+        wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    served = {"mrays_s": st["rays"] / st["wall_s"] / 1e6, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+              "mean_ms": st["mean_ms"], "max_ms": st["max_ms"], "queries": st["rays"], "makespan_s": st["wall_s"],
+              "busy_s": st["busy_s"], "launches": st["launches"], "peak_device_bytes": st["peak_bytes"] + resident}
+
+    plain = None
+    if not args.no_plain:
+        popt = dm.TraversalOptions(schedule="simple")
+        lat, queries = [], 0
+        t0 = time.perf_counter()
+        for r in trace:
+            now = time.perf_counter() - t0
+            if r["t"] > now:
+                time.sleep(r["t"] - now)
+            if r["kind"] == 1:
+                _, rs, _ = d_pt.render(request_view(r), pt.emitter, seed=r["seed"], use_graph=False, options=popt,
+                                       **rkw)
+                queries += rs["extension_rays"] + rs["shadow_rays"]
+            else:
+                rays = request_rays(r)
+                d = devs[r["scene"]] if r["kind"] == 0 else d_pt
+                d.intersect(rays, dm.TraversalOptions(schedule="simple",
+                                                      mode="occluded" if r["kind"] == 2 else "closest"), np.float32)
+                queries += len(rays)
+            lat.append((time.perf_counter() - t0 - r["t"]) * 1e3)
+        mk = time.perf_counter() - t0
+        lat = np.sort(np.array(lat))
+        plain = {"mrays_s": queries / mk / 1e6, "p50_ms": float(np.percentile(lat, 50, method="inverted_cdf")),
+                 "p99_ms": float(np.percentile(lat, 99, method="inverted_cdf")), "mean_ms": float(lat.mean()),
+                 "makespan_s": mk, "queries": queries}
+    line = {"metric": METRIC, "value": served["mrays_s"], "unit": "Mrays/s", "n_gpus": world, "steps": 1,
+            "warmup": args.warmup, "ms_per_step": served["makespan_s"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"serving: {args.requests} Poisson requests (mean inter-arrival "
+                                   f"{args.interarrival_ms} ms), rays log-uniform in [1K, {'1M' if small else '4M'}], "
+                                   "60% primary / 30% path-traced (4 spp, depth 3) / 10% shadow-only, scenes: quad "
+                                   f"{128 if small else 512}^2, cube sphere 96 x {256 if small else 2048}^2, "
+                                   "cube sphere + ground + emitter (shared assets), 120 GB budget",
+                       "resident_scene_bytes": resident},
+            "served": served, "plain": plain,
+            "served_over_plain": (served["mrays_s"] / plain["mrays_s"]) if plain else None,
+            "e2e": {"value": served["mrays_s"], "unit": "Mrays/s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None, "note": "every request through the host API"},
+            "gpu_launches": served["launches"], "setup_s": setup_s}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

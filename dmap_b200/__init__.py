@@ -82,6 +82,19 @@ class _RayRecord(C.Structure):
                 ("t", C.c_void_p), ("count", C.c_int64)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch_rays", C.c_int64), ("max_inflight", C.c_int),
+                ("slots", C.c_int), ("options", _Options)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("cancelled", C.c_int64),
+                ("queued", C.c_int64), ("active", C.c_int64), ("rays", C.c_int64), ("launches", C.c_int64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+                ("held_bytes", C.c_size_t), ("peak_bytes", C.c_size_t), ("busy_s", C.c_double),
+                ("wall_s", C.c_double)]
+
+
 _lib = None
 
 
@@ -113,6 +126,16 @@ def lib() -> C.CDLL:
             "dmap_intersect_host": (i32, [vp, vp, i32, i64, C.POINTER(_Options), vp, i32, vp]),
             "dmap_render": (i32, [vp, C.POINTER(_RenderDesc), C.POINTER(_Options), vp, C.POINTER(_RenderStats),
                                   C.POINTER(_RayRecord)]),
+            "dmap_server_create": (i32, [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]),
+            "dmap_server_destroy": (None, [vp]),
+            "dmap_server_submit_rays": (i32, [vp, vp, vp, i64, i32, vp, C.POINTER(C.c_uint64)]),
+            "dmap_server_submit_render": (i32, [vp, vp, C.POINTER(_RenderDesc), vp, C.POINTER(C.c_uint64)]),
+            "dmap_server_poll": (i32, [vp, C.c_uint64]),
+            "dmap_server_wait": (i32, [vp, C.c_uint64, dbl]),
+            "dmap_server_cancel": (i32, [vp, C.c_uint64]),
+            "dmap_server_latency": (i32, [vp, C.c_uint64, C.POINTER(dbl)]),
+            "dmap_server_drain": (i32, [vp, dbl]),
+            "dmap_server_get_stats": (i32, [vp, C.POINTER(_ServerStats)]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -288,12 +311,7 @@ class Scene:
         """The batched path tracer (dmap_render): view as scenes.path_tracer_view,
         emitter as the (4, 3) corners p00, p10, p01, p11 of the light rectangle.
         Returns (image (h, w, 3) float32, stats dict, record dict or None)."""
-        cam = _Camera((C.c_double * 3)(*view["eye"]), (C.c_double * 3)(*view["target"]),
-                      (C.c_double * 3)(*view["up"]), view["fov_deg"], view["width"], view["height"])
-        e = np.asarray(emitter, np.float64)
-        d = _RenderDesc(cam, (C.c_double * 3)(*e[0]), (C.c_double * 3)(*(e[1] - e[0])),
-                        (C.c_double * 3)(*(e[2] - e[0])), (C.c_double * 3)(*radiance), (C.c_double * 3)(*albedo),
-                        spp, max_depth, rr_depth, seed, paths_per_batch, int(use_graph))
+        d = render_desc(view, emitter, spp, max_depth, rr_depth, radiance, albedo, seed, paths_per_batch, use_graph)
         img = np.empty((view["height"], view["width"], 3), np.float32)
         st = _RenderStats()
         rec = None
@@ -317,6 +335,102 @@ class Scene:
         if getattr(self, "h", None):
             lib().dmap_scene_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render_desc(view: dict, emitter: np.ndarray, spp: int = 1, max_depth: int = 5, rr_depth: int = 3,
+                radiance=(10.0, 10.0, 10.0), albedo=(0.7, 0.7, 0.7), seed: int = 2027, paths_per_batch: int = 0,
+                use_graph: bool = True) -> _RenderDesc:
+    """dmap_render_desc of a view (scenes.path_tracer_view) and the (4, 3)
+    corners p00, p10, p01, p11 of the emitter rectangle."""
+    cam = _Camera((C.c_double * 3)(*view["eye"]), (C.c_double * 3)(*view["target"]),
+                  (C.c_double * 3)(*view["up"]), view["fov_deg"], view["width"], view["height"])
+    e = np.asarray(emitter, np.float64)
+    return _RenderDesc(cam, (C.c_double * 3)(*e[0]), (C.c_double * 3)(*(e[1] - e[0])),
+                       (C.c_double * 3)(*(e[2] - e[0])), (C.c_double * 3)(*radiance), (C.c_double * 3)(*albedo),
+                       spp, max_depth, rr_depth, seed, paths_per_batch, int(use_graph))
+
+
+class Server:
+    """Continuous-batching server over resident scenes (dmap_server_*).
+    Submitted buffers are kept alive here until their request completes."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_batch_rays: int = 0, max_inflight: int = 0,
+                 slots: int = 0, options: Optional[TraversalOptions] = None):
+        self.ctx = ctx
+        cfg = _ServerConfig(hbm_budget_bytes, max_batch_rays, max_inflight, slots, (options or TraversalOptions()).c())
+        h = C.c_void_p()
+        ctx.check(lib().dmap_server_create(ctx.h, C.byref(cfg), C.byref(h)), "dmap_server_create")
+        self.h = h
+        self._bufs = {}
+
+    def submit_rays(self, scene: Scene, rays: np.ndarray, mode: str = "closest", hits: Optional[np.ndarray] = None):
+        """rays (n, 8) float32 (pinned or not) -> (request id, HIT32 array filled on completion)."""
+        r = np.ascontiguousarray(rays, np.float32)
+        out = np.empty(len(r), HIT32) if hits is None else hits
+        rid = C.c_uint64()
+        s = lib().dmap_server_submit_rays(self.h, scene.h, r.ctypes.data, len(r), MODE[mode], out.ctypes.data,
+                                          C.byref(rid))
+        if s:
+            raise DmapError(s, f"dmap_server_submit_rays: {lib().dmap_status_string(s).decode()}")
+        self._bufs[rid.value] = (r, out)
+        return rid.value, out
+
+    def submit_render(self, scene: Scene, view: dict, emitter: np.ndarray, **kw):
+        """A render request (render_desc's keywords) -> (request id, image filled on completion)."""
+        d = render_desc(view, emitter, **kw)
+        img = np.empty((view["height"], view["width"], 3), np.float32)
+        rid = C.c_uint64()
+        s = lib().dmap_server_submit_render(self.h, scene.h, C.byref(d), img.ctypes.data, C.byref(rid))
+        if s:
+            raise DmapError(s, f"dmap_server_submit_render: {lib().dmap_status_string(s).decode()}")
+        self._bufs[rid.value] = (img,)
+        if len(self._bufs) % 256 == 0:
+            self.reap()
+        return rid.value, img
+
+    def poll(self, rid: int) -> int:
+        return lib().dmap_server_poll(self.h, rid)
+
+    def wait(self, rid: int, timeout_s: float = -1.0) -> int:
+        return lib().dmap_server_wait(self.h, rid, timeout_s)
+
+    def cancel(self, rid: int) -> int:
+        return lib().dmap_server_cancel(self.h, rid)
+
+    def latency_ms(self, rid: int) -> float:
+        ms = C.c_double()
+        s = lib().dmap_server_latency(self.h, rid, C.byref(ms))
+        if s:
+            raise DmapError(s, f"dmap_server_latency: {lib().dmap_status_string(s).decode()}")
+        return ms.value
+
+    def drain(self, timeout_s: float = -1.0) -> int:
+        s = lib().dmap_server_drain(self.h, timeout_s)
+        if s == 0:
+            self._bufs.clear()   # every request is done with its buffers
+        return s
+
+    def reap(self):
+        """Drops the references to the buffers of finished requests."""
+        for rid in [r for r in self._bufs if lib().dmap_server_poll(self.h, r) != 7]:
+            del self._bufs[rid]
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        lib().dmap_server_get_stats(self.h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dmap_server_destroy(self.h)
+            self.h = None
+            self._bufs.clear()
 
     def __del__(self):
         try:

@@ -179,5 +179,23 @@ inline size_t wave_bytes(int64_t n)
 dmap_status check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, const dmap_options *opt,
                         dmap_dtype hit_dtype, dmapk::QueryOpts &q);
 
+// A path-tracer render as a resumable job (render.cu): begin allocates its
+// device buffers stream-ordered on `stream` and, with use_graph, captures
+// one batch's stages there; each enqueue_batch runs the next batch of whole
+// image samples on the stream given; end (once the job's work is done)
+// copies the image, the counts and the record out. dmap_render is begin,
+// every batch, end.
+struct RenderJob;
+size_t render_device_bytes(const dmap_render_desc *desc, int64_t record_capacity);
+dmap_status render_begin(dmap_scene *s, const dmap_render_desc *desc, const dmap_options *opt,
+                         const dmap_ray_record *record, cudaStream_t stream, RenderJob **out);
+int render_batches(const RenderJob *job);
+int render_enqueued(const RenderJob *job);
+size_t render_bytes(const RenderJob *job);
+cudaError_t render_enqueue_batch(RenderJob *job, cudaStream_t stream);
+dmap_status render_end(RenderJob *job, float *rgb_host, dmap_render_stats *stats, dmap_ray_record *record,
+                       double device_ms);
+void render_free(RenderJob *job, cudaStream_t stream); // stream-ordered free
+
 } // namespace dmapi
 

@@ -267,9 +267,25 @@ bool finite_n(const double *v, int n)
     return true;
 }
 
-// Device buffers of one render.
-struct RenderBufs
+} // namespace
+
+namespace dmapi
 {
+
+// One render in progress: its parameters, device buffers, the captured
+// batch graph and the count of batches enqueued.
+struct RenderJob
+{
+    dmap_context *ctx = nullptr;
+    dmap_scene *scene = nullptr;
+    dmapk::QueryOpts q{};
+    RenderDev R{};
+    int spp = 0, n_batches = 0, enqueued = 0;
+    bool use_graph = false;
+    long long P = 0, wh = 0, cap = 0;
+    int64_t launches_per_batch = 0;
+    size_t bytes = 0;
+    // device buffers
     float *ray[2] = {nullptr, nullptr};
     int *path[2] = {nullptr, nullptr};
     dmapdev::Hit32 *hit = nullptr, *shit = nullptr;
@@ -280,23 +296,98 @@ struct RenderBufs
     float *rec_rays = nullptr, *rec_t = nullptr;
     int *rec_kind = nullptr, *rec_tri = nullptr;
     dmapk::WaveScratch wave;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
 
-    ~RenderBufs()
+    // Device memory is stream-ordered (cudaMallocAsync on the stream begin
+    // was given, cudaFreeAsync here), so that jobs come and go while other
+    // streams' kernels run; the caller makes sure none of the job's work is
+    // still in flight.
+    void release(cudaStream_t stream)
     {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
         void *all[] = {ray[0], ray[1], path[0], path[1], hit, shit, beta, Lp, srays, scontrib, accum, spath,
-                       cnt, p0, totals, rec_n, rec_rays, rec_t, rec_kind, rec_tri};
+                       cnt, p0, totals, rec_n, rec_rays, rec_t, rec_kind, rec_tri,
+                       wave.state, wave.queue[0], wave.queue[1], wave.leaves, wave.counters};
         for (void *p : all)
-            cudaFree(p);
-        wave_release(wave);
+            if (p)
+                cudaFreeAsync(p, stream);
+        wave = dmapk::WaveScratch{};
+    }
+
+    // One batch's stages on `stream`.
+    cudaError_t enqueue_stages(cudaStream_t stream)
+    {
+        cudaError_t err;
+        int64_t lc = 0;
+        const unsigned g = (unsigned)((P + 255) / 256);
+        dmap_scene *s = scene;
+        if ((err = cudaMemsetAsync(cnt, 0, sizeof(long long) * 2 * kMaxDepth, stream)) != cudaSuccess)
+            return err;
+        camera_kernel<<<g, 256, 0, stream>>>(R, ray[0], path[0], beta, Lp, cnt);
+        ++lc;
+        for (int v = 0; v < R.max_depth; ++v) {
+            dmapk::QueryOpts qe = q, qs = q;
+            qe.mode = DMAP_MODE_CLOSEST;
+            qe.ray_dtype = qe.hit_dtype = 0;
+            qe.n_dev = cnt + v;
+            if ((err = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, ray[v & 1], P, qe,
+                                            hit, nullptr, ctx->status_dev, wave, stream)) != cudaSuccess)
+                return err;
+            lc += dmapk::walk32_launches(qe);
+            if (cap > 0) {
+                record_kernel<<<g, 256, 0, stream>>>(0, cnt + v, ray[v & 1], hit, rec_n, cap, rec_rays, rec_kind,
+                                                     rec_tri, rec_t);
+                ++lc;
+            }
+            shade_kernel<<<g, 256, 0, stream>>>(R, v, ray[v & 1], path[v & 1], hit, cnt, beta, Lp, ray[(v + 1) & 1],
+                                                path[(v + 1) & 1], srays, spath, scontrib);
+            ++lc;
+            qs.mode = DMAP_MODE_OCCLUDED;
+            qs.ray_dtype = qs.hit_dtype = 0;
+            qs.n_dev = cnt + R.max_depth + v;
+            if ((err = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, srays, P, qs, shit,
+                                            nullptr, ctx->status_dev, wave, stream)) != cudaSuccess)
+                return err;
+            lc += dmapk::walk32_launches(qs);
+            if (cap > 0) {
+                record_kernel<<<g, 256, 0, stream>>>(1, cnt + R.max_depth + v, srays, shit, rec_n, cap, rec_rays,
+                                                     rec_kind, rec_tri, rec_t);
+                ++lc;
+            }
+            shadow_kernel<<<g, 256, 0, stream>>>(R, v, cnt, shit, spath, scontrib, Lp);
+            ++lc;
+        }
+        resolve_kernel<<<(unsigned)((wh + 255) / 256), 256, 0, stream>>>(R, Lp, accum);
+        advance_kernel<<<1, 1, 0, stream>>>(R, cnt, p0, totals);
+        lc += 2;
+        launches_per_batch = lc;
+        return cudaGetLastError();
     }
 };
 
-} // namespace
-
-extern "C" dmap_status dmap_render(dmap_scene *s, const dmap_render_desc *desc, const dmap_options *opt,
-                                   float *rgb_host, dmap_render_stats *stats, dmap_ray_record *record)
+size_t render_device_bytes(const dmap_render_desc *desc, int64_t record_capacity)
 {
-    if (!s || !desc || !rgb_host)
+    const dmap_camera &C = desc->camera;
+    long long wh = (long long)C.width * C.height;
+    long long ppb = desc->paths_per_batch > 0 ? desc->paths_per_batch : (4ll << 20);
+    long long s_batch = std::max(1ll, std::min((long long)desc->spp, ppb / std::max(1ll, wh)));
+    long long P = s_batch * wh;
+    size_t per_path = 2 * (32 + 4) + 2 * sizeof(dmapdev::Hit32) + 12 + 12 + 32 + 12 + 4;
+    return (size_t)P * per_path + wave_bytes(P) + (size_t)wh * 12 +
+           (size_t)std::max<int64_t>(record_capacity, 0) * 44 + 4096;
+}
+
+dmap_status render_begin(dmap_scene *s, const dmap_render_desc *desc, const dmap_options *opt,
+                         const dmap_ray_record *record, cudaStream_t stream, RenderJob **out)
+{
+    *out = nullptr;
+    if (!s || !desc)
         return fail(s ? s->ctx : nullptr, DMAP_ERR_INVALID, "dmap_render: null argument");
     dmap_context *ctx = s->ctx;
     const dmap_render_desc &D = *desc;
@@ -358,181 +449,185 @@ extern "C" dmap_status dmap_render(dmap_scene *s, const dmap_render_desc *desc, 
     long long ppb = D.paths_per_batch > 0 ? D.paths_per_batch : (4ll << 20);
     R.s_batch = (int)std::max(1ll, std::min((long long)D.spp, ppb / wh));
     R.P = (long long)R.s_batch * wh;
-    const int n_batches = (D.spp + R.s_batch - 1) / R.s_batch;
-    const long long P = R.P;
-    const long long cap = record ? std::max<int64_t>(record->capacity, 0) : 0;
 
     DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
-    RenderBufs B;
-    cudaError_t e;
+    auto *J = new RenderJob;
+    J->ctx = ctx;
+    J->scene = s;
+    J->q = q;
+    J->spp = D.spp;
+    J->P = R.P;
+    J->wh = wh;
+    J->n_batches = (D.spp + R.s_batch - 1) / R.s_batch;
+    J->use_graph = D.use_graph != 0;
+    J->cap = record ? std::max<int64_t>(record->capacity, 0) : 0;
+    J->bytes = render_device_bytes(desc, J->cap);
+    const long long P = R.P, cap = J->cap;
+    cudaError_t e = cudaSuccess;
     auto alloc = [&](void **p, size_t bytes) {
         if (e == cudaSuccess)
-            e = cudaMalloc(p, bytes);
+            e = cudaMallocAsync(p, bytes, stream);
     };
-    e = cudaSuccess;
     for (int k = 0; k < 2; ++k) {
-        alloc((void **)&B.ray[k], sizeof(float) * 8 * P);
-        alloc((void **)&B.path[k], sizeof(int) * P);
+        alloc((void **)&J->ray[k], sizeof(float) * 8 * P);
+        alloc((void **)&J->path[k], sizeof(int) * P);
     }
-    alloc((void **)&B.hit, sizeof(dmapdev::Hit32) * P);
-    alloc((void **)&B.shit, sizeof(dmapdev::Hit32) * P);
-    alloc((void **)&B.beta, sizeof(float) * 3 * P);
-    alloc((void **)&B.Lp, sizeof(float) * 3 * P);
-    alloc((void **)&B.srays, sizeof(float) * 8 * P);
-    alloc((void **)&B.scontrib, sizeof(float) * 3 * P);
-    alloc((void **)&B.spath, sizeof(int) * P);
-    alloc((void **)&B.accum, sizeof(float) * 3 * wh);
-    alloc((void **)&B.cnt, sizeof(long long) * 2 * kMaxDepth);
-    alloc((void **)&B.p0, sizeof(long long));
-    alloc((void **)&B.totals, sizeof(unsigned long long) * 4);
+    alloc((void **)&J->hit, sizeof(dmapdev::Hit32) * P);
+    alloc((void **)&J->shit, sizeof(dmapdev::Hit32) * P);
+    alloc((void **)&J->beta, sizeof(float) * 3 * P);
+    alloc((void **)&J->Lp, sizeof(float) * 3 * P);
+    alloc((void **)&J->srays, sizeof(float) * 8 * P);
+    alloc((void **)&J->scontrib, sizeof(float) * 3 * P);
+    alloc((void **)&J->spath, sizeof(int) * P);
+    alloc((void **)&J->accum, sizeof(float) * 3 * wh);
+    alloc((void **)&J->cnt, sizeof(long long) * 2 * kMaxDepth);
+    alloc((void **)&J->p0, sizeof(long long));
+    alloc((void **)&J->totals, sizeof(unsigned long long) * 4);
     if (cap > 0) {
-        alloc((void **)&B.rec_n, sizeof(unsigned long long));
-        alloc((void **)&B.rec_rays, sizeof(float) * 8 * cap);
-        alloc((void **)&B.rec_t, sizeof(float) * cap);
-        alloc((void **)&B.rec_kind, sizeof(int) * cap);
-        alloc((void **)&B.rec_tri, sizeof(int) * cap);
+        alloc((void **)&J->rec_n, sizeof(unsigned long long));
+        alloc((void **)&J->rec_rays, sizeof(float) * 8 * cap);
+        alloc((void **)&J->rec_t, sizeof(float) * cap);
+        alloc((void **)&J->rec_kind, sizeof(int) * cap);
+        alloc((void **)&J->rec_tri, sizeof(int) * cap);
     }
-    if (e != cudaSuccess)
-        return cuda_fail(ctx, e, "dmap_render: cudaMalloc");
-    if ((st = wave_reserve(ctx, B.wave, P)) != DMAP_OK)
-        return st;
-    R.p0 = B.p0;
-    cudaStream_t stream = ctx->stream;
-    DMAP_CUDA(ctx, cudaMemsetAsync(B.p0, 0, sizeof(long long), stream));
-    DMAP_CUDA(ctx, cudaMemsetAsync(B.accum, 0, sizeof(float) * 3 * wh, stream));
-    DMAP_CUDA(ctx, cudaMemsetAsync(B.totals, 0, sizeof(unsigned long long) * 4, stream));
-    if (cap > 0)
-        DMAP_CUDA(ctx, cudaMemsetAsync(B.rec_n, 0, sizeof(unsigned long long), stream));
+    alloc(&J->wave.state, dmapk::wave_state_bytes() * P);
+    alloc((void **)&J->wave.queue[0], sizeof(int) * P);
+    alloc((void **)&J->wave.queue[1], sizeof(int) * P);
+    alloc(&J->wave.leaves, dmapk::wave_leaf_bytes() * P);
+    alloc((void **)&J->wave.counters, sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1));
+    J->wave.capacity = P;
+    if (e != cudaSuccess) {
+        J->release(stream);
+        delete J;
+        return cuda_fail(ctx, e, "dmap_render: cudaMallocAsync");
+    }
+    R.p0 = J->p0;
+    J->R = R;
+    if ((e = cudaMemsetAsync(J->p0, 0, sizeof(long long), stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(J->accum, 0, sizeof(float) * 3 * wh, stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(J->totals, 0, sizeof(unsigned long long) * 4, stream)) != cudaSuccess ||
+        (cap > 0 && (e = cudaMemsetAsync(J->rec_n, 0, sizeof(unsigned long long), stream)) != cudaSuccess)) {
+        J->release(stream);
+        delete J;
+        return cuda_fail(ctx, e, "dmap_render: clear");
+    }
+    if (J->use_graph) {
+        // capture one batch's stages once; each replay runs the next batch
+        cudaError_t eq = cudaSuccess;
+        if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed)) == cudaSuccess) {
+            eq = J->enqueue_stages(stream);
+            e = cudaStreamEndCapture(stream, &J->graph);
+        }
+        if (eq != cudaSuccess || e != cudaSuccess ||
+            (e = cudaGraphInstantiate(&J->exec, J->graph, 0)) != cudaSuccess) {
+            J->release(stream);
+            delete J;
+            return cuda_fail(ctx, eq != cudaSuccess ? eq : e, "dmap_render: graph capture");
+        }
+    } else {
+        J->launches_per_batch = 0;
+    }
+    *out = J;
+    return DMAP_OK;
+}
 
-    // one batch's stages
-    int64_t launches_per_batch = 0;
-    auto enqueue_batch = [&]() -> cudaError_t {
-        cudaError_t err;
-        int64_t lc = 0;
-        const unsigned g = (unsigned)((P + 255) / 256);
-        if ((err = cudaMemsetAsync(B.cnt, 0, sizeof(long long) * 2 * kMaxDepth, stream)) != cudaSuccess)
-            return err;
-        camera_kernel<<<g, 256, 0, stream>>>(R, B.ray[0], B.path[0], B.beta, B.Lp, B.cnt);
-        ++lc;
-        for (int v = 0; v < R.max_depth; ++v) {
-            dmapk::QueryOpts qe = q, qs = q;
-            qe.mode = DMAP_MODE_CLOSEST;
-            qe.ray_dtype = qe.hit_dtype = 0;
-            qe.n_dev = B.cnt + v;
-            if ((err = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, B.ray[v & 1], P, qe,
-                                            B.hit, nullptr, ctx->status_dev, B.wave, stream)) != cudaSuccess)
-                return err;
-            lc += dmapk::walk32_launches(qe);
-            if (cap > 0) {
-                record_kernel<<<g, 256, 0, stream>>>(0, B.cnt + v, B.ray[v & 1], B.hit, B.rec_n, cap, B.rec_rays,
-                                                     B.rec_kind, B.rec_tri, B.rec_t);
-                ++lc;
-            }
-            shade_kernel<<<g, 256, 0, stream>>>(R, v, B.ray[v & 1], B.path[v & 1], B.hit, B.cnt, B.beta, B.Lp,
-                                                B.ray[(v + 1) & 1], B.path[(v + 1) & 1], B.srays, B.spath,
-                                                B.scontrib);
-            ++lc;
-            qs.mode = DMAP_MODE_OCCLUDED;
-            qs.ray_dtype = qs.hit_dtype = 0;
-            qs.n_dev = B.cnt + R.max_depth + v;
-            if ((err = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, B.srays, P, qs,
-                                            B.shit, nullptr, ctx->status_dev, B.wave, stream)) != cudaSuccess)
-                return err;
-            lc += dmapk::walk32_launches(qs);
-            if (cap > 0) {
-                record_kernel<<<g, 256, 0, stream>>>(1, B.cnt + R.max_depth + v, B.srays, B.shit, B.rec_n, cap,
-                                                     B.rec_rays, B.rec_kind, B.rec_tri, B.rec_t);
-                ++lc;
-            }
-            shadow_kernel<<<g, 256, 0, stream>>>(R, v, B.cnt, B.shit, B.spath, B.scontrib, B.Lp);
-            ++lc;
-        }
-        resolve_kernel<<<(unsigned)((wh + 255) / 256), 256, 0, stream>>>(R, B.Lp, B.accum);
-        advance_kernel<<<1, 1, 0, stream>>>(R, B.cnt, B.p0, B.totals);
-        lc += 2;
-        launches_per_batch = lc;
-        return cudaGetLastError();
-    };
+int render_batches(const RenderJob *J) { return J->n_batches; }
+int render_enqueued(const RenderJob *J) { return J->enqueued; }
+size_t render_bytes(const RenderJob *J) { return J->bytes; }
 
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    auto cleanup = [&]() {
-        if (exec)
-            cudaGraphExecDestroy(exec);
-        if (graph)
-            cudaGraphDestroy(graph);
-        if (ev0)
-            cudaEventDestroy(ev0);
-        if (ev1)
-            cudaEventDestroy(ev1);
-    };
-    if ((e = cudaEventCreate(&ev0)) != cudaSuccess || (e = cudaEventCreate(&ev1)) != cudaSuccess) {
-        cleanup();
-        return cuda_fail(ctx, e, "dmap_render: events");
+cudaError_t render_enqueue_batch(RenderJob *J, cudaStream_t stream)
+{
+    if (J->enqueued >= J->n_batches)
+        return cudaSuccess;
+    cudaError_t e = J->use_graph ? cudaGraphLaunch(J->exec, stream) : J->enqueue_stages(stream);
+    if (e == cudaSuccess) {
+        ++J->enqueued;
+        J->ctx->launches += J->launches_per_batch;
     }
-    if (D.use_graph) {
-        if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
-            cleanup();
-            return cuda_fail(ctx, e, "dmap_render: begin capture");
-        }
-        cudaError_t eq = enqueue_batch();
-        e = cudaStreamEndCapture(stream, &graph);
-        if (eq != cudaSuccess || e != cudaSuccess) {
-            cleanup();
-            return cuda_fail(ctx, eq != cudaSuccess ? eq : e, "dmap_render: capture");
-        }
-        if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) {
-            cleanup();
-            return cuda_fail(ctx, e, "dmap_render: graph instantiate");
-        }
-    }
-    cudaEventRecord(ev0, stream);
-    for (int b = 0; b < n_batches; ++b) {
-        e = D.use_graph ? cudaGraphLaunch(exec, stream) : enqueue_batch();
-        if (e != cudaSuccess) {
-            cleanup();
-            return cuda_fail(ctx, e, "dmap_render: batch launch");
-        }
-    }
-    cudaEventRecord(ev1, stream);
-    ctx->launches += launches_per_batch * n_batches;
-    st = sync_and_check(ctx, "dmap_render");
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    cleanup();
-    if (st != DMAP_OK)
-        return st;
+    return e;
+}
 
-    std::vector<float> acc((size_t)3 * wh);
+dmap_status render_end(RenderJob *J, float *rgb_host, dmap_render_stats *stats, dmap_ray_record *record,
+                       double device_ms)
+{
+    dmap_context *ctx = J->ctx;
+    std::vector<float> acc((size_t)3 * J->wh);
     unsigned long long tot[4] = {0, 0, 0, 0};
-    DMAP_CUDA(ctx, cudaMemcpy(acc.data(), B.accum, sizeof(float) * 3 * wh, cudaMemcpyDeviceToHost));
-    DMAP_CUDA(ctx, cudaMemcpy(tot, B.totals, sizeof(tot), cudaMemcpyDeviceToHost));
-    const float inv_spp = 1.0f / (float)D.spp;
-    for (size_t k = 0; k < acc.size(); ++k)
-        rgb_host[k] = acc[k] * inv_spp;
+    DMAP_CUDA(ctx, cudaMemcpy(acc.data(), J->accum, sizeof(float) * 3 * J->wh, cudaMemcpyDeviceToHost));
+    DMAP_CUDA(ctx, cudaMemcpy(tot, J->totals, sizeof(tot), cudaMemcpyDeviceToHost));
+    const float inv_spp = 1.0f / (float)J->spp;
+    if (rgb_host)
+        for (size_t k = 0; k < acc.size(); ++k)
+            rgb_host[k] = acc[k] * inv_spp;
     if (stats) {
         stats->paths = (int64_t)tot[0];
         stats->extension_rays = (int64_t)tot[1];
         stats->shadow_rays = (int64_t)tot[2];
-        stats->batches = n_batches;
-        stats->kernel_launches = launches_per_batch * n_batches;
-        stats->device_ms = ms;
+        stats->batches = J->n_batches;
+        stats->kernel_launches = J->launches_per_batch * J->n_batches;
+        stats->device_ms = device_ms;
     }
     if (record) {
-        record->count = 0;
-        if (cap > 0) {
+        record->count = (int64_t)(tot[1] + tot[2]);
+        if (J->cap > 0) {
             unsigned long long rn = 0;
-            DMAP_CUDA(ctx, cudaMemcpy(&rn, B.rec_n, sizeof(rn), cudaMemcpyDeviceToHost));
+            DMAP_CUDA(ctx, cudaMemcpy(&rn, J->rec_n, sizeof(rn), cudaMemcpyDeviceToHost));
             record->count = (int64_t)rn;
-            size_t m = (size_t)std::min<long long>((long long)rn, cap);
-            DMAP_CUDA(ctx, cudaMemcpy(record->rays, B.rec_rays, sizeof(float) * 8 * m, cudaMemcpyDeviceToHost));
-            DMAP_CUDA(ctx, cudaMemcpy(record->kind, B.rec_kind, sizeof(int) * m, cudaMemcpyDeviceToHost));
-            DMAP_CUDA(ctx, cudaMemcpy(record->tri, B.rec_tri, sizeof(int) * m, cudaMemcpyDeviceToHost));
-            DMAP_CUDA(ctx, cudaMemcpy(record->t, B.rec_t, sizeof(float) * m, cudaMemcpyDeviceToHost));
-        } else {
-            record->count = (int64_t)(tot[1] + tot[2]);
+            size_t m = (size_t)std::min<long long>((long long)rn, J->cap);
+            DMAP_CUDA(ctx, cudaMemcpy(record->rays, J->rec_rays, sizeof(float) * 8 * m, cudaMemcpyDeviceToHost));
+            DMAP_CUDA(ctx, cudaMemcpy(record->kind, J->rec_kind, sizeof(int) * m, cudaMemcpyDeviceToHost));
+            DMAP_CUDA(ctx, cudaMemcpy(record->tri, J->rec_tri, sizeof(int) * m, cudaMemcpyDeviceToHost));
+            DMAP_CUDA(ctx, cudaMemcpy(record->t, J->rec_t, sizeof(float) * m, cudaMemcpyDeviceToHost));
         }
     }
     return DMAP_OK;
+}
+
+void render_free(RenderJob *J, cudaStream_t stream)
+{
+    J->release(stream);
+    delete J;
+}
+
+} // namespace dmapi
+
+extern "C" dmap_status dmap_render(dmap_scene *s, const dmap_render_desc *desc, const dmap_options *opt,
+                                   float *rgb_host, dmap_render_stats *stats, dmap_ray_record *record)
+{
+    if (!s || !desc || !rgb_host)
+        return fail(s ? s->ctx : nullptr, DMAP_ERR_INVALID, "dmap_render: null argument");
+    dmap_context *ctx = s->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    RenderJob *J = nullptr;
+    dmap_status st = render_begin(s, desc, opt, record, stream, &J);
+    if (st != DMAP_OK)
+        return st;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaError_t e;
+    if ((e = cudaEventCreate(&ev0)) != cudaSuccess || (e = cudaEventCreate(&ev1)) != cudaSuccess) {
+        render_free(J, stream);
+        return cuda_fail(ctx, e, "dmap_render: events");
+    }
+    cudaEventRecord(ev0, stream);
+    for (int b = 0; b < J->n_batches && e == cudaSuccess; ++b)
+        e = render_enqueue_batch(J, stream);
+    cudaEventRecord(ev1, stream);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(stream);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        render_free(J, stream);
+        return cuda_fail(ctx, e, "dmap_render: batch launch");
+    }
+    st = sync_and_check(ctx, "dmap_render");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (st == DMAP_OK)
+        st = render_end(J, rgb_host, stats, record, ms);
+    render_free(J, stream);
+    cudaStreamSynchronize(stream);
+    return st;
 }

@@ -278,6 +278,69 @@ typedef struct dmap_ray_record {
 dmap_status dmap_render(dmap_scene *scene, const dmap_render_desc *desc, const dmap_options *opt, float *rgb_host,
                         dmap_render_stats *stats, dmap_ray_record *record);
 
+/* ---- serving: continuous batching over resident scenes -------------------- */
+
+/*
+ * No counterpart in the reference, whose renderer runs one task at a time.
+ * A server owns a worker thread and `slots` launch slots (each a stream, a
+ * batch of device ray and hit buffers of max_batch_rays, and the wavefront
+ * scratch). Requests are queued on submit and admitted in arrival order
+ * while fewer than max_inflight are active and the device bytes the server
+ * holds (slots, render jobs, and the assets of every scene it has served)
+ * stay within hbm_budget_bytes. Admitted ray requests are cut into pieces
+ * and packed, with the pieces of every other admitted request of the same
+ * scene and mode, into one query per slot, so small requests share launches
+ * and a large one does not hold back the rest; render requests run one batch
+ * of image samples per slot turn. While one slot's launch runs the worker
+ * fills the next, so requests that arrive mid-launch join the next launch.
+ * Each result equals the one the request would get alone (a ray's answer
+ * does not depend on the rays it shares a launch with; a render's image
+ * does not depend on its batching). Latency is submit to completion.
+ */
+typedef struct dmap_server_config {
+    size_t hbm_budget_bytes; /* device bytes the server may hold, scene assets included (0 = no limit) */
+    int64_t max_batch_rays;  /* rays per launch (0 = 4M) */
+    int max_inflight;        /* admitted requests at once (0 = 256) */
+    int slots;               /* launch slots in flight (0 = 2) */
+    dmap_options options;    /* query options of every request (FP32 path) */
+} dmap_server_config;
+
+typedef struct dmap_server_stats {
+    int64_t submitted, completed, failed, cancelled, queued, active;
+    int64_t rays;              /* rays answered (render queries included) */
+    int64_t launches;          /* slot launches (queries or render batches) */
+    double p50_ms, p99_ms, mean_ms, max_ms; /* latency of completed requests */
+    size_t held_bytes, peak_bytes;
+    double busy_s, wall_s;     /* time with a launch in flight; since the first submit */
+} dmap_server_stats;
+
+dmap_status dmap_server_create(dmap_context *ctx, const dmap_server_config *cfg, dmap_server **out);
+/* Cancels what is queued, waits for what runs, joins the worker. */
+void dmap_server_destroy(dmap_server *srv);
+/*
+ * A batch of n rays (8 F32 each, host) answered into n dmap_hit32 (host);
+ * mode DMAP_MODE_CLOSEST or DMAP_MODE_OCCLUDED. Both buffers are borrowed
+ * until the request completes; pinned (cudaHostAlloc / registered) buffers
+ * are copied asynchronously, others through the server's pinned staging.
+ * DMAP_ERR_BUDGET when the request could never fit the budget.
+ */
+dmap_status dmap_server_submit_rays(dmap_server *srv, dmap_scene *scene, const float *rays_host, int64_t n, int mode,
+                                    dmap_hit32 *hits_host, uint64_t *id);
+/* A render (dmap_render's parameters; rgb_host borrowed until completion). */
+dmap_status dmap_server_submit_render(dmap_server *srv, dmap_scene *scene, const dmap_render_desc *desc,
+                                      float *rgb_host, uint64_t *id);
+/* DMAP_OK once complete, DMAP_ERR_NOT_READY before, DMAP_ERR_CANCELLED, or the request's error. */
+dmap_status dmap_server_poll(dmap_server *srv, uint64_t id);
+/* Blocks until the request completes or timeout_s passes (< 0: no limit). */
+dmap_status dmap_server_wait(dmap_server *srv, uint64_t id, double timeout_s);
+/* Cancels a request that is still queued (DMAP_ERR_NOT_READY once it runs). */
+dmap_status dmap_server_cancel(dmap_server *srv, uint64_t id);
+/* Latency in ms of a completed request (submit to completion). */
+dmap_status dmap_server_latency(dmap_server *srv, uint64_t id, double *ms);
+/* Blocks until every submitted request has completed (or timeout_s passes). */
+dmap_status dmap_server_drain(dmap_server *srv, double timeout_s);
+dmap_status dmap_server_get_stats(dmap_server *srv, dmap_server_stats *out);
+
 #ifdef __cplusplus
 }
 #endif
