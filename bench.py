@@ -250,6 +250,8 @@ def main():
     ap.add_argument("--requests", type=int, default=4096, help="serve: requests in the arrival trace")
     ap.add_argument("--interarrival-ms", type=float, default=15.0, help="serve: mean Poisson inter-arrival time")
     ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-request comparison")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="keep --rounds / --blocks-per-sm instead of the autotuner's choice")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
     ap.add_argument("--rounds", type=int, default=6)
@@ -297,7 +299,8 @@ def main():
     rays_all = np.concatenate([prim, bounce, extra_rays(args.config, sc, args.small)]).astype(np.float32)
     # this rank's share
     n_all = len(rays_all)
-    lo, hi = rank * n_all // world, (rank + 1) * n_all // world
+    from dmap_b200.shard import shard_range
+    lo, hi = shard_range(n_all, rank, world)
     my = np.ascontiguousarray(rays_all[lo:hi])
     n = len(my)
     # algorithmic work of the reference algorithm on these rays (FP64 path counters)
@@ -306,10 +309,14 @@ def main():
     # the measured path's own counters (its bounds are wider: more cells may pass)
     _, st_path = dev.intersect(my, opt, np.float64, stats=True)
     counts_path = work_per_ray(st_path)[2]
-    setup_s = time.perf_counter() - t_setup
-
     rays_d = torch.from_numpy(my).cuda()
     hits_d = torch.empty((n, 12), dtype=torch.int32, device="cuda")   # 48 B hit32 records
+    tuned = None
+    if args.tune and args.precision == "f32" and args.schedule == "wavefront":
+        # the launch shape the autotuner picks on these rays (setup, not timed)
+        opt, tune_ms = dev.autotune(rays_d.data_ptr(), dm.F32, n, opt)
+        tuned = {"rounds": opt.rounds, "blocks_per_sm": opt.blocks_per_sm, "sample_ms": tune_ms}
+    setup_s = time.perf_counter() - t_setup
     # one explicit stream for the kernels, the L2 flush and the events
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -381,7 +388,9 @@ def main():
             "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
             "config": {"workload": workload_name(args), "rays_per_step": n_all, "precision": args.precision,
                        "l2": "flushed between steps (256 MB write); pyramids 17 GB exceed L2",
-                       "parallelism": f"replicated scene, rays split over {world} rank(s)"},
+                       "parallelism": f"replicated scene, rays split over {world} rank(s)",
+                       "schedule": args.schedule, "autotuned": tuned,
+                       "rounds": opt.rounds, "blocks_per_sm": opt.blocks_per_sm},
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": int(my.nbytes),
                     "d2h_bytes_per_step": int(n * 48)},
             "gpu_launches": int(launches),

@@ -126,6 +126,8 @@ def lib() -> C.CDLL:
             "dmap_intersect_host": (i32, [vp, vp, i32, i64, C.POINTER(_Options), vp, i32, vp]),
             "dmap_render": (i32, [vp, C.POINTER(_RenderDesc), C.POINTER(_Options), vp, C.POINTER(_RenderStats),
                                   C.POINTER(_RayRecord)]),
+            "dmap_autotune": (i32, [vp, vp, i32, i64, C.POINTER(_Options), C.c_char_p, C.POINTER(_Options),
+                                    C.POINTER(dbl)]),
             "dmap_server_create": (i32, [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]),
             "dmap_server_destroy": (None, [vp]),
             "dmap_server_submit_rays": (i32, [vp, vp, vp, i64, i32, vp, C.POINTER(C.c_uint64)]),
@@ -304,6 +306,20 @@ class Scene:
         opt = (options or TraversalOptions()).c()
         self.ctx.check(lib().dmap_intersect(self.h, rays_ptr, ray_dtype, n, C.byref(opt), hits_ptr, hit_dtype,
                                             stats_ptr or None, stream or None), "dmap_intersect")
+
+    def autotune(self, rays_ptr: int, ray_dtype: int, n: int, base: Optional[TraversalOptions] = None,
+                 cache_path: Optional[str] = None):
+        """dmap_autotune on device rays: (TraversalOptions with the fastest
+        rounds / blocks_per_sm, its time in ms on the sample)."""
+        b = base or TraversalOptions()
+        out = _Options()
+        ms = C.c_double()
+        self.ctx.check(lib().dmap_autotune(self.h, rays_ptr, ray_dtype, n, C.byref(b.c()),
+                                           cache_path.encode() if cache_path else None, C.byref(out), C.byref(ms)),
+                       "dmap_autotune")
+        t = TraversalOptions(**{**b.__dict__, "schedule": "wavefront", "rounds": out.rounds,
+                                "blocks_per_sm": out.blocks_per_sm})
+        return t, ms.value
 
     def render(self, view: dict, emitter: np.ndarray, spp: int = 1, max_depth: int = 5, rr_depth: int = 3,
                radiance=(10.0, 10.0, 10.0), albedo=(0.7, 0.7, 0.7), seed: int = 2027, paths_per_batch: int = 0,

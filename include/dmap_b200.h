@@ -208,6 +208,17 @@ dmap_status dmap_intersect(dmap_scene *scene, const void *rays_dev, dmap_dtype r
 dmap_status dmap_intersect_host(dmap_scene *scene, const void *rays_host, dmap_dtype ray_dtype, int64_t n,
                                 const dmap_options *opt, void *hits_host, dmap_dtype hit_dtype, int64_t *stats_host);
 
+/*
+ * Schedule autotuner (no counterpart in the reference). Times the wavefront
+ * schedule's launch shapes (rounds x blocks_per_sm) with `base`'s other
+ * options on the first min(n, 2^20) of the caller's device rays and returns
+ * `base` with the fastest shape in `best` (and its time in best_ms). With a
+ * cache_path, a result is looked up first and appended after tuning, one
+ * line per scene and query shape ("key rounds blocks_per_sm ms").
+ */
+dmap_status dmap_autotune(dmap_scene *scene, const void *rays_dev, dmap_dtype ray_dtype, int64_t n,
+                          const dmap_options *base, const char *cache_path, dmap_options *best, double *best_ms);
+
 /* ---- batched path tracer ------------------------------------------------- */
 
 /*
