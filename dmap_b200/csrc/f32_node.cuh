@@ -6,6 +6,7 @@
 #include "device_types.cuh"
 #include "f64_math.cuh"
 #include "f64_leaf.cuh"
+#include "f64_node.cuh"
 #include "launch.h"
 
 namespace d32
@@ -319,11 +320,18 @@ __device__ __forceinline__ void store_hit(H *hits, int64_t k, bool found, const 
     hits[k] = out;
 }
 
+// A leaf cell the FP32 walk reached: first the reference's own node test of
+// the cell in double (the FP32 tests, widened by the ray's rounding, admit
+// more leaf cells than the FP64 walk; a cell the FP64 walk rejects has no
+// leaf there), then the certified Newton leaf.
 __device__ __noinline__ inline bool leaf64(const TriDev &T, const AssetDev &g, const double *o, const double *d,
-                                           double t_min, double t_max, int i, int j, d64::hit64 &h, int64_t *st)
+                                           double t_min, double t_max, int i, int j, d64::hit64 &h, int64_t *st,
+                                           const dmapk::QueryOpts &opt)
 {
-    return d64::intersect_newton(T, g, d64::V3(o[0], o[1], o[2]), d64::V3(d[0], d[1], d[2]), t_min, t_max, i, j,
-                                 h, st);
+    d64::v3 O = d64::V3(o[0], o[1], o[2]), D = d64::V3(d[0], d[1], d[2]);
+    if (!d64::leaf_cell_admitted(T, g, O, D, t_min, t_max, i, j, opt))
+        return false;
+    return d64::intersect_newton(T, g, O, D, t_min, t_max, i, j, h, st);
 }
 
 } // namespace d32

@@ -71,7 +71,10 @@ extern "C" dmap_status dmap_autotune(dmap_scene *s, const void *rays_dev, dmap_d
         return st;
     if (q.precision != DMAP_PRECISION_F32)
         return fail(ctx, DMAP_ERR_UNSUPPORTED, "dmap_autotune: the wavefront schedule is on the FP32 path");
-    const int64_t m = std::min<int64_t>(n, 1 << 20); // the sample: the first rays
+    // the sample: the first rays, the whole batch up to 4M (the best shape
+    // depends on how many rays are in flight, so a small prefix of a large
+    // batch misleads)
+    const int64_t m = std::min<int64_t>(n, 4 << 20);
     const std::string key = tune_key(s, q, m);
     int r_best = o.rounds, b_best = o.blocks_per_sm;
     double t_best = 0.0;

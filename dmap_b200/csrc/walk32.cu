@@ -79,30 +79,36 @@ __device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, c
     return ok && !(t0 > t1 + tol32(fmaxf(fabsf(t0), fabsf(t1))));
 }
 
-// The tangent-space ray of a triangle: transformed in double (the
-// reference's own ray), rounded, and E covering that rounding over
-// t in [0, t_far].
+// The tangent-space ray of a triangle: transformed in double, rounded to
+// float, and E covering, for t in [0, t_far], the distance between the float
+// ray and the reference's double ray (A (o - q0), A d in its own operation
+// order): the rounding to float, at most 2^-24 of each coordinate (2^-22
+// taken), plus the difference of two double evaluations of the transform,
+// a few units of 2^-53 of the sums of the terms' magnitudes (2^-40 taken).
 __device__ __forceinline__ void tangent_ray(const TriDev32 &T, const double *o, const double *d, float t_far,
                                             Ray32 &r)
 {
-    float ro[3], rd[3];
+    float ro[3], rd[3], e[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        double x = (o[0] - T.q0[0]) * T.A[a][0];
-        x = __fma_rn(T.A[a][1], o[1] - T.q0[1], x);
-        x = __fma_rn(T.A[a][2], o[2] - T.q0[2], x);
+        double u0 = o[0] - T.q0[0], u1 = o[1] - T.q0[1], u2 = o[2] - T.q0[2];
+        double x = u0 * T.A[a][0];
+        x = __fma_rn(T.A[a][1], u1, x);
+        x = __fma_rn(T.A[a][2], u2, x);
         double y = __fma_rn(T.A[a][2], d[2], __fma_rn(T.A[a][1], d[1], T.A[a][0] * d[0]));
+        double mx = fabs(T.A[a][0] * u0) + fabs(T.A[a][1] * u1) + fabs(T.A[a][2] * u2);
+        double my = fabs(T.A[a][0] * d[0]) + fabs(T.A[a][1] * d[1]) + fabs(T.A[a][2] * d[2]);
         ro[a] = (float)x;
         rd[a] = (float)y;
+        float sum = ru_add(__double2float_ru(mx), ru_mul(t_far, __double2float_ru(my)));
+        e[a] = ru_add(ru_mul(0x1p-22f, ru_add(fabsf(ro[a]), ru_mul(t_far, fabsf(rd[a])))), ru_mul(0x1p-40f, sum));
     }
     r.ox = ro[0], r.oy = ro[1], r.oz = ro[2];
     r.dx = rd[0], r.dy = rd[1], r.dz = rd[2];
     r.ix = r.dx != 0.0f ? __frcp_rn(r.dx) : 0.0f;
     r.iy = r.dy != 0.0f ? __frcp_rn(r.dy) : 0.0f;
     r.iz = r.dz != 0.0f ? __frcp_rn(r.dz) : 0.0f;
-    r.ex = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.ox), ru_mul(t_far, fabsf(r.dx))), 1.0f));
-    r.ey = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.oy), ru_mul(t_far, fabsf(r.dy))), 1.0f));
-    r.ez = ru_mul(2.0f * G, ru_add(ru_add(fabsf(r.oz), ru_mul(t_far, fabsf(r.dz))), 1.0f));
+    r.ex = e[0], r.ey = e[1], r.ez = e[2];
 }
 
 __device__ __forceinline__ float far_bound(float t1) { return ru_add(ru_mul(t1, 1.0f + 4.0f * G), G); }
@@ -155,7 +161,7 @@ __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const Asse
                 ++lah;
             }
             d64::hit64 lh;
-            if (leaf64(T64, g, o, d, t_min, t_max, cur.i, cur.j, lh, st) && lh.t < t_max) {
+            if (leaf64(T64, g, o, d, t_min, t_max, cur.i, cur.j, lh, st, opt) && lh.t < t_max) {
                 hit = lh;
                 t_max = lh.t;
                 found = true;
@@ -546,7 +552,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     // the last round: the few remaining rays finish here
                     d64::hit64 lh;
                     if (leaf64(tris64[tri], assets[T.asset], o, d, t_min, t_max, cur.i, cur.j, lh,
-                               ST ? stl : nullptr) &&
+                               ST ? stl : nullptr, opt) &&
                         lh.t < t_max) {
                         t_max = lh.t;
                         best_tri = tri;
@@ -646,10 +652,19 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
             break;
         const TriDev &T = tris64[tri];
         const AssetDev &g = assets[T.asset];
-        // leaf q of the job: the texel's corners, its normal form, the ray's plane basis (:239-264)
+        // leaf q of the job: the reference's node test of the cell in double
+        // (a cell it rejects has an empty search), then the texel's corners,
+        // its normal form and the ray's plane basis (:239-264)
+        bool admitted = false;
         if (phase == SETUP) {
             li = q_leaf[item].i[q];
             lj = q_leaf[item].j[q];
+            sp = 0;
+            first = false;
+            phase = SEARCH;
+            admitted = leaf_cell_admitted(T, g, O, D, t_min, t_max, li, lj, opt);
+        }
+        if (admitted) {
             L.w = cell_width(g, 0);
             L.lo = {li * L.w, lj * L.w};
             L.h00 = grid_h(g, L.lo.x, L.lo.y);
@@ -665,10 +680,8 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
             L.d_len = norm3(D);
             L.dn = div3(D, L.d_len);
             plane_basis(L.dn, L.d1, L.d2);
-            sp = 0;
             stack[sp++] = {0.5, 0.5, -INFINITY, 0};
             first = true;
-            phase = SEARCH;
         }
         // the next live entry of the search (a pop is a call of search_leaf;
         // an entry at or beyond t_max is the sorted loop's break)

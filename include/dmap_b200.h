@@ -211,7 +211,7 @@ dmap_status dmap_intersect_host(dmap_scene *scene, const void *rays_host, dmap_d
 /*
  * Schedule autotuner (no counterpart in the reference). Times the wavefront
  * schedule's launch shapes (rounds x blocks_per_sm) with `base`'s other
- * options on the first min(n, 2^20) of the caller's device rays and returns
+ * options on the first min(n, 2^22) of the caller's device rays and returns
  * `base` with the fastest shape in `best` (and its time in best_ms). With a
  * cache_path, a result is looked up first and appended after tuning, one
  * line per scene and query shape ("key rounds blocks_per_sm ms").
