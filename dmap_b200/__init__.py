@@ -11,8 +11,11 @@ of include/dmap_b200.h (libdmap_b200.so, built in place by
   queries (ObjectIntersector::intersect, embree intersect_callback) and
   occlusion queries (occluded_callback) for a batch of rays.
 - ``TraversalOptions``: the reference's bound / slab_max_level / leaf
-  (traversal_options.h:600-608) plus precision, mode and the FP64 polish
-  threshold.
+  (traversal_options.h:600-608) plus precision, mode and the schedule.
+- ``Scene.render``: the batched path tracer (emitter-sampled shadow rays
+  through the occlusion query); ``Server``: continuous batching of many
+  callers' requests over resident scenes; ``Scene.autotune``: the schedule
+  autotuner.
 
 There is no CPU fallback: without the built library or a CUDA device every
 entry point raises.
@@ -45,7 +48,7 @@ HIT64 = np.dtype([("t", "<f8"), ("st", "<f8", 2), ("bary", "<f8", 2), ("ng", "<f
                   ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
 STATS = ("triangle_tests", "node_tests", "leaf_tests", "sub_squares", "newton_iters", "node_tests_after_hit",
          "leaf_tests_after_hit", "reserved")
-HIT_POLISHED, HIT_CAPPED = 1, 2
+HIT_FP64_LEAF, HIT_CAPPED = 1, 2
 
 
 class DmapError(RuntimeError):

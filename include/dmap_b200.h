@@ -138,7 +138,10 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *o
 #define DMAP_LEAF_NEWTON 0
 #define DMAP_LEAF_TWO_TRIANGLE 1
 #define DMAP_PRECISION_F64 0 /* the reference's double arithmetic, operation for operation */
-#define DMAP_PRECISION_F32 1 /* FP32 walk and leaf, bounds widened outward, FP64 Newton polish */
+/* FP32 walk, bounds widened outward so it admits every cell the FP64 walk
+ * admits; each leaf cell re-tested and its leaf run in FP64 with the
+ * reference's arithmetic, so every hit equals the FP64 path's */
+#define DMAP_PRECISION_F32 1
 #define DMAP_MODE_CLOSEST 0  /* closest hit in (t_min, t_max): rtcIntersect1 / intersect_callback */
 #define DMAP_MODE_OCCLUDED 1 /* any hit in (t_min, t_max): rtcOccluded1 / occluded_callback */
 
@@ -151,7 +154,8 @@ typedef struct dmap_options {
     int leaf;           /* DMAP_LEAF_*, default NEWTON */
     int precision;      /* DMAP_PRECISION_*, default F32 */
     int mode;           /* DMAP_MODE_*, default CLOSEST */
-    double polish_cond; /* FP32 path: FP64 Newton polish when cond(J) exceeds this (default 1e4; 0 = always) */
+    double polish_cond; /* reserved for an FP32 leaf with FP64 refinement above this cond(J) (default
+                           1e4); this build's leaves are FP64 throughout and ignore it */
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32, default 6) */
     int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 4) */
@@ -175,7 +179,7 @@ typedef struct dmap_hit64 {
     int32_t tri, i, j, flags;
 } dmap_hit64;
 /* dmap_hit*.flags bits */
-#define DMAP_HIT_POLISHED 1 /* FP32 path: the hit went through the FP64 Newton polish */
+#define DMAP_HIT_FP64_LEAF 1 /* the root came from the FP64 certified Newton leaf (every hit of this build) */
 #define DMAP_HIT_CAPPED 2   /* a device iteration cap ran out for this ray */
 
 /* Per-ray counters (TraversalStats, displaced_intersector.h:89-105), 8 int64 per ray. */
