@@ -96,8 +96,11 @@ struct Hit64
 
 } // namespace dmapdev
 
-// Hit flag bits, as DMAP_HIT_* of include/dmap_b200.h.
-constexpr int32_t DMAP_HIT_FP64_LEAF = 1; // the root came from the FP64 Newton leaf or polish
+// Hit flag bits, as DMAP_HIT_* of include/dmap_b200.h (which defines the
+// same names when it is included first).
+#ifndef DMAP_HIT_FP64_LEAF
+#define DMAP_HIT_FP64_LEAF 1 // the root came from the FP64 certified Newton leaf
+#endif
 
 // Per-ray counter slots (TraversalStats), as DMAP_ST_* of include/dmap_b200.h.
 enum
