@@ -167,16 +167,21 @@ __device__ inline bool node_interval(const nodebound &nb, const tray &r, const d
     return true;
 }
 
-// The reference's own node test of leaf cell (i, j) at the ray's current
-// t_max: false exactly when the FP64 walk would reject the cell there.
-__device__ inline bool leaf_cell_admitted(const TriDev &T, const AssetDev &a, v3 o, v3 d, double t_min,
-                                          double t_max, int64_t i, int64_t j, const dmapk::QueryOpts &opt)
+// The reference's own node test of leaf cell (i, j) for the tangent-space
+// ray r: false exactly when the FP64 walk would reject the cell at r.t_max.
+__device__ inline bool leaf_cell_admitted(const TriDev &T, const AssetDev &a, const tray &r, int64_t i, int64_t j,
+                                          const dmapk::QueryOpts &opt)
 {
     nodebound nb;
     node_bound_of(nb, T, a, 0, i, j, leaf_node(a, i, j));
-    tray r = tangent_ray64(T, o, d, t_min, t_max);
     double t0, t1;
     return node_interval(nb, r, opt, t0, t1);
+}
+
+__device__ inline bool leaf_cell_admitted(const TriDev &T, const AssetDev &a, v3 o, v3 d, double t_min,
+                                          double t_max, int64_t i, int64_t j, const dmapk::QueryOpts &opt)
+{
+    return leaf_cell_admitted(T, a, tangent_ray64(T, o, d, t_min, t_max), i, j, opt);
 }
 
 } // namespace d64

@@ -587,6 +587,47 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     }
 }
 
+// The leaf cells of a round's jobs through the reference's own node test in
+// double (node_bounds.cpp:83-211 at level 0, the node computed from the
+// grid): the FP32 walk, widened by its roundings, reaches more leaf cells
+// than the FP64 walk, and a cell the FP64 walk rejects has no leaf there.
+// The ray's t_max is the one it parked with; earlier leaves of the same job
+// can only shrink it, so a cell kept here may still be rejected by the FP64
+// walk at that point, and its search then finds nothing the reference
+// would not. Cells are compacted in walk order; a job may end up empty.
+// Kept apart from the leaf kernel so that kernel's code stays small.
+template <typename R>
+__global__ void __launch_bounds__(128)
+    wave_filter(const TriDev *__restrict__ tris64, const AssetDev *__restrict__ assets, const R *__restrict__ rays,
+                dmapk::QueryOpts opt, const RayState *__restrict__ states, LeafJob *__restrict__ q_leaf, int round,
+                const unsigned long long *ctr)
+{
+    const unsigned long long count = *round_ctr(const_cast<unsigned long long *>(ctr), round, 1);
+    for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < count;
+         k += (unsigned long long)gridDim.x * blockDim.x) {
+        LeafJob job = q_leaf[k];
+        double o[3], d[3], t_min, t_max;
+        load_ray(rays, job.ray, o, d, t_min, t_max);
+        t_max = states[job.ray].t_max;
+        const TriDev &T = tris64[job.tri];
+        const AssetDev &g = assets[T.asset];
+        d64::tray r = d64::tangent_ray64(T, d64::V3(o[0], o[1], o[2]), d64::V3(d[0], d[1], d[2]), t_min, t_max);
+        int m = 0;
+#pragma unroll 1
+        for (int q = 0; q < job.n; ++q) {
+            if (d64::leaf_cell_admitted(T, g, r, job.i[q], job.j[q], opt)) {
+                job.i[m] = job.i[q];
+                job.j[m] = job.j[q];
+                ++m;
+            }
+        }
+        if (m != job.n) {
+            job.n = m;
+            q_leaf[k] = job;
+        }
+    }
+}
+
 // The parked leaves of a round (the certified leaf, d64::intersect_newton,
 // displaced_intersector.cpp:239-323). Each lane holds one job at a time and
 // takes the next one as soon as its own is done, so a warp's lanes stay busy
@@ -637,14 +678,20 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
                     tri = J.tri;
                     n_leaves = J.n;
                     q = 0;
-                    double o[3], d[3];
-                    load_ray(rays, ray, o, d, t_min, t_max);
-                    O = V3(o[0], o[1], o[2]);
-                    D = V3(d[0], d[1], d[2]);
-                    t_max = states[ray].t_max;
-                    answered = false;
-                    subs = iters = 0;
-                    phase = SETUP;
+                    if (n_leaves == 0) {
+                        // the filter rejected every cell of the job: the walk goes on
+                        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 3), 1ull);
+                        q_out[slot] = ray;
+                    } else {
+                        double o[3], d[3];
+                        load_ray(rays, ray, o, d, t_min, t_max);
+                        O = V3(o[0], o[1], o[2]);
+                        D = V3(d[0], d[1], d[2]);
+                        t_max = states[ray].t_max;
+                        answered = false;
+                        subs = iters = 0;
+                        phase = SETUP;
+                    }
                 }
             }
         }
@@ -652,19 +699,13 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
             break;
         const TriDev &T = tris64[tri];
         const AssetDev &g = assets[T.asset];
-        // leaf q of the job: the reference's node test of the cell in double
-        // (a cell it rejects has an empty search), then the texel's corners,
+        // leaf q of the job (a cell wave_filter kept): the texel's corners,
         // its normal form and the ray's plane basis (:239-264)
-        bool admitted = false;
         if (phase == SETUP) {
             li = q_leaf[item].i[q];
             lj = q_leaf[item].j[q];
             sp = 0;
-            first = false;
             phase = SEARCH;
-            admitted = leaf_cell_admitted(T, g, O, D, t_min, t_max, li, lj, opt);
-        }
-        if (admitted) {
             L.w = cell_width(g, 0);
             L.lo = {li * L.w, lj * L.w};
             L.h00 = grid_h(g, L.lo.x, L.lo.y);
@@ -787,7 +828,8 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
     cudaError_t e;
     if (stats && (e = cudaMemsetAsync(stats, 0, sizeof(int64_t) * DMAP_ST_N * n, stream)) != cudaSuccess)
         return e;
-    int rounds = opt.rounds > 0 ? opt.rounds : 6;
+    // rounds = 0: a single walk that runs every leaf inline
+    int rounds = opt.rounds > 0 ? opt.rounds : 0;
     if (rounds > dmapk::kMaxRounds)
         rounds = dmapk::kMaxRounds;
     if ((e = cudaMemsetAsync(ws.counters, 0, sizeof(unsigned long long) * 4 * (rounds + 1), stream)) != cudaSuccess)
@@ -827,6 +869,7 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
         if (last)
             break;
         int lgrid = sm_count() * 4;
+        wave_filter<R><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, states, leaves, rd, ws.counters);
         if (stats)
             wave_leaf<true, R, H, Fp><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, hh, stats, states, leaves, rd,
                                                                 q_out, ws.counters);
@@ -850,10 +893,10 @@ int walk32_launches(const QueryOpts &opt)
 {
     if (opt.schedule == 1)
         return 1;
-    int rounds = opt.rounds > 0 ? opt.rounds : 6;
+    int rounds = opt.rounds > 0 ? opt.rounds : 0;
     if (rounds > kMaxRounds)
         rounds = kMaxRounds;
-    return 2 * rounds + 1;
+    return 3 * rounds + 1; // per round: walk, cell filter, leaves; then the inline walk
 }
 
 cudaError_t launch_walk32(const dmapdev::TriDev32 *t32, const dmapdev::TriDev *t64, int n_tri,

@@ -157,7 +157,8 @@ typedef struct dmap_options {
     double polish_cond; /* reserved for an FP32 leaf with FP64 refinement above this cond(J) (default
                            1e4); this build's leaves are FP64 throughout and ignore it */
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
-    int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32, default 6) */
+    int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
+                           default 6; 0 = one walk with every leaf inline) */
     int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 4) */
 } dmap_options;
 
