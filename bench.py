@@ -246,7 +246,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
-    ap.add_argument("--config", default="sphere", choices=["sphere", "sphere16", "quad", "pathtrace", "serve"])
+    ap.add_argument("--config", default="sphere",
+                    choices=["sphere", "sphere16", "quad", "pathtrace", "serve", "pyramid"])
     ap.add_argument("--requests", type=int, default=4096, help="serve: requests in the arrival trace")
     ap.add_argument("--interarrival-ms", type=float, default=15.0, help="serve: mean Poisson inter-arrival time")
     ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-request comparison")
@@ -282,6 +283,9 @@ def main():
         return
     if args.config == "serve":
         run_serve(args, rank, world, local, dist)
+        return
+    if args.config == "pyramid":
+        run_pyramid(args, rank, world, local, dist)
         return
 
     t_setup = time.perf_counter()
@@ -492,6 +496,48 @@ def run_pathtrace(args, rank, world, local, dist):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def run_pyramid(args, rank, world, local, dist):
+    """The pyramid build (K1): the cube sphere's 96 maps of 2048^2 FP32
+    texels, each built into its outward FP32 pyramid (the product path: the
+    FP64 levels are scratch). A step builds all 96; its time is the sum of
+    the build kernels' CUDA-event times. Algorithmic bytes per map: the node
+    grid read once, the FP32 pyramid written once."""
+    import torch
+    import dmap_b200 as dm
+    sc, _ = build_scene("sphere", args.small)
+    ctx = dm.Context(local)
+    per_map = []
+    for s in range(args.warmup + args.steps):
+        ms = 0.0
+        with Clocks(local) as clk:
+            for a in sc.assets:
+                asset = dm.Asset(ctx, a.nodes)
+                ms += asset.build_ms
+                asset.close()
+        if s >= args.warmup:
+            per_map.append(ms)
+    ms = float(np.mean(per_map))
+    nodes = sc.assets[0].nodes.shape[0]
+    n = nodes - 1
+    cells = sum((n >> l) ** 2 for l in range(n.bit_length()))
+    byts = len(sc.assets) * (nodes * nodes * 4 + 32 * cells)
+    hbm, peak_src = peaks()
+    gbs = byts / (ms * 1e-3) / 1e9
+    line = {"metric": "pyramid build GB/s (algorithmic)", "value": gbs, "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"pyramid build, 96 maps of {n}^2 FP32 texels, outward FP32 pyramid",
+                       "maps_per_step": len(sc.assets), "cells_per_map": cells},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "traffic": None, "peak_source": peak_src, "kernel": "pyramid_leaf_kernel + folds",
+                         "bytes_per_map": byts / len(sc.assets)}}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def serve_trace(n_req: int, interarrival_ms: float, seed: int, small: bool):

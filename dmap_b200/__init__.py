@@ -120,6 +120,7 @@ def lib() -> C.CDLL:
             "dmap_asset_destroy": (None, [vp]),
             "dmap_asset_levels": (i32, [vp]),
             "dmap_asset_bytes": (C.c_size_t, [vp]),
+            "dmap_asset_build_ms": (dbl, [vp]),
             "dmap_asset_pyramid_level": (i32, [vp, i32, i32, vp]),
             "dmap_scene_create": (i32, [vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
             "dmap_scene_destroy": (None, [vp]),
@@ -235,6 +236,11 @@ class Asset:
     @property
     def device_bytes(self) -> int:
         return lib().dmap_asset_bytes(self.h)
+
+    @property
+    def build_ms(self) -> float:
+        """CUDA-event time of the pyramid build kernels."""
+        return lib().dmap_asset_build_ms(self.h)
 
     def level(self, level: int, precision: str = "f64") -> dict:
         m = self.n_leaf >> level

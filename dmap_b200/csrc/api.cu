@@ -41,6 +41,14 @@ dmap_status dmap_create(int device, dmap_context **out)
         delete ctx;
         return DMAP_ERR_CUDA;
     }
+    // stream-ordered allocations (render jobs, served requests) stay cached in
+    // the device's default pool between calls instead of going back to the
+    // driver at every synchronization
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = ctx;
     return DMAP_OK;
 }
@@ -155,8 +163,18 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS)
         return cleanup(fail(ctx, DMAP_ERR_CUDA, "dmap_asset_create: cuTensorMapEncodeTiled failed"));
-    if ((e = dmapk::launch_pyramid(&tmap, d, T, a->pyr64, a->pyr32, ctx->status_dev, ctx->stream)) != cudaSuccess)
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    cudaEventRecord(ev[0], ctx->stream);
+    e = dmapk::launch_pyramid(&tmap, d, T, a->pyr64, a->pyr32, ctx->status_dev, ctx->stream,
+                              (flags & DMAP_ASSET_KEEP_F64) != 0);
+    cudaEventRecord(ev[1], ctx->stream);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
         return cleanup(cuda_fail(ctx, e, "dmap_asset_create: pyramid launch"));
+    }
     {
         // one leaf launch plus one fold launch per five levels above the tile
         int level = 0, t = T, launches = 1;
@@ -169,6 +187,9 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
         ctx->launches += launches;
     }
     dmap_status s = sync_and_check(ctx, "dmap_asset_create");
+    cudaEventElapsedTime(&a->build_ms, ev[0], ev[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
     if (s != DMAP_OK)
         return cleanup(s);
     if (!(flags & DMAP_ASSET_KEEP_F64)) {
@@ -195,6 +216,7 @@ void dmap_asset_destroy(dmap_asset *a)
 
 int dmap_asset_levels(const dmap_asset *a) { return a ? a->dev.n_levels : 0; }
 size_t dmap_asset_bytes(const dmap_asset *a) { return a ? a->bytes : 0; }
+double dmap_asset_build_ms(const dmap_asset *a) { return a ? a->build_ms : 0.0; }
 
 dmap_status dmap_asset_pyramid_level(const dmap_asset *a, int level, int precision, double *out)
 {

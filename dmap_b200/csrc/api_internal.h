@@ -50,6 +50,7 @@ struct dmap_asset
     float *pyr32 = nullptr;
     size_t bytes = 0;
     int64_t cells = 0;
+    float build_ms = 0.0f; // CUDA-event time of the pyramid kernels
 };
 
 struct dmap_scene

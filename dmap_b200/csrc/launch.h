@@ -46,8 +46,10 @@ int walk32_launches(const QueryOpts &opt);
 // grid (128 bytes), `tile` the leaf cells per CTA side. Writes the FP64
 // levels without the offset into pyr64 and the outward-rounded FP32 levels
 // with it into pyr32.
+// all64: write every FP64 level (the FP64 pyramid is kept); otherwise only
+// the levels the fold launches read back, which are scratch.
 cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int tile, double *pyr64, float *pyr32,
-                           unsigned *status, cudaStream_t stream);
+                           unsigned *status, cudaStream_t stream, bool all64 = true);
 
 // Per-triangle setup (setup.cu).
 cudaError_t launch_setup(const double *tris_dev, const int *tri_asset_dev, const dmapdev::AssetDev *assets_dev,

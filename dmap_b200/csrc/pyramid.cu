@@ -101,13 +101,18 @@ __device__ __forceinline__ Node8 fold4(const Node8 &c, int a, int b, double s)
     return p;
 }
 
-__device__ __forceinline__ void store_node(const Node8 &n, double offset, size_t k, double *pyr64, float *pyr32)
+// store64: write the FP64 cell too (every level when the FP64 pyramid is
+// kept; otherwise only the levels a later fold launch reads).
+__device__ __forceinline__ void store_node(const Node8 &n, double offset, size_t k, double *pyr64, float *pyr32,
+                                           bool store64)
 {
-    double2 *p = reinterpret_cast<double2 *>(pyr64 + 8 * k);
-    p[0] = make_double2(n.h0, n.gu);
-    p[1] = make_double2(n.gv, n.r);
-    p[2] = make_double2(n.ru, n.rv);
-    p[3] = make_double2(n.mn, n.mx);
+    if (store64) {
+        double2 *p = reinterpret_cast<double2 *>(pyr64 + 8 * k);
+        p[0] = make_double2(n.h0, n.gu);
+        p[1] = make_double2(n.gv, n.r);
+        p[2] = make_double2(n.ru, n.rv);
+        p[3] = make_double2(n.mn, n.mx);
+    }
     double h0 = n.h0, mn = n.mn, mx = n.mx;
     if (offset != 0.0) {
         h0 += offset;
@@ -127,7 +132,7 @@ __device__ __forceinline__ void store_node(const Node8 &n, double offset, size_t
 // to one cell, storing each level. `level0` is the level of the held cells,
 // (tx, ty) the tile's position in units of T cells at level0.
 __device__ void fold_tile(Node8 v, int T, int level0, int tx, int ty, const AssetDev &a, double *pyr64,
-                          float *pyr32, Node8 *smem)
+                          float *pyr32, Node8 *smem, bool all64)
 {
     int t = threadIdx.x;
     int count = T * T;
@@ -147,7 +152,7 @@ __device__ void fold_tile(Node8 v, int T, int level0, int tx, int ty, const Asse
             int x = (int)compact1by1((unsigned)pc), y = (int)compact1by1((unsigned)pc >> 1);
             int ps = side >> 1;
             size_t k = (size_t)a.level_off[lvl] + (size_t)(ty * ps + y) * m + (tx * ps + x);
-            store_node(p, a.offset, k, pyr64, pyr32);
+            store_node(p, a.offset, k, pyr64, pyr32, all64 || count == 4); // the tile's top: the next launch reads it
         }
         __syncthreads();
         count >>= 2;
@@ -191,7 +196,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar_addr, unsigned phase)
 // Leaf level + in-tile folds. Block: T*T threads. Grid: (n_leaf/T)^2 tiles.
 template <typename In>
 __global__ void __launch_bounds__(256) pyramid_leaf_kernel(const __grid_constant__ CUtensorMap tmap, AssetDev a,
-                                                            int T, double *pyr64, float *pyr32, unsigned *status)
+                                                            int T, double *pyr64, float *pyr32, unsigned *status,
+                                                            bool all64)
 {
     __shared__ alignas(128) In tile[(kMaxTile + 1) * kTilePitch];
     __shared__ alignas(8) unsigned long long bar;
@@ -242,14 +248,14 @@ __global__ void __launch_bounds__(256) pyramid_leaf_kernel(const __grid_constant
     n.mx = dmax(dmax(v00, v10), dmax(v01, v11));
     size_t k = (size_t)(ty * T + y) * a.n_leaf + (tx * T + x);
     if (active)
-        store_node(n, a.offset, k, pyr64, pyr32);
-    fold_tile(n, T, 0, tx, ty, a, pyr64, pyr32, smem);
+        store_node(n, a.offset, k, pyr64, pyr32, all64 || T == 1);
+    fold_tile(n, T, 0, tx, ty, a, pyr64, pyr32, smem, all64);
 }
 
 // Folds level `level0` (m0 x m0 cells, FP64 without offset) upward.
 // Block: T*T threads, grid: (m0/T)^2.
 __global__ void __launch_bounds__(256) pyramid_fold_kernel(AssetDev a, int level0, int T, double *pyr64,
-                                                            float *pyr32)
+                                                            float *pyr32, bool all64)
 {
     __shared__ Node8 smem[kMaxTile * kMaxTile / 4];
     int m0 = a.n_leaf >> level0;
@@ -262,17 +268,17 @@ __global__ void __launch_bounds__(256) pyramid_fold_kernel(AssetDev a, int level
     const double2 *p = reinterpret_cast<const double2 *>(pyr64 + 8 * k);
     double2 q0 = p[0], q1 = p[1], q2 = p[2], q3 = p[3];
     Node8 n = {q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y};
-    fold_tile(n, T, level0, tx, ty, a, pyr64, pyr32, smem);
+    fold_tile(n, T, level0, tx, ty, a, pyr64, pyr32, smem, all64);
 }
 
 template <typename In>
 cudaError_t launch_leaf(const void *tmap, const AssetDev &a, int T, double *pyr64, float *pyr32, unsigned *status,
-                        cudaStream_t stream)
+                        bool all64, cudaStream_t stream)
 {
     int tiles = (a.n_leaf / T) * (a.n_leaf / T);
     int threads = T * T < 32 ? 32 : T * T;
     pyramid_leaf_kernel<In><<<tiles, threads, 0, stream>>>(*reinterpret_cast<const CUtensorMap *>(tmap), a, T,
-                                                           pyr64, pyr32, status);
+                                                           pyr64, pyr32, status, all64);
     return cudaGetLastError();
 }
 
@@ -281,15 +287,15 @@ cudaError_t launch_leaf(const void *tmap, const AssetDev &a, int T, double *pyr6
 namespace dmapk
 {
 cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int tile, double *pyr64, float *pyr32,
-                           unsigned *status, cudaStream_t stream)
+                           unsigned *status, cudaStream_t stream, bool all64)
 {
     cudaError_t e;
     if (a.dtype == 0)
-        e = launch_leaf<float>(tmap, a, tile, pyr64, pyr32, status, stream);
+        e = launch_leaf<float>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
     else if (a.dtype == 1)
-        e = launch_leaf<__half>(tmap, a, tile, pyr64, pyr32, status, stream);
+        e = launch_leaf<__half>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
     else
-        e = launch_leaf<double>(tmap, a, tile, pyr64, pyr32, status, stream);
+        e = launch_leaf<double>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
     if (e != cudaSuccess)
         return e;
     // levels above the first tile fold
@@ -299,7 +305,7 @@ cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int til
         int m = a.n_leaf >> level;
         T = m < kMaxTile ? m : kMaxTile;
         int threads = T * T < 32 ? 32 : T * T;
-        pyramid_fold_kernel<<<(m / T) * (m / T), threads, 0, stream>>>(a, level, T, pyr64, pyr32);
+        pyramid_fold_kernel<<<(m / T) * (m / T), threads, 0, stream>>>(a, level, T, pyr64, pyr32, all64);
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
     }

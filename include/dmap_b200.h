@@ -73,6 +73,10 @@ void dmap_asset_destroy(dmap_asset *asset);
 int dmap_asset_levels(const dmap_asset *asset);
 /* Device bytes the asset holds. */
 size_t dmap_asset_bytes(const dmap_asset *asset);
+/* CUDA-event time in ms of the asset's pyramid build kernels (no reference
+ * counterpart: the measurement of the build, which the reference times on
+ * the CPU around the TaylorPyramid constructor). */
+double dmap_asset_build_ms(const dmap_asset *asset);
 /*
  * Copies pyramid level `level` to the host as 8 channel planes (h0, gu, gv, r,
  * ru, rv, h_min, h_max), each m*m doubles with m = 2^L >> level, [j*m + i]

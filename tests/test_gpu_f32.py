@@ -102,3 +102,20 @@ def test_f32_occluded(ctx, oracle):
     ho, _ = cpu.intersect(rays)
     h = dev.intersect(rays, dm.TraversalOptions(precision="f32", mode="occluded"))
     assert np.array_equal(h["tri"] >= 0, ho[:, 10] >= 0)
+
+
+def test_f32_grazing_rays_f16(ctx, oracle):
+    """The precision variant's stress case: FP16 texels and rays 0.1-5 deg
+    above the tangent plane, aimed at base-surface points, some aimed at
+    displaced surface points; every hit record equals the oracle's."""
+    sc = helpers.small_sphere(64, patches=(0, 1, 5, 16))
+    for a in sc.assets:
+        a.nodes = a.nodes.astype(np.float16)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    p, m = scenes.base_points(sc, 3000, seed=77)
+    rng = np.random.default_rng(78)
+    _, _, S = helpers.surface_points(cpu, rng, 1000)
+    nrm = S / np.linalg.norm(S, axis=1, keepdims=True)   # sphere patches: radial normals
+    rays = np.concatenate([scenes.grazing_rays(p, m, seed=79), scenes.grazing_rays(S, nrm, seed=80)])
+    n, _ = _check(cpu, dev, rays)
+    assert n > 1000
