@@ -256,7 +256,7 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
     ap.add_argument("--rounds", type=int, default=6)
-    ap.add_argument("--blocks-per-sm", type=int, default=4)
+    ap.add_argument("--blocks-per-sm", type=int, default=5)
     ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     args = ap.parse_args()

@@ -168,7 +168,7 @@ class TraversalOptions:
     polish_cond: float = 1e4
     schedule: str = "wavefront"
     rounds: int = 6
-    blocks_per_sm: int = 4
+    blocks_per_sm: int = 5
 
     def c(self) -> _Options:
         return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],

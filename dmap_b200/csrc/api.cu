@@ -83,7 +83,7 @@ void dmap_options_default(dmap_options *opt)
     opt->polish_cond = 1e4;
     opt->schedule = DMAP_SCHEDULE_WAVEFRONT;
     opt->rounds = 6;
-    opt->blocks_per_sm = 4;
+    opt->blocks_per_sm = 5;
 }
 
 // ---- assets ---------------------------------------------------------------

@@ -94,9 +94,9 @@ extern "C" dmap_status dmap_autotune(dmap_scene *s, const void *rays_dev, dmap_d
     cudaEventCreate(&e1);
     // rounds: how long rays park at leaves before the inline drain takes the
     // rest; blocks per SM: resident walk warps (the kernels are compiled for
-    // at most 4 CTAs of 128 threads per SM)
+    // at most 5 CTAs of 128 threads per SM)
     const int rounds_c[] = {2, 3, 4, 6, 8, 12};
-    const int bps_c[] = {2, 3, 4};
+    const int bps_c[] = {3, 4, 5};
     t_best = 1e30;
     for (int r : rounds_c)
         for (int b : bps_c) {

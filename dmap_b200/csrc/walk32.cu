@@ -46,10 +46,14 @@ using dmapdev::TriDev32;
 // Resident 128-thread CTAs per SM the walk and leaf kernels are compiled for
 // (register budget: 65536 / (128 x blocks) per thread).
 #ifndef DMAP_WALK_MIN_BLOCKS
-#define DMAP_WALK_MIN_BLOCKS 4
+#define DMAP_WALK_MIN_BLOCKS 5
 #endif
 #ifndef DMAP_LEAF_MIN_BLOCKS
 #define DMAP_LEAF_MIN_BLOCKS 1
+#endif
+// Node tests a ray may run past its first collected leaf before it parks.
+#ifndef DMAP_STALE_CAP
+#define DMAP_STALE_CAP 32
 #endif
 
 constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the object-box candidate mask
@@ -245,7 +249,12 @@ struct RayState
 // the smaller t_max of a hit; the leaf kernel runs them with that smaller
 // t_max, where they cannot report a nearer root than the one found, so the
 // ray's hit is unchanged.
-constexpr int kCollect = 4;
+constexpr int kCollect = 4; // leaf slots of a job
+// Leaves a ray collects before it parks (at most kCollect).
+#ifndef DMAP_COLLECT
+#define DMAP_COLLECT 4
+#endif
+static_assert(DMAP_COLLECT >= 1 && DMAP_COLLECT <= kCollect, "leaf slots");
 struct LeafJob
 {
     int ray, tri, n, pad;
@@ -253,7 +262,7 @@ struct LeafJob
 };
 // RayState.flags
 constexpr int kFoundInTri = 1; // a hit was taken in the triangle in progress
-constexpr int kAtEnd = 2;      // parked at the end of a triangle's walk: resume without cell_next
+constexpr int kResumeHere = 2; // parked before visiting cell `cur` (or at the walk's end): resume without cell_next
 
 // Counter slots of one round: the walk's fetch counter, the leaf queue's
 // length, the leaf kernel's fetch counter, the resume queue's length.
@@ -294,6 +303,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
         mask[w] = 0u;
     int64_t stl[DMAP_ST_N];
     int nl = 0, li0 = 0, lj0 = 0, li1 = 0, lj1 = 0, li2 = 0, lj2 = 0, li3 = 0, lj3 = 0; // collected leaves
+    int since = 0; // node tests since the first collected leaf
 
     auto flush_stats = [&]() {
         if (ST)
@@ -301,14 +311,16 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 stats[DMAP_ST_N * (int64_t)ray + q] += stl[q];
     };
     // Park the ray: its collected leaves become one job, its walk state
-    // waits for the next round (at_end: the triangle's walk is over).
-    auto park = [&](bool at_end) {
+    // waits for the next round (here: resume at `cur` itself, which is the
+    // next cell to visit or the end of the triangle's walk; otherwise `cur`
+    // is the last collected leaf and the walk resumes past it).
+    auto park = [&](bool here) {
         RayState &s = states[ray];
         s.t_max = t_max;
         s.tri = tri;
         s.root = root;
         s.best_tri = best_tri;
-        s.flags = at_end ? (flags | kAtEnd) : (flags & ~kAtEnd);
+        s.flags = here ? (flags | kResumeHere) : (flags & ~kResumeHere);
         s.cl = cur.level, s.ci = cur.i, s.cj = cur.j;
         s.el = end.level, s.ei = end.i, s.ej = end.j;
         s.nah = nah;
@@ -326,6 +338,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
         job.i[2] = li2, job.j[2] = lj2, job.i[3] = li3, job.j[3] = lj3;
         q_leaf[slot] = job;
         nl = 0;
+        since = 0;
         flush_stats();
         phase = NEED;
     };
@@ -385,9 +398,9 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                         sj = r.dy < 0.0f;
                         cur = {s.cl, s.ci, s.cj};
                         end = {s.el, s.ei, s.ej};
-                        if (!(flags & kAtEnd))
+                        if (!(flags & kResumeHere))
                             cell_next(cur, si, sj, T.root_level); // past the last leaf (displaced_intersector.cpp:229)
-                        flags &= ~kAtEnd;
+                        flags &= ~kResumeHere;
                         guard = 0;
                         nl = 0;
                         phase = WALK;
@@ -576,13 +589,18 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     lj2 = nl == 2 ? cur.j : lj2;
                     li3 = nl == 3 ? cur.i : li3;
                     lj3 = nl == 3 ? cur.j : lj3;
-                    if (++nl == kCollect)
+                    if (++nl == DMAP_COLLECT)
                         park(false);
                     else
                         cell_next(cur, si, sj, T.root_level);
                 }
             }
         }
+        // a ray holding collected leaves walks on with the t_max it had
+        // before them; after DMAP_STALE_CAP such node tests it parks (at the
+        // next cell to visit) so that the leaves can shrink t_max first
+        if (!INLINE_LEAF && phase == WALK && nl > 0 && ++since > DMAP_STALE_CAP)
+            park(true);
         __syncwarp();
     }
 }

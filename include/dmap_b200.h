@@ -163,7 +163,7 @@ typedef struct dmap_options {
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
                            default 6; 0 = one walk with every leaf inline) */
-    int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 4) */
+    int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 5, at most 5 resident) */
 } dmap_options;
 
 /* Fills the defaults above. */
