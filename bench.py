@@ -251,6 +251,7 @@ def main():
     ap.add_argument("--requests", type=int, default=4096, help="serve: requests in the arrival trace")
     ap.add_argument("--interarrival-ms", type=float, default=15.0, help="serve: mean Poisson inter-arrival time")
     ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-request comparison")
+    ap.add_argument("--build", default="fold", choices=["fold", "direct"], help="pyramid: the build to time")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="keep --rounds / --blocks-per-sm instead of the autotuner's choice")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
@@ -513,7 +514,7 @@ def run_pyramid(args, rank, world, local, dist):
         ms = 0.0
         with Clocks(local) as clk:
             for a in sc.assets:
-                asset = dm.Asset(ctx, a.nodes)
+                asset = dm.Asset(ctx, a.nodes, build=args.build)
                 ms += asset.build_ms
                 asset.close()
         if s >= args.warmup:
@@ -528,10 +529,12 @@ def run_pyramid(args, rank, world, local, dist):
     line = {"metric": "pyramid build GB/s (algorithmic)", "value": gbs, "unit": "GB/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"pyramid build, 96 maps of {n}^2 FP32 texels, outward FP32 pyramid",
-                       "maps_per_step": len(sc.assets), "cells_per_map": cells},
+            "config": {"workload": f"pyramid build ({args.build}), 96 maps of {n}^2 FP32 texels, outward FP32 "
+                                   "pyramid", "maps_per_step": len(sc.assets), "cells_per_map": cells},
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
-                         "traffic": None, "peak_source": peak_src, "kernel": "pyramid_leaf_kernel + folds",
+                         "traffic": None, "peak_source": peak_src,
+                         "kernel": "pyramid_leaf_kernel + folds" if args.build == "fold"
+                         else "direct_hull_* + direct_cells",
                          "bytes_per_map": byts / len(sc.assets)}}
     clk_s = clk.summary()
     if clk_s:

@@ -40,7 +40,7 @@ LEAF = {"newton": 0, "two_triangle": 1}
 PRECISION = {"f64": 0, "f32": 1}
 MODE = {"closest": 0, "occluded": 1}
 SCHEDULE = {"wavefront": 0, "simple": 1}
-KEEP_F64 = 1
+KEEP_F64, BUILD_DIRECT = 1, 2
 
 HIT32 = np.dtype([("t", "<f4"), ("st", "<f4", 2), ("bary", "<f4", 2), ("ng", "<f4", 3), ("tri", "<i4"),
                   ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
@@ -215,16 +215,19 @@ class Asset:
     """HeightGrid + TaylorPyramid of one node grid on the device."""
 
     def __init__(self, ctx: Context, nodes: np.ndarray, scale: float = 1.0, offset: float = 0.0,
-                 repeat: bool = False, keep_f64: bool = False):
+                 repeat: bool = False, keep_f64: bool = False, build: str = "fold"):
         v = np.ascontiguousarray(nodes)
         if v.dtype not in _DT:
             v = v.astype(np.float64)
         if v.ndim != 2 or v.shape[0] != v.shape[1]:
             raise ValueError("the node grid must be square")
+        if build not in ("fold", "direct"):
+            raise ValueError("build is 'fold' or 'direct'")
         self.ctx = ctx
         h = C.c_void_p()
+        flags = (KEEP_F64 if keep_f64 else 0) | (BUILD_DIRECT if build == "direct" else 0)
         ctx.check(lib().dmap_asset_create(ctx.h, v.ctypes.data, _DT[v.dtype], v.shape[0], scale, offset, int(repeat),
-                                          KEEP_F64 if keep_f64 else 0, C.byref(h)), "dmap_asset_create")
+                                          flags, C.byref(h)), "dmap_asset_create")
         self.h = h
         self.nodes = v.shape[0]
         self.n_leaf = v.shape[0] - 1
@@ -254,9 +257,11 @@ class Asset:
         return [self.level(l, precision) for l in range(self.n_levels)]
 
     def close(self):
-        if getattr(self, "h", None):
+        # after its context (finalizers at interpreter exit run in any
+        # order) the handle is only forgotten: the process frees the device
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
             lib().dmap_asset_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -282,9 +287,9 @@ class Scene:
         self.n_tri = len(t)
 
     @classmethod
-    def from_synthetic(cls, ctx: Context, scene, keep_f64: bool = False):
+    def from_synthetic(cls, ctx: Context, scene, keep_f64: bool = False, build: str = "fold"):
         """A dmap_b200.scenes.Scene on the device."""
-        assets = [Asset(ctx, a.nodes, a.scale, a.offset, a.repeat, keep_f64) for a in scene.assets]
+        assets = [Asset(ctx, a.nodes, a.scale, a.offset, a.repeat, keep_f64, build) for a in scene.assets]
         return cls(ctx, assets, scene.tris, scene.tri_asset)
 
     def triangle_info(self, tri: int) -> np.ndarray:
@@ -357,9 +362,9 @@ class Scene:
         return img, stats, rec
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
             lib().dmap_scene_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -452,10 +457,10 @@ class Server:
         return {k: getattr(st, k) for k, _ in _ServerStats._fields_}
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
             lib().dmap_server_destroy(self.h)
-            self.h = None
-            self._bufs.clear()
+        self.h = None
+        self._bufs.clear()
 
     def __del__(self):
         try:

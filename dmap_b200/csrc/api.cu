@@ -166,16 +166,26 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaEventCreate(&ev[0]);
     cudaEventCreate(&ev[1]);
+    const bool direct = (flags & DMAP_ASSET_BUILD_DIRECT) != 0;
+    void *hull = nullptr; // the Direct build's slope hulls, 32 B per cell
+    if (direct && (e = cudaMalloc(&hull, (size_t)cells * 32)) != cudaSuccess)
+        return cleanup(cuda_fail(ctx, e, "dmap_asset_create: cudaMalloc"));
     cudaEventRecord(ev[0], ctx->stream);
-    e = dmapk::launch_pyramid(&tmap, d, T, a->pyr64, a->pyr32, ctx->status_dev, ctx->stream,
-                              (flags & DMAP_ASSET_KEEP_F64) != 0);
+    e = direct ? dmapk::launch_pyramid_direct(d, a->pyr64, a->pyr32, hull, ctx->stream,
+                                              (flags & DMAP_ASSET_KEEP_F64) != 0)
+               : dmapk::launch_pyramid(&tmap, d, T, a->pyr64, a->pyr32, ctx->status_dev, ctx->stream,
+                                       (flags & DMAP_ASSET_KEEP_F64) != 0);
     cudaEventRecord(ev[1], ctx->stream);
     if (e != cudaSuccess) {
         cudaEventDestroy(ev[0]);
         cudaEventDestroy(ev[1]);
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(hull);
         return cleanup(cuda_fail(ctx, e, "dmap_asset_create: pyramid launch"));
     }
-    {
+    if (direct) {
+        ctx->launches += 2 * d.n_levels;
+    } else {
         // one leaf launch plus one fold launch per five levels above the tile
         int level = 0, t = T, launches = 1;
         while ((1 << level) * t < n) {
@@ -190,6 +200,7 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
     cudaEventElapsedTime(&a->build_ms, ev[0], ev[1]);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
+    cudaFree(hull);
     if (s != DMAP_OK)
         return cleanup(s);
     if (!(flags & DMAP_ASSET_KEEP_F64)) {

@@ -51,6 +51,11 @@ int walk32_launches(const QueryOpts &opt);
 cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int tile, double *pyr64, float *pyr32,
                            unsigned *status, cudaStream_t stream, bool all64 = true);
 
+// The Direct build (taylor_pyramid.cpp:151-202): every level from the node
+// grid. hull_scratch holds 32 bytes per pyramid cell; 2 launches per level.
+cudaError_t launch_pyramid_direct(const dmapdev::AssetDev &a, double *pyr64, float *pyr32, void *hull_scratch,
+                                  cudaStream_t stream, bool all64);
+
 // Per-triangle setup (setup.cu).
 cudaError_t launch_setup(const double *tris_dev, const int *tri_asset_dev, const dmapdev::AssetDev *assets_dev,
                          int n_tri, dmapdev::TriDev *out, dmapdev::TriDev32 *out32, unsigned *status,

@@ -271,6 +271,143 @@ __global__ void __launch_bounds__(256) pyramid_fold_kernel(AssetDev a, int level
     fold_tile(n, T, level0, tx, ty, a, pyr64, pyr32, smem, all64);
 }
 
+// ---- the Direct build (taylor_pyramid.cpp:151-202) -------------------------
+// Every level from the node grid instead of by folding: a cell's gradient
+// plane is the middle of the hull of its texels' bilinear slopes widened by
+// their twist, and h0, r the middle and half-width of the node residuals
+// against that plane over the cell's (k+1)^2 nodes. Max and min are exact in
+// any order, so the hierarchical and team reductions below give the
+// reference's serial loops' values bit for bit.
+
+__device__ __forceinline__ double direct_value(const AssetDev &a, int j, int i) // V = values * scale
+{
+    size_t k = (size_t)j * a.pitch + i;
+    double v = a.dtype == 0   ? (double)static_cast<const float *>(a.nodes)[k]
+               : a.dtype == 1 ? (double)__half2float(static_cast<const __half *>(a.nodes)[k])
+                              : static_cast<const double *>(a.nodes)[k];
+    return v * a.scale;
+}
+
+// Level 0 of the slope hull: {gu_hi, gu_lo, gv_hi, gv_lo} per texel.
+__global__ void direct_hull_leaf(AssetDev a, double4 *hull)
+{
+    const int n = a.n_leaf;
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * n)
+        return;
+    int i = (int)(t % n), j = (int)(t / n);
+    double v00 = direct_value(a, j, i), v10 = direct_value(a, j, i + 1);
+    double v01 = direct_value(a, j + 1, i), v11 = direct_value(a, j + 1, i + 1);
+    double w = 1.0 / n;
+    double s_texel = 0.5 / n;
+    double c1 = 0.5 * ((v10 - v00) + (v11 - v01)) / w;
+    double c2 = 0.5 * ((v01 - v00) + (v11 - v10)) / w;
+    double c3 = (((v00 - v10) - v01) + v11) / (w * w);
+    double spread = fabs(c3) * s_texel;
+    hull[t] = make_double4(c1 + spread, c1 - spread, c2 + spread, c2 - spread);
+}
+
+// The slope hull one level up (m x m parent cells).
+__global__ void direct_hull_fold(int m, const double4 *child, double4 *parent)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)m * m)
+        return;
+    int I = (int)(t % m), J = (int)(t / m);
+    double4 h = child[(int64_t)(2 * J) * (2 * m) + 2 * I];
+    for (int q = 1; q < 4; ++q) {
+        double4 c = child[(int64_t)(2 * J + (q >> 1)) * (2 * m) + 2 * I + (q & 1)];
+        h.x = dmax(h.x, c.x);
+        h.y = dmin(h.y, c.y);
+        h.z = dmax(h.z, c.z);
+        h.w = dmin(h.w, c.w);
+    }
+    parent[t] = h;
+}
+
+// One level's cells: TEAM threads per cell (1, a warp, or the block).
+template <int TEAM>
+__global__ void __launch_bounds__(256) direct_cells(AssetDev a, int level, const double4 *hull, double *pyr64,
+                                                   float *pyr32, bool all64)
+{
+    const int n = a.n_leaf, k = 1 << level, m = n >> level;
+    int64_t c;
+    int lane;
+    if (TEAM == 1) {
+        c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        lane = 0;
+    } else if (TEAM == 32) {
+        c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        lane = threadIdx.x & 31;
+    } else {
+        c = blockIdx.x;
+        lane = threadIdx.x;
+    }
+    const bool live = c < (int64_t)m * m; // whole teams are live or not
+    double upper = -INFINITY, lower = INFINITY, h_min = INFINITY, h_max = -INFINITY;
+    double gu = 0.0, gv = 0.0, ru = 0.0, rv = 0.0;
+    int I = 0, J = 0;
+    if (live) {
+        I = (int)(c % m);
+        J = (int)(c / m);
+        double4 h = hull[c];
+        gu = 0.5 * (h.x + h.y);
+        ru = 0.5 * (h.x - h.y);
+        gv = 0.5 * (h.z + h.w);
+        rv = 0.5 * (h.z - h.w);
+        const int side = k + 1;
+        for (int idx = lane; idx < side * side; idx += TEAM) {
+            int b = idx / side, aa = idx % side;
+            double dv = (b - 0.5 * k) / n;
+            double du = (aa - 0.5 * k) / n;
+            double value = direct_value(a, J * k + b, I * k + aa);
+            double residual = (value - gu * du) - gv * dv;
+            upper = dmax(upper, residual);
+            lower = dmin(lower, residual);
+            h_min = dmin(h_min, value);
+            h_max = dmax(h_max, value);
+        }
+    }
+    if (TEAM >= 32) {
+        for (int o = 16; o > 0; o >>= 1) {
+            upper = dmax(upper, __shfl_xor_sync(0xffffffffu, upper, o));
+            lower = dmin(lower, __shfl_xor_sync(0xffffffffu, lower, o));
+            h_min = dmin(h_min, __shfl_xor_sync(0xffffffffu, h_min, o));
+            h_max = dmax(h_max, __shfl_xor_sync(0xffffffffu, h_max, o));
+        }
+    }
+    if (TEAM > 32) {
+        __shared__ double red[4][TEAM > 32 ? TEAM / 32 : 1];
+        int wid = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) {
+            red[0][wid] = upper;
+            red[1][wid] = lower;
+            red[2][wid] = h_min;
+            red[3][wid] = h_max;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int q = 1; q < TEAM / 32; ++q) {
+                upper = dmax(upper, red[0][q]);
+                lower = dmin(lower, red[1][q]);
+                h_min = dmin(h_min, red[2][q]);
+                h_max = dmax(h_max, red[3][q]);
+            }
+    }
+    if (live && lane == 0) {
+        Node8 nd;
+        nd.h0 = 0.5 * (upper + lower);
+        nd.gu = gu;
+        nd.gv = gv;
+        nd.r = 0.5 * (upper - lower);
+        nd.ru = ru;
+        nd.rv = rv;
+        nd.mn = h_min;
+        nd.mx = h_max;
+        store_node(nd, a.offset, (size_t)a.level_off[level] + (size_t)c, pyr64, pyr32, all64);
+    }
+}
+
 template <typename In>
 cudaError_t launch_leaf(const void *tmap, const AssetDev &a, int T, double *pyr64, float *pyr32, unsigned *status,
                         bool all64, cudaStream_t stream)
@@ -306,6 +443,35 @@ cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int til
         T = m < kMaxTile ? m : kMaxTile;
         int threads = T * T < 32 ? 32 : T * T;
         pyramid_fold_kernel<<<(m / T) * (m / T), threads, 0, stream>>>(a, level, T, pyr64, pyr32, all64);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_pyramid_direct(const dmapdev::AssetDev &a, double *pyr64, float *pyr32, void *hull_scratch,
+                                  cudaStream_t stream, bool all64)
+{
+    double4 *hull = static_cast<double4 *>(hull_scratch);
+    const int n = a.n_leaf;
+    cudaError_t e;
+    for (int l = 0; l < a.n_levels; ++l) {
+        int m = n >> l;
+        int64_t cells = (int64_t)m * m;
+        double4 *h = hull + a.level_off[l];
+        if (l == 0)
+            direct_hull_leaf<<<(unsigned)((cells + 255) / 256), 256, 0, stream>>>(a, h);
+        else
+            direct_hull_fold<<<(unsigned)((cells + 255) / 256), 256, 0, stream>>>(m, hull + a.level_off[l - 1], h);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+        int k = 1 << l;
+        if (k <= 4)
+            direct_cells<1><<<(unsigned)((cells + 255) / 256), 256, 0, stream>>>(a, l, h, pyr64, pyr32, all64);
+        else if (k <= 64)
+            direct_cells<32><<<(unsigned)((cells * 32 + 255) / 256), 256, 0, stream>>>(a, l, h, pyr64, pyr32, all64);
+        else
+            direct_cells<256><<<(unsigned)cells, 256, 0, stream>>>(a, l, h, pyr64, pyr32, all64);
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
     }

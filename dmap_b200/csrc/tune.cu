@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <fstream>
+#include <iomanip>
 #include <sstream>
 
 using namespace dmapi;
@@ -135,7 +136,7 @@ extern "C" dmap_status dmap_autotune(dmap_scene *s, const void *rays_dev, dmap_d
         *best_ms = t_best;
     if (cache_path) {
         std::ofstream f(cache_path, std::ios::app);
-        f << key << " " << r_best << " " << b_best << " " << t_best << "\n";
+        f << std::setprecision(17) << key << " " << r_best << " " << b_best << " " << t_best << "\n";
     }
     return DMAP_OK;
 }

@@ -57,6 +57,9 @@ int64_t dmap_kernel_launches(const dmap_context *ctx);
 
 /* Asset flags. */
 #define DMAP_ASSET_KEEP_F64 1u /* keep the FP64 pyramid resident (needed by DMAP_PRECISION_F64) */
+/* build every level from the node grid (PyramidBuild::Direct, taylor_pyramid.cpp:151-202:
+ * tighter r than the default fold, about twice the work) */
+#define DMAP_ASSET_BUILD_DIRECT 2u
 
 /*
  * Uploads a (nodes x nodes) node grid, nodes = 2^L + 1, row major with

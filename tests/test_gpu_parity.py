@@ -126,3 +126,36 @@ def test_f64_occluded_matches_closest(sphere_pair):
     closest = dev.intersect(rays, dm.TraversalOptions(precision="f64"))
     occl = dev.intersect(rays, dm.TraversalOptions(precision="f64", mode="occluded"))
     assert np.array_equal(closest["tri"] >= 0, occl["tri"] >= 0)
+
+
+@pytest.mark.parametrize("n,dtype,scale,offset", [(65, np.float32, 1.0, 0.0), (129, np.float16, 0.7, -0.2),
+                                                  (257, np.float64, 0.013, 0.5)])
+def test_device_direct_pyramid_equals_oracle(ctx, oracle, n, dtype, scale, offset):
+    """The Direct build (every level from the node grid) == the oracle's,
+    bit for bit, in FP64; the FP32 levels enclose them."""
+    rng = np.random.default_rng(5)
+    v = rng.random((n, n)).astype(dtype)
+    a = dm.Asset(ctx, v, scale, offset, keep_f64=True, build="direct")
+    ref = oracle.pyramid(v.astype(np.float64), scale, offset, build="direct")
+    assert a.n_levels == len(ref)
+    for k, lv in enumerate(ref):
+        got = a.level(k, "f64")
+        for ch in CHANNELS:
+            assert np.array_equal(got[ch], lv[ch]), (k, ch)
+        f = a.level(k, "f32")
+        assert (f["h_min"] <= lv["h_min"]).all() and (f["h_max"] >= lv["h_max"]).all()
+
+
+def test_direct_build_walk_equals_oracle(ctx, oracle):
+    """A scene on Direct-built pyramids: the FP64 and FP32 paths' hits == the
+    oracle's on the same build."""
+    sc = scenes.quad_scene(64)
+    cpu = py_oracle.CpuScene(oracle, sc, build="direct")
+    dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=True, build="direct")
+    rays = np.concatenate([scenes.quad_camera_rays(48, 48), helpers.near_surface_rays(cpu, 1500)])
+    _compare(cpu, dev, rays)
+    ho, _ = cpu.intersect(rays)
+    h32 = dev.intersect(rays, dm.TraversalOptions(precision="f32"), np.float64)
+    assert np.array_equal(h32["tri"], ho[:, 10].astype(np.int32))
+    hit = ho[:, 10] >= 0
+    assert np.array_equal(h32["t"][hit], ho[hit, 0])
