@@ -168,7 +168,7 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
     cudaEventCreate(&ev[1]);
     const bool direct = (flags & DMAP_ASSET_BUILD_DIRECT) != 0;
     void *hull = nullptr; // the Direct build's slope hulls, 32 B per cell
-    if (direct && (e = cudaMalloc(&hull, (size_t)cells * 32)) != cudaSuccess)
+    if (direct && (e = cudaMalloc(&hull, ((size_t)cells + 32768) * 32)) != cudaSuccess)
         return cleanup(cuda_fail(ctx, e, "dmap_asset_create: cudaMalloc"));
     cudaEventRecord(ev[0], ctx->stream);
     e = direct ? dmapk::launch_pyramid_direct(d, a->pyr64, a->pyr32, hull, ctx->stream,
@@ -184,7 +184,7 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
         return cleanup(cuda_fail(ctx, e, "dmap_asset_create: pyramid launch"));
     }
     if (direct) {
-        ctx->launches += 2 * d.n_levels;
+        ctx->launches += dmapk::direct_launches(n);
     } else {
         // one leaf launch plus one fold launch per five levels above the tile
         int level = 0, t = T, launches = 1;

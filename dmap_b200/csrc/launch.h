@@ -52,7 +52,9 @@ cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int til
                            unsigned *status, cudaStream_t stream, bool all64 = true);
 
 // The Direct build (taylor_pyramid.cpp:151-202): every level from the node
-// grid. hull_scratch holds 32 bytes per pyramid cell; 2 launches per level.
+// grid. hull_scratch holds 32 bytes per pyramid cell plus 32768 x 32 bytes
+// of partial hulls; 2 or 3 launches per level (direct_launches).
+int direct_launches(int n_leaf);
 cudaError_t launch_pyramid_direct(const dmapdev::AssetDev &a, double *pyr64, float *pyr32, void *hull_scratch,
                                   cudaStream_t stream, bool all64);
 

@@ -18,6 +18,7 @@
 #include "dmap_b200.h"
 #include "device_types.cuh"
 #include "launch.h"
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cuda.h>
@@ -27,6 +28,7 @@ namespace
 {
 using dmapdev::AssetDev;
 
+constexpr int64_t kDirectPartials = 32768; // partial hulls after the cells' slope hulls in the Direct scratch
 constexpr int kMaxTile = 16;  // 256 threads per CTA: the FP64 fold keeps its registers
 constexpr int kTilePitch = 24; // staged row pitch bound in elements (>= 17, TMA box inner extent rounded to 16 B)
 
@@ -408,6 +410,81 @@ __global__ void __launch_bounds__(256) direct_cells(AssetDev a, int level, const
     }
 }
 
+// Coarse levels have few cells of many nodes: each cell's node rows are cut
+// into `chunks` pieces, one block each, whose partial hulls (upper, lower,
+// h_min, h_max) a second kernel reduces and stores.
+__global__ void __launch_bounds__(256) direct_cells_partial(AssetDev a, int level, const double4 *hull, int chunks,
+                                                            double4 *partial)
+{
+    const int n = a.n_leaf, k = 1 << level, m = n >> level, side = k + 1;
+    const int64_t c = blockIdx.x / chunks;
+    const int piece = blockIdx.x % chunks;
+    const int I = (int)(c % m), J = (int)(c / m);
+    double4 h = hull[c];
+    double gu = 0.5 * (h.x + h.y), gv = 0.5 * (h.z + h.w);
+    int r0 = (int)((int64_t)side * piece / chunks), r1 = (int)((int64_t)side * (piece + 1) / chunks);
+    double upper = -INFINITY, lower = INFINITY, h_min = INFINITY, h_max = -INFINITY;
+    for (int b = r0; b < r1; ++b) {
+        double dv = (b - 0.5 * k) / n;
+        for (int aa = threadIdx.x; aa < side; aa += blockDim.x) {
+            double du = (aa - 0.5 * k) / n;
+            double value = direct_value(a, J * k + b, I * k + aa);
+            double residual = (value - gu * du) - gv * dv;
+            upper = dmax(upper, residual);
+            lower = dmin(lower, residual);
+            h_min = dmin(h_min, value);
+            h_max = dmax(h_max, value);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        upper = dmax(upper, __shfl_xor_sync(0xffffffffu, upper, o));
+        lower = dmin(lower, __shfl_xor_sync(0xffffffffu, lower, o));
+        h_min = dmin(h_min, __shfl_xor_sync(0xffffffffu, h_min, o));
+        h_max = dmax(h_max, __shfl_xor_sync(0xffffffffu, h_max, o));
+    }
+    __shared__ double4 red[8];
+    if ((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = make_double4(upper, lower, h_min, h_max);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+            upper = dmax(upper, red[q].x);
+            lower = dmin(lower, red[q].y);
+            h_min = dmin(h_min, red[q].z);
+            h_max = dmax(h_max, red[q].w);
+        }
+        partial[blockIdx.x] = make_double4(upper, lower, h_min, h_max);
+    }
+}
+
+__global__ void direct_cells_final(AssetDev a, int level, const double4 *hull, int chunks, const double4 *partial,
+                                   double *pyr64, float *pyr32, bool all64)
+{
+    const int m = a.n_leaf >> level;
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int64_t)m * m)
+        return;
+    double4 p = partial[c * chunks];
+    for (int q = 1; q < chunks; ++q) {
+        double4 x = partial[c * chunks + q];
+        p.x = dmax(p.x, x.x);
+        p.y = dmin(p.y, x.y);
+        p.z = dmin(p.z, x.z);
+        p.w = dmax(p.w, x.w);
+    }
+    double4 h = hull[c];
+    Node8 nd;
+    nd.h0 = 0.5 * (p.x + p.y);
+    nd.gu = 0.5 * (h.x + h.y);
+    nd.gv = 0.5 * (h.z + h.w);
+    nd.r = 0.5 * (p.x - p.y);
+    nd.ru = 0.5 * (h.x - h.y);
+    nd.rv = 0.5 * (h.z - h.w);
+    nd.mn = p.z;
+    nd.mx = p.w;
+    store_node(nd, a.offset, (size_t)a.level_off[level] + (size_t)c, pyr64, pyr32, all64);
+}
+
 template <typename In>
 cudaError_t launch_leaf(const void *tmap, const AssetDev &a, int T, double *pyr64, float *pyr32, unsigned *status,
                         bool all64, cudaStream_t stream)
@@ -449,11 +526,22 @@ cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int til
     return cudaSuccess;
 }
 
+int direct_launches(int n_leaf)
+{
+    int c = 0;
+    for (int l = 0; (1 << l) <= n_leaf; ++l)
+        c += ((1 << l) <= 64 || (int64_t)(n_leaf >> l) * (n_leaf >> l) >= 2048) ? 2 : 3;
+    return c;
+}
+
 cudaError_t launch_pyramid_direct(const dmapdev::AssetDev &a, double *pyr64, float *pyr32, void *hull_scratch,
                                   cudaStream_t stream, bool all64)
 {
     double4 *hull = static_cast<double4 *>(hull_scratch);
     const int n = a.n_leaf;
+    int64_t total_cells = 0;
+    for (int l = 0; l < a.n_levels; ++l)
+        total_cells += (int64_t)(n >> l) * (n >> l);
     cudaError_t e;
     for (int l = 0; l < a.n_levels; ++l) {
         int m = n >> l;
@@ -466,12 +554,23 @@ cudaError_t launch_pyramid_direct(const dmapdev::AssetDev &a, double *pyr64, flo
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
         int k = 1 << l;
-        if (k <= 4)
+        if (k <= 4) {
             direct_cells<1><<<(unsigned)((cells + 255) / 256), 256, 0, stream>>>(a, l, h, pyr64, pyr32, all64);
-        else if (k <= 64)
+        } else if (k <= 64) {
             direct_cells<32><<<(unsigned)((cells * 32 + 255) / 256), 256, 0, stream>>>(a, l, h, pyr64, pyr32, all64);
-        else
+        } else if (cells >= 2048) {
             direct_cells<256><<<(unsigned)cells, 256, 0, stream>>>(a, l, h, pyr64, pyr32, all64);
+        } else {
+            // about 2048 blocks per level, at least one node row each
+            int64_t chunks = std::min<int64_t>((2048 + cells - 1) / cells, k + 1);
+            chunks = std::min<int64_t>(chunks, kDirectPartials / cells);
+            double4 *partial = hull + total_cells;
+            direct_cells_partial<<<(unsigned)(cells * chunks), 256, 0, stream>>>(a, l, h, (int)chunks, partial);
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+            direct_cells_final<<<(unsigned)((cells + 255) / 256), 256, 0, stream>>>(a, l, h, (int)chunks, partial,
+                                                                                  pyr64, pyr32, all64);
+        }
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
     }
