@@ -85,6 +85,10 @@ class _RayRecord(C.Structure):
                 ("t", C.c_void_p), ("count", C.c_int64)]
 
 
+class _UvMap(C.Structure):
+    _fields_ = [("uv_scale", C.c_double * 2), ("uv_offset", C.c_double * 2), ("flip_v", C.c_int)]
+
+
 class _ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch_rays", C.c_int64), ("max_inflight", C.c_int),
                 ("slots", C.c_int), ("options", _Options)]
@@ -132,6 +136,8 @@ def lib() -> C.CDLL:
                                   C.POINTER(_RayRecord)]),
             "dmap_autotune": (i32, [vp, vp, i32, i64, C.POINTER(_Options), C.c_char_p, C.POINTER(_Options),
                                     C.POINTER(dbl)]),
+            "dmap_surface_points": (i32, [vp, vp, i32, i64, C.POINTER(_UvMap), vp, vp]),
+            "dmap_surface_points_host": (i32, [vp, vp, i32, i64, C.POINTER(_UvMap), vp]),
             "dmap_server_create": (i32, [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]),
             "dmap_server_destroy": (None, [vp]),
             "dmap_server_submit_rays": (i32, [vp, vp, vp, i64, i32, vp, C.POINTER(C.c_uint64)]),
@@ -320,6 +326,17 @@ class Scene:
         opt = (options or TraversalOptions()).c()
         self.ctx.check(lib().dmap_intersect(self.h, rays_ptr, ray_dtype, n, C.byref(opt), hits_ptr, hit_dtype,
                                             stats_ptr or None, stream or None), "dmap_intersect")
+
+    def surface_points(self, hits: np.ndarray, uv_scale=(1.0, 1.0), uv_offset=(0.0, 0.0), flip_v: bool = False):
+        """DisplacedGeometry::surface_point for every hit record (HIT32 or
+        HIT64 array): (n, 14) doubles p, ng, dpdu, dpdv, uv; zeros for misses."""
+        h = np.ascontiguousarray(hits)
+        dt = F64 if h.dtype == HIT64 else F32
+        out = np.empty((len(h), 14))
+        m = _UvMap((C.c_double * 2)(*uv_scale), (C.c_double * 2)(*uv_offset), int(flip_v))
+        self.ctx.check(lib().dmap_surface_points_host(self.h, h.ctypes.data, dt, len(h), C.byref(m),
+                                                      out.ctypes.data), "dmap_surface_points_host")
+        return out
 
     def autotune(self, rays_ptr: int, ray_dtype: int, n: int, base: Optional[TraversalOptions] = None,
                  cache_path: Optional[str] = None):

@@ -1,7 +1,8 @@
 """Builds libdmap_b200.so in place: every CUDA source for sm_100a with nvcc.
 
 The translation units with FP64 arithmetic that must round like the
-reference (pyramid.cu, setup.cu, walk64.cu, and walk32.cu for its FP64 leaf)
+reference (pyramid.cu, setup.cu, walk64.cu, walk32.cu for its FP64 leaf,
+shade.cu)
 are compiled with -fmad=false so that each double operation rounds on its
 own, as the reference's CPU build does; FP32 code there asks for fused
 multiply-adds explicitly (fmaf, __fmaf_ru).
@@ -24,7 +25,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libdmap_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-I", str(CSRC)]
-EXACT_FP64 = {"pyramid.cu", "setup.cu", "walk64.cu", "walk32.cu"}
+EXACT_FP64 = {"pyramid.cu", "setup.cu", "walk64.cu", "walk32.cu", "shade.cu"}
 
 
 def nvcc() -> str:

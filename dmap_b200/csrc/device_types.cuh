@@ -42,6 +42,7 @@ struct TriDev
     double J[2][2];
     double A[3][3]; // to_tangent
     double ng[3];
+    double wn[3];           // winding normal (p1 - p0) x (p2 - p0)
     double un[3][2], ud[3]; // inward edge normals and offsets
     double lo[2], hi[2];    // texture-space bounding box of the domain
     double residual_tol;

@@ -59,6 +59,8 @@ __device__ bool init_triangle(TriDev &T, const double *r)
     v2 t0 = L2(r + 18), t1 = L2(r + 20), t2 = L2(r + 22);
     T.t0[0] = t0.x, T.t0[1] = t0.y, T.t1[0] = t1.x, T.t1[1] = t1.y, T.t2[0] = t2.x, T.t2[1] = t2.y;
     v3 eb1 = sub3(p1, p0), eb2 = sub3(p2, p0), Mb1 = sub3(m1, m0), Mb2 = sub3(m2, m0);
+    v3 wn = cross3(eb1, eb2); // winding_normal (displaced_surface.cpp:158)
+    T.wn[0] = wn.x, T.wn[1] = wn.y, T.wn[2] = wn.z;
     double T00 = t1.x - t0.x, T10 = t1.y - t0.y, T01 = t2.x - t0.x, T11 = t2.y - t0.y;
     double det = T00 * T11 - T10 * T01;
     if (!(fabs(det) > 1e-30))

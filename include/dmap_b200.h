@@ -221,6 +221,26 @@ dmap_status dmap_intersect_host(dmap_scene *scene, const void *rays_host, dmap_d
                                 const dmap_options *opt, void *hits_host, dmap_dtype hit_dtype, int64_t *stats_host);
 
 /*
+ * Hit records to surface points: DisplacedGeometry::surface_point
+ * (displaced_geometry.cpp:126-152), the step from a hit to the shading
+ * record, for every hit at once. Per hit (tri, bary = the base triangle's
+ * barycentrics u, v) 14 doubles: the displaced position p, the geometric
+ * normal ng (oriented along the base face's winding (p1 - p0) x (p2 - p0),
+ * unit), dpdu and dpdv (the surface tangents along the chart, scaled by the
+ * object's uv map), and the object uv (DisplacedObject::object_uv,
+ * scene_spec.cpp:382-388). Misses (tri < 0) give zeros. map NULL = identity.
+ */
+typedef struct dmap_uv_map {
+    double uv_scale[2], uv_offset[2]; /* tile coordinates = uv * uv_scale + uv_offset */
+    int flip_v;                       /* v' = 1 - v */
+} dmap_uv_map;
+dmap_status dmap_surface_points(dmap_scene *scene, const void *hits_dev, dmap_dtype hit_dtype, int64_t n,
+                                const dmap_uv_map *map, double *out_dev, void *stream);
+/* The same on host buffers (synchronous). */
+dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, dmap_dtype hit_dtype, int64_t n,
+                                     const dmap_uv_map *map, double *out_host);
+
+/*
  * Schedule autotuner (no counterpart in the reference). Times the wavefront
  * schedule's launch shapes (rounds x blocks_per_sm) with `base`'s other
  * options on the first min(n, 2^22) of the caller's device rays and returns

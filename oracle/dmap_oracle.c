@@ -1632,3 +1632,42 @@ void o_triangle_param(const o_scene *s, int tri, double u, double v, double *out
     out[0] = p.x;
     out[1] = p.y;
 }
+
+/* DisplacedGeometry::surface_point (displaced_geometry.cpp:126-152) on
+ * triangle tri at barycentrics (u, v), with the object's uv map
+ * (DisplacedObject::object_uv, scene_spec.cpp:382-388): out14 = p, ng, dpdu,
+ * dpdv, uv. Eigen's normalize() leaves a zero vector as it is. */
+static v3 eigen_normalized(v3 a)
+{
+    double z = dot3(a, a);
+    return z > 0.0 ? div3(a, sqrt(z)) : a;
+}
+
+void o_surface_point(const o_scene *s, int tri, double u, double v, const double *uv_scale, const double *uv_offset,
+                     int flip_v, double *out)
+{
+    const o_isect *X = find_tri(s, tri, NULL);
+    const o_tri *T = X->tri;
+    v2 st = tri_param(T, u, v);
+    double sp = st.x, tp = st.y;
+    o_nframe f = normal_frame_at(T, sp, tp);
+    double h = grid_h(X->field, sp, tp);
+    v2 gh = grid_grad(X->field, sp, tp);
+    v3 Ss = add3(add3(T->e1, mul3(gh.x, f.N)), mul3(h, f.Nu));
+    v3 St = add3(add3(T->e2, mul3(gh.y, f.N)), mul3(h, f.Nv));
+    v3 p = add3(tri_P(T, sp, tp), mul3(h, f.N));
+    v3 wn = cross3(sub3(T->p1, T->p0), sub3(T->p2, T->p0));
+    v3 ng = cross3(Ss, St);
+    if (dot3(ng, wn) < 0.0)
+        ng = V3(-ng.x, -ng.y, -ng.z);
+    ng = eigen_normalized(ng);
+    if (!(isfinite(ng.x) && isfinite(ng.y) && isfinite(ng.z)))
+        ng = eigen_normalized(wn);
+    double su = uv_scale[0], sv = flip_v ? -uv_scale[1] : uv_scale[1];
+    v3 dpdu = mul3(su, Ss), dpdv = mul3(sv, St);
+    double uvx = (sp - uv_offset[0]) / uv_scale[0], uvy = (tp - uv_offset[1]) / uv_scale[1];
+    if (flip_v)
+        uvy = 1.0 - uvy;
+    double o[14] = {p.x, p.y, p.z, ng.x, ng.y, ng.z, dpdu.x, dpdu.y, dpdu.z, dpdv.x, dpdv.y, dpdv.z, uvx, uvy};
+    memcpy(out, o, sizeof(o));
+}

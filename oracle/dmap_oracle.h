@@ -99,6 +99,10 @@ void o_node_bound(const o_scene *s, int tri, int level, int64_t i, int64_t j, co
 void o_displaced_position(const o_scene *s, int tri, double sp, double tp, double *out3);
 /* BaseTriangle::param (displaced_surface.h:304). */
 void o_triangle_param(const o_scene *s, int tri, double u, double v, double *out2);
+/* DisplacedGeometry::surface_point (displaced_geometry.cpp:126-152) with the
+ * object's uv map: out14 = p, ng, dpdu, dpdv, uv. */
+void o_surface_point(const o_scene *s, int tri, double u, double v, const double *uv_scale, const double *uv_offset,
+                     int flip_v, double *out14);
 
 #ifdef __cplusplus
 }

@@ -75,6 +75,8 @@ class _Lib:
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
                                _dp, _lp, _lp, C.c_int)
             self._param = f("triangle_param", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp)
+            self._surf = f("surface_point", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp, _dp, C.c_int,
+                           _dp)
         else:
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
                                _dp, _lp, C.c_int)
@@ -173,4 +175,13 @@ class CpuScene:
     def displaced_position(self, tri, s, t):
         out = np.empty(3)
         self.lib._disp(self.h, tri, s, t, _ptr(out))
+        return out
+
+    def surface_point(self, tri, u, v, uv_scale=(1.0, 1.0), uv_offset=(0.0, 0.0), flip_v=False):
+        """DisplacedGeometry::surface_point at barycentrics (u, v): 14 values
+        p, ng, dpdu, dpdv, uv (C oracle only)."""
+        out = np.empty(14)
+        sc = np.array(uv_scale, np.float64)
+        of = np.array(uv_offset, np.float64)
+        self.lib._surf(self.h, tri, u, v, _ptr(sc), _ptr(of), int(flip_v), _ptr(out))
         return out
