@@ -4,6 +4,8 @@
 // walk64.cu and walk32.cu.
 #include "api_internal.h"
 
+#include <algorithm>
+
 using namespace dmapi;
 
 extern "C" {
@@ -296,6 +298,7 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
         cudaFree(s->assets_dev);
         cudaFree(s->tris_dev);
         cudaFree(s->tris32_dev);
+        cudaFree(s->block_box_dev);
         delete s;
         return st;
     };
@@ -317,6 +320,28 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
     dmap_status st = sync_and_check(ctx, "dmap_scene_create");
     if (st != DMAP_OK)
         return cleanup(st);
+    if (n_tri > 256) {
+        // the object box of each block of 32 consecutive triangles, from the
+        // outward FP32 boxes the walk tests
+        std::vector<TriDev32> t32(n_tri);
+        if ((e = cudaMemcpy(t32.data(), s->tris32_dev, sizeof(TriDev32) * n_tri, cudaMemcpyDeviceToHost)))
+            return cleanup(cuda_fail(ctx, e, "dmap_scene_create: readback"));
+        int nb = (n_tri + 31) / 32;
+        std::vector<float> bb((size_t)6 * nb);
+        for (int b = 0; b < nb; ++b)
+            for (int a3 = 0; a3 < 3; ++a3) {
+                float lo = INFINITY, hi = -INFINITY;
+                for (int k = 32 * b; k < std::min(n_tri, 32 * b + 32); ++k) {
+                    lo = std::min(lo, t32[k].box_lo[a3]);
+                    hi = std::max(hi, t32[k].box_hi[a3]);
+                }
+                bb[6 * b + a3] = lo;
+                bb[6 * b + 3 + a3] = hi;
+            }
+        if ((e = cudaMalloc((void **)&s->block_box_dev, sizeof(float) * bb.size())) ||
+            (e = cudaMemcpy(s->block_box_dev, bb.data(), sizeof(float) * bb.size(), cudaMemcpyHostToDevice)))
+            return cleanup(cuda_fail(ctx, e, "dmap_scene_create: block boxes"));
+    }
     s->tris_host.resize(n_tri);
     if ((e = cudaMemcpy(s->tris_host.data(), s->tris_dev, sizeof(TriDev) * n_tri, cudaMemcpyDeviceToHost)))
         return cleanup(cuda_fail(ctx, e, "dmap_scene_create: readback"));
@@ -337,6 +362,7 @@ void dmap_scene_destroy(dmap_scene *s)
     cudaFree(s->assets_dev);
     cudaFree(s->tris_dev);
     cudaFree(s->tris32_dev);
+    cudaFree(s->block_box_dev);
     delete s;
 }
 
@@ -388,6 +414,7 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.schedule = o.schedule;
     q.rounds = o.rounds;
     q.blocks_per_sm = o.blocks_per_sm;
+    q.block_box = s->block_box_dev;
     return DMAP_OK;
 }
 

@@ -61,6 +61,7 @@ struct dmap_scene
     AssetDev *assets_dev = nullptr;
     TriDev *tris_dev = nullptr;
     TriDev32 *tris32_dev = nullptr;
+    float *block_box_dev = nullptr; // more than 256 triangles: boxes of blocks of 32 (QueryOpts::block_box)
     std::vector<TriDev> tris_host;
     bool all_f64 = true;
 };

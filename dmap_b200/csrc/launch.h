@@ -22,6 +22,9 @@ struct QueryOpts
     // runs (at most the n the launch is given, which sizes grids and scratch):
     // stages of a device-driven pipeline pass counts they produced themselves.
     const long long *n_dev = nullptr;
+    // Scenes of more than 256 triangles: the object box of every block of 32
+    // consecutive triangles (6 floats, outward), for the walk's candidate mask.
+    const float *block_box = nullptr;
 };
 
 constexpr int kMaxRounds = 32;

@@ -228,6 +228,7 @@ struct dmap_server
             // one query over the whole batch
             dmapk::QueryOpts qq = q;
             qq.mode = first->mode;
+            qq.block_box = first->scene->block_box_dev;
             qq.ray_dtype = qq.hit_dtype = 0;
             dmap_scene *s = first->scene;
             if (e == cudaSuccess)

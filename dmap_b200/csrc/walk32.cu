@@ -63,15 +63,15 @@ constexpr unsigned FULL = 0xffffffffu;
 // the caller's): where the exact ray is inside the box, |t d| <= |o| + |box|,
 // so the float ray is within u (2|o| + |box|) of it. On a pass t1 is the
 // exit parameter, rounded up.
-__device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, const float *df, const float *invf,
-                                           float t0, float &t1)
+__device__ __forceinline__ bool box_pass(const float *box_lo, const float *box_hi, const float *of, const float *df,
+                                         const float *invf, float t0, float &t1)
 {
     bool ok = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float bmag = fmaxf(fabsf(T.box_lo[a]), fabsf(T.box_hi[a]));
+        float bmag = fmaxf(fabsf(box_lo[a]), fabsf(box_hi[a]));
         float pad = ru_mul(2.0f * G, ru_add(ru_fma(2.0f, fabsf(of[a]), bmag), 1.0f));
-        float lo = __fsub_rd(T.box_lo[a], pad), hi = __fadd_ru(T.box_hi[a], pad);
+        float lo = __fsub_rd(box_lo[a], pad), hi = __fadd_ru(box_hi[a], pad);
         if (df[a] != 0.0f) {
             float ta = (lo - of[a]) * invf[a], tb = (hi - of[a]) * invf[a];
             t0 = fmaxf(t0, fminf(ta, tb));
@@ -81,6 +81,12 @@ __device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, c
         }
     }
     return ok && !(t0 > t1 + tol32(fmaxf(fabsf(t0), fabsf(t1))));
+}
+
+__device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, const float *df, const float *invf,
+                                           float t0, float &t1)
+{
+    return box_pass(T.box_lo, T.box_hi, of, df, invf, t0, t1);
 }
 
 // The tangent-space ray of a triangle: transformed in double, rounded to
@@ -274,7 +280,7 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // One lane's walk from its parked or fresh state to the next leaf (parked,
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
-template <bool ST, bool INLINE_LEAF, typename R, typename H, typename Fp>
+template <bool ST, bool INLINE_LEAF, bool BLOCKS, typename R, typename H, typename Fp>
 __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
@@ -284,7 +290,12 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
 {
     enum : int { NEED = 0, TOP = 1, WALK = 2, DONE = 3 };
     const int lane = threadIdx.x & 31;
-    const bool use_mask = n_tri <= 32 * kMaskWords;
+    // the candidate mask: one bit per triangle (up to 256 triangles), or
+    // (BLOCKS) one bit per block of 32 consecutive triangles (up to 8192),
+    // visited in order
+    constexpr bool use_blocks = BLOCKS;
+    const bool use_mask = BLOCKS || n_tri <= 32 * kMaskWords;
+    const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
     if (round == 0 && opt.n_dev && (unsigned long long)*opt.n_dev < count)
@@ -427,7 +438,10 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 for (int w = 0; w < kMaskWords; ++w) {
                     int t = 32 * w + lane;
                     float t1 = s_tmax;
-                    bool pass = t < n_tri && object_box(tris32[t], so, sd, sv, s_tmin, t1);
+                    bool pass = t < n_items &&
+                                (use_blocks ? box_pass(opt.block_box + 6 * t, opt.block_box + 6 * t + 3, so, sd, sv,
+                                                       s_tmin, t1)
+                                            : object_box(tris32[t], so, sd, sv, s_tmin, t1));
                     unsigned bits = __ballot_sync(FULL, pass);
                     if (lane == src) {
 #pragma unroll
@@ -444,7 +458,34 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
         if (phase == TOP) {
             float t1 = 0.0f;
             bool hit_box = false;
-            if (use_mask) {
+            if (use_blocks) {
+                // the next block whose box the ray met, then its triangles in order
+                while (tri < n_tri) {
+                    int blk = tri >> 5, w = blk >> 5;
+                    unsigned bits = mask[0];
+#pragma unroll
+                    for (int q = 1; q < kMaskWords; ++q)
+                        bits = w == q ? mask[q] : bits;
+                    bits &= ~0u << (blk & 31);
+                    if (!bits) {
+                        tri = (w + 1) << 10;
+                        continue;
+                    }
+                    int nb = (w << 5) + __ffs(bits) - 1;
+                    if (nb != blk)
+                        tri = nb << 5;
+                    const int stop = min(n_tri, (nb + 1) << 5);
+                    for (; tri < stop; ++tri) {
+                        t1 = __double2float_ru(t_max);
+                        if (object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
+                            hit_box = true;
+                            break;
+                        }
+                    }
+                    if (hit_box)
+                        break;
+                }
+            } else if (use_mask) {
                 while (tri < n_tri) {
                     int w = tri >> 5;
                     unsigned bits = mask[0];
@@ -863,25 +904,25 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
         const int *q_in = ws.queue[(rd + 1) & 1];
         int *q_out = ws.queue[rd & 1];
         bool last = rd == rounds;
+        // the block mask has its own instances so that scenes of up to 256
+        // triangles keep the smaller kernel
+        const bool blocks = n_tri > 32 * kMaskWords && opt.block_box && n_tri <= 32 * 32 * kMaskWords;
+#define DMAP_WALK_LAUNCH(ST_, IL_, BL_)                                                                             \
+    wave_walk<ST_, IL_, BL_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,           \
+                                                                 ST_ ? stats : nullptr, states, q_in, rd, leaves, \
+                                                                 ws.counters, status)
         if (stats) {
             if (last)
-                wave_walk<true, true, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
-                                                                          stats, states, q_in, rd, leaves,
-                                                                          ws.counters, status);
+                blocks ? DMAP_WALK_LAUNCH(true, true, true) : DMAP_WALK_LAUNCH(true, true, false);
             else
-                wave_walk<true, false, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
-                                                                           stats, states, q_in, rd, leaves,
-                                                                           ws.counters, status);
+                blocks ? DMAP_WALK_LAUNCH(true, false, true) : DMAP_WALK_LAUNCH(true, false, false);
         } else {
             if (last)
-                wave_walk<false, true, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,
-                                                                           nullptr, states, q_in, rd, leaves,
-                                                                           ws.counters, status);
+                blocks ? DMAP_WALK_LAUNCH(false, true, true) : DMAP_WALK_LAUNCH(false, true, false);
             else
-                wave_walk<false, false, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt,
-                                                                            hh, nullptr, states, q_in, rd, leaves,
-                                                                            ws.counters, status);
+                blocks ? DMAP_WALK_LAUNCH(false, false, true) : DMAP_WALK_LAUNCH(false, false, false);
         }
+#undef DMAP_WALK_LAUNCH
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
         if (last)

@@ -119,3 +119,20 @@ def test_f32_grazing_rays_f16(ctx, oracle):
     rays = np.concatenate([scenes.grazing_rays(p, m, seed=79), scenes.grazing_rays(S, nrm, seed=80)])
     n, _ = _check(cpu, dev, rays)
     assert n > 1000
+
+
+@pytest.mark.parametrize("n,k", [(16, 8), (8, 24)])
+def test_f32_many_triangles_block_mask(ctx, oracle, n, k):
+    """Scenes of more than 256 triangles (768 and 6912) take the per-ray mask
+    of 32-triangle blocks; hits equal the oracle's flat loop and the simple
+    schedule's."""
+    sc = scenes.cube_sphere_scene(n, k)
+    assert len(sc.tris) > 256
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 1500),
+                           helpers.aimed_rays(cpu, 1500)[0]])
+    n_hit, _ = _check(cpu, dev, rays)
+    assert n_hit > 1000
+    a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront"), np.float64)
+    b = dev.intersect(rays, dm.TraversalOptions(schedule="simple"), np.float64)
+    assert a.tobytes() == b.tobytes()
