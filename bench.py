@@ -247,7 +247,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dmap", choices=["dmap", "reference"])
     ap.add_argument("--config", default="sphere",
-                    choices=["sphere", "sphere16", "quad", "pathtrace", "serve", "pyramid"])
+                    choices=["sphere", "sphere16", "quad", "pathtrace", "serve", "pyramid", "tessellate"])
     ap.add_argument("--requests", type=int, default=4096, help="serve: requests in the arrival trace")
     ap.add_argument("--interarrival-ms", type=float, default=15.0, help="serve: mean Poisson inter-arrival time")
     ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-request comparison")
@@ -287,6 +287,9 @@ def main():
         return
     if args.config == "pyramid":
         run_pyramid(args, rank, world, local, dist)
+        return
+    if args.config == "tessellate":
+        run_tessellate(args, rank, world, local, dist)
         return
 
     t_setup = time.perf_counter()
@@ -536,6 +539,99 @@ def run_pyramid(args, rank, world, local, dist):
                          "kernel": "pyramid_leaf_kernel + folds" if args.build == "fold"
                          else "direct_hull_* + direct_cells",
                          "bytes_per_map": byts / len(sc.assets)}}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_tessellate(args, rank, world, local, dist):
+    """The oracle meshes: the texel-aligned tessellation (m = 1, the
+    two-triangle leaf's surface) of 4 cube-sphere patches (8 base
+    triangles over 2048^2 FP32 maps), through dmap_tessellate_texel on
+    device buffers; a step is one whole call (count, scan, emit). The
+    uniform tessellation of all 192 triangles at n = 256 is timed beside it.
+    Algorithmic bytes: what the mesh holds, 152 B per face (9 + 6 + 9 floats
+    and the 56-byte TexelFace record); the map reads are a few MB."""
+    import ctypes as C
+    import torch
+    import dmap_b200 as dm
+    sc_all, _ = build_scene("sphere", args.small)
+    sub = scenes.Scene(sc_all.assets[:4], sc_all.tris[:8], sc_all.tri_asset[:8], name="4 patches")
+    ctx = dm.Context(local)
+    dev = dm.Scene.from_synthetic(ctx, sub)
+    L = dm.lib()
+    stream = torch.cuda.Stream()   # a stream of its own, so the events and the library's kernels share it
+    sp = C.c_void_p(stream.cuda_stream)
+    nf = C.c_int64()
+    ctx.check(L.dmap_tessellate_texel(dev.h, 1, 0, None, None, None, None, C.byref(nf), sp), "count")
+    F = nf.value
+    pos = torch.empty(F * 9, dtype=torch.float32, device="cuda")
+    uv = torch.empty(F * 6, dtype=torch.float32, device="cuda")
+    nrm = torch.empty(F * 9, dtype=torch.float32, device="cuda")
+    faces = torch.empty(F * dm.TEXEL_FACE.itemsize, dtype=torch.uint8, device="cuda")
+
+    def texel():
+        ctx.check(L.dmap_tessellate_texel(dev.h, 1, F, pos.data_ptr(), uv.data_ptr(), nrm.data_ptr(),
+                                          faces.data_ptr(), C.byref(nf), sp), "dmap_tessellate_texel")
+
+    dev_all = dm.Scene.from_synthetic(ctx, sc_all)
+    n_u = 256
+    Vt, Ft = (n_u + 1) * (n_u + 2) // 2 * dev_all.n_tri, n_u * n_u * dev_all.n_tri
+    upos = torch.empty(Vt * 3, dtype=torch.float32, device="cuda")
+    uuv = torch.empty(Vt * 2, dtype=torch.float32, device="cuda")
+    unrm = torch.empty(Vt * 3, dtype=torch.float32, device="cuda")
+    uidx = torch.empty(Ft * 3, dtype=torch.int32, device="cuda")
+
+    def uniform():
+        ctx.check(L.dmap_tessellate_uniform(dev_all.h, n_u, upos.data_ptr(), uuv.data_ptr(), unrm.data_ptr(),
+                                            uidx.data_ptr(), sp), "dmap_tessellate_uniform")
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return float(np.mean(ms))
+
+    l0 = ctx.kernel_launches
+    with Clocks(local) as clk:
+        ms = timed(texel)
+    launches = (ctx.kernel_launches - l0) // (args.warmup + args.steps)
+    ms_u = timed(uniform)
+    face_bytes = 9 * 4 + 6 * 4 + 9 * 4 + dm.TEXEL_FACE.itemsize
+    gbs = F * face_bytes / (ms * 1e-3) / 1e9
+    u_bytes = Vt * 32 + Ft * 12
+    hbm, peak_src = peaks()
+    line = {"metric": "texel tessellation faces/s", "value": F / (ms * 1e-3), "unit": "faces/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "gpu_launches": launches,
+            "config": {"workload": f"append_texel_tessellation m=1, 4 cube-sphere patches (8 triangles) of "
+                                   f"{sub.assets[0].n_leaf}^2 FP32 maps", "faces": F,
+                       "l2": "output larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "traffic": None, "peak_source": peak_src, "kernel": "texel_kernel<count|emit> + scan",
+                         "bytes_per_face": face_bytes},
+            "uniform": {"workload": f"append_displaced_triangle n={n_u}, 192 triangles", "vertices": Vt,
+                        "faces": Ft, "ms": ms_u, "GB/s": u_bytes / (ms_u * 1e-3) / 1e9}}
+    if not args.no_cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import py_oracle
+        cpu = py_oracle.CpuScene(py_oracle.Oracle(), sub)
+        t0 = time.perf_counter()
+        got = cpu.tessellate_texel(0, 1)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": len(got["interior"]) / dt, "unit": "faces/s", "cores": 1, "kind": "port",
+                                "sample": "triangle 0 of the workload through the oracle's restatement"}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s

@@ -41,6 +41,7 @@ PRECISION = {"f64": 0, "f32": 1}
 MODE = {"closest": 0, "occluded": 1}
 SCHEDULE = {"wavefront": 0, "simple": 1}
 KEEP_F64, BUILD_DIRECT = 1, 2
+OK, ERR_INVALID, ERR_CUDA, ERR_OOM = 0, 1, 2, 3  # dmap_status
 
 HIT32 = np.dtype([("t", "<f4"), ("st", "<f4", 2), ("bary", "<f4", 2), ("ng", "<f4", 3), ("tri", "<i4"),
                   ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
@@ -87,6 +88,10 @@ class _RayRecord(C.Structure):
 
 class _UvMap(C.Structure):
     _fields_ = [("uv_scale", C.c_double * 2), ("uv_offset", C.c_double * 2), ("flip_v", C.c_int)]
+
+
+# dmap_texel_face: triangle, interior, st[3][2]
+TEXEL_FACE = np.dtype([("triangle", np.int32), ("interior", np.int32), ("st", np.float64, (3, 2))])
 
 
 class _ServerConfig(C.Structure):
@@ -138,6 +143,10 @@ def lib() -> C.CDLL:
                                     C.POINTER(dbl)]),
             "dmap_surface_points": (i32, [vp, vp, i32, i64, C.POINTER(_UvMap), vp, vp]),
             "dmap_surface_points_host": (i32, [vp, vp, i32, i64, C.POINTER(_UvMap), vp]),
+            "dmap_tessellate_uniform": (i32, [vp, i32, vp, vp, vp, vp, vp]),
+            "dmap_tessellate_uniform_host": (i32, [vp, i32, vp, vp, vp, vp]),
+            "dmap_tessellate_texel": (i32, [vp, i32, i64, vp, vp, vp, vp, C.POINTER(i64), vp]),
+            "dmap_tessellate_texel_host": (i32, [vp, i32, i64, vp, vp, vp, vp, C.POINTER(i64)]),
             "dmap_server_create": (i32, [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]),
             "dmap_server_destroy": (None, [vp]),
             "dmap_server_submit_rays": (i32, [vp, vp, vp, i64, i32, vp, C.POINTER(C.c_uint64)]),
@@ -336,6 +345,37 @@ class Scene:
         m = _UvMap((C.c_double * 2)(*uv_scale), (C.c_double * 2)(*uv_offset), int(flip_v))
         self.ctx.check(lib().dmap_surface_points_host(self.h, h.ctypes.data, dt, len(h), C.byref(m),
                                                       out.ctypes.data), "dmap_surface_points_host")
+        return out
+
+    def tessellate_uniform(self, n: int) -> dict:
+        """dmap_tessellate_uniform_host (append_displaced_triangle over the
+        scene's triangles at subdivision n): positions (V, 3), texcoords
+        (V, 2), normals (V, 3) float32, indices (F, 3) uint32 (global)."""
+        nt = self.n_tri
+        V, F = (n + 1) * (n + 2) // 2 * nt, n * n * nt
+        out = {"positions": np.empty((V, 3), np.float32), "texcoords": np.empty((V, 2), np.float32),
+               "normals": np.empty((V, 3), np.float32), "indices": np.empty((F, 3), np.uint32)}
+        self.ctx.check(lib().dmap_tessellate_uniform_host(self.h, n, out["positions"].ctypes.data,
+                                                          out["texcoords"].ctypes.data, out["normals"].ctypes.data,
+                                                          out["indices"].ctypes.data), "dmap_tessellate_uniform_host")
+        return out
+
+    def tessellate_texel(self, m: int = 1) -> dict:
+        """dmap_tessellate_texel_host (append_texel_tessellation over the
+        scene's triangles, m x m sub-cells per leaf cell): per face positions
+        (F, 3, 3), texcoords (F, 3, 2), normals (F, 3, 3) float32 and the
+        TexelFace records (F,) of TEXEL_FACE."""
+        n = C.c_int64()
+        self.ctx.check(lib().dmap_tessellate_texel_host(self.h, m, 0, None, None, None, None, C.byref(n)),
+                       "dmap_tessellate_texel_host")
+        F = n.value
+        out = {"positions": np.empty((F, 3, 3), np.float32), "texcoords": np.empty((F, 3, 2), np.float32),
+               "normals": np.empty((F, 3, 3), np.float32), "faces": np.empty(F, TEXEL_FACE)}
+        if F:
+            self.ctx.check(lib().dmap_tessellate_texel_host(self.h, m, F, out["positions"].ctypes.data,
+                                                            out["texcoords"].ctypes.data,
+                                                            out["normals"].ctypes.data, out["faces"].ctypes.data,
+                                                            C.byref(n)), "dmap_tessellate_texel_host")
         return out
 
     def autotune(self, rays_ptr: int, ray_dtype: int, n: int, base: Optional[TraversalOptions] = None,

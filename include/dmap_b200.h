@@ -241,6 +241,52 @@ dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, d
                                      const dmap_uv_map *map, double *out_host);
 
 /*
+ * Oracle meshes (displaced_tessellation.h:17-53): the displaced surface of
+ * every scene triangle as a float mesh, for mesh-based cross-checks.
+ * Positions S = P + h N, texture coordinates (s, t) and unit vertex normals
+ * are evaluated in double with the reference's operation order and rounded
+ * to float, so both meshes are bit-identical to the reference's.
+ *
+ * dmap_tessellate_uniform replaces append_displaced_triangle
+ * (displaced_tessellation.cpp:32-56) over the scene's triangles in order:
+ * the uniform barycentric grid at subdivision n (tessellation_grid, :11-30),
+ * (n+1)(n+2)/2 vertices and n*n faces per triangle; triangle k's vertices
+ * start at k (n+1)(n+2)/2 and its faces at k n^2, with indices global (the
+ * reference's `base + f`). Buffers: vertices and normals 3 floats per
+ * vertex, texcoords 2, indices 3 uint32 per face; the MeshData padding of
+ * finalize_mesh_data is the caller's. Fails when the vertex count exceeds
+ * the uint32 index range.
+ */
+dmap_status dmap_tessellate_uniform(dmap_scene *scene, int n, float *vertices_dev, float *texcoords_dev,
+                                    float *normals_dev, uint32_t *indices_dev, void *stream);
+dmap_status dmap_tessellate_uniform_host(dmap_scene *scene, int n, float *vertices, float *texcoords,
+                                         float *normals, uint32_t *indices);
+
+/*
+ * The texel-aligned tessellation (append_texel_tessellation,
+ * displaced_tessellation.cpp:97-137) over the scene's triangles in order:
+ * every leaf cell meeting a triangle's uv domain split into m x m sub-cells,
+ * each inside sub-cell into two faces along the (1,0)-(0,1) diagonal and each
+ * straddling one into the fan of its clipped polygon; faces keep the base
+ * face's winding. Three unshared vertices per face (vertex 3f + q of face
+ * f), as append_face writes them, so the index buffer is the identity and is
+ * not returned. faces_dev gets the TexelFace records (triangle = scene
+ * triangle index). Synchronous on `stream`: *n_faces returns the face count.
+ * With vertices_dev NULL only the count is computed; otherwise a count above
+ * capacity writes nothing and returns DMAP_ERR_INVALID (with *n_faces set).
+ */
+typedef struct dmap_texel_face {
+    int32_t triangle;
+    int32_t interior; /* 1: from a sub-cell inside the domain; 0: a fan face of a clipped sub-cell */
+    double st[3][2];  /* tile coordinates of the three vertices */
+} dmap_texel_face;
+dmap_status dmap_tessellate_texel(dmap_scene *scene, int m, int64_t capacity, float *vertices_dev,
+                                  float *texcoords_dev, float *normals_dev, dmap_texel_face *faces_dev,
+                                  int64_t *n_faces, void *stream);
+dmap_status dmap_tessellate_texel_host(dmap_scene *scene, int m, int64_t capacity, float *vertices,
+                                       float *texcoords, float *normals, dmap_texel_face *faces, int64_t *n_faces);
+
+/*
  * Schedule autotuner (no counterpart in the reference). Times the wavefront
  * schedule's launch shapes (rounds x blocks_per_sm) with `base`'s other
  * options on the first min(n, 2^22) of the caller's device rays and returns

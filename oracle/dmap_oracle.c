@@ -1671,3 +1671,180 @@ void o_surface_point(const o_scene *s, int tri, double u, double v, const double
     double o[14] = {p.x, p.y, p.z, ng.x, ng.y, ng.z, dpdu.x, dpdu.y, dpdu.z, dpdv.x, dpdv.y, dpdv.z, uvx, uvy};
     memcpy(out, o, sizeof(o));
 }
+
+/* ------------------------------------------------------------------------ */
+/* Oracle meshes, displaced_tessellation.cpp.                                */
+/* ------------------------------------------------------------------------ */
+
+/* pointwise_fields(tri, field, s, t).n (displaced_surface.cpp:110-158): the
+ * unnormalized surface normal Su x Sv, h and its gradient from the grid. */
+static v3 pointwise_normal(const o_tri *T, const o_grid *g, double s, double t)
+{
+    v2 gh = grid_grad(g, s, t);
+    double h = grid_h(g, s, t);
+    o_nframe f = normal_frame_at(T, s, t);
+    v3 Su = add3(add3(T->e1, mul3(gh.x, f.N)), mul3(h, f.Nu));
+    v3 Sv = add3(add3(T->e2, mul3(gh.y, f.N)), mul3(h, f.Nv));
+    return cross3(Su, Sv);
+}
+
+/* chart_mirrored (displaced_surface.cpp:160). */
+static int chart_mirrored(const o_tri *T)
+{
+    v3 wn = cross3(sub3(T->p1, T->p0), sub3(T->p2, T->p0));
+    return dot3(cross3(T->e1, T->e2), wn) < 0.0;
+}
+
+static void put_vertex(v3 S, v2 st, v3 n, float *pos, float *uv, float *nrm)
+{
+    pos[0] = (float)S.x;
+    pos[1] = (float)S.y;
+    pos[2] = (float)S.z;
+    uv[0] = (float)st.x;
+    uv[1] = (float)st.y;
+    nrm[0] = (float)n.x;
+    nrm[1] = (float)n.y;
+    nrm[2] = (float)n.z;
+}
+
+void o_tessellate_uniform(const o_scene *s, int tri, int n, float *pos, float *uv, float *nrm, uint32_t *idx)
+{
+    /* tessellation_grid (:11-30) and append_displaced_triangle (:32-56),
+     * vertex indices relative to the triangle's first vertex */
+    const o_isect *X = find_tri(s, tri, NULL);
+    const o_tri *T = X->tri;
+    int64_t k = 0;
+    for (int j = 0; j <= n; ++j)
+        for (int i = 0; i <= n - j; ++i, ++k) {
+            v2 st = tri_param(T, (double)i / n, (double)j / n);
+            v3 S = displaced_position(T, X->field, st.x, st.y);
+            v3 nr = eigen_normalized(pointwise_normal(T, X->field, st.x, st.y));
+            put_vertex(S, st, nr, pos + 3 * k, uv + 2 * k, nrm + 3 * k);
+        }
+#define TESS_INDEX(i, j) ((uint32_t)((j) * (n + 1) - (j) * ((j)-1) / 2 + (i)))
+    int64_t f = 0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n - j; ++i) {
+            idx[3 * f] = TESS_INDEX(i, j);
+            idx[3 * f + 1] = TESS_INDEX(i + 1, j);
+            idx[3 * f + 2] = TESS_INDEX(i, j + 1);
+            ++f;
+            if (i + j < n - 1) {
+                idx[3 * f] = TESS_INDEX(i + 1, j);
+                idx[3 * f + 1] = TESS_INDEX(i + 1, j + 1);
+                idx[3 * f + 2] = TESS_INDEX(i, j + 1);
+                ++f;
+            }
+        }
+#undef TESS_INDEX
+}
+
+typedef struct {
+    int n;
+    v2 p[8];
+} o_clip;
+
+/* clip_square (uv_clip.cpp:61-90): Sutherland-Hodgman of the square (c, s)
+ * against the domain's three inward half-planes. */
+static o_clip clip_square(const o_uvtri *U, v2 c, double s)
+{
+    o_clip in;
+    in.n = 4;
+    in.p[0] = add2(c, V2(-s, -s));
+    in.p[1] = add2(c, V2(s, -s));
+    in.p[2] = add2(c, V2(s, s));
+    in.p[3] = add2(c, V2(-s, s));
+    for (int k = 0; k < 3; ++k) {
+        o_clip out;
+        out.n = 0;
+        for (int a = 0; a < in.n; ++a) {
+            v2 pa = in.p[a], pb = in.p[(a + 1) % in.n];
+            double fa = dot2(U->n[k], pa) - U->d[k], fb = dot2(U->n[k], pb) - U->d[k];
+            if (fa >= 0.0)
+                out.p[out.n++] = pa;
+            if ((fa >= 0.0) != (fb >= 0.0)) {
+                double t = fa / (fa - fb);
+                out.p[out.n++] = add2(pa, mul2(t, sub2(pb, pa)));
+            }
+        }
+        in = out;
+        if (in.n == 0)
+            break;
+    }
+    return in;
+}
+
+typedef struct {
+    const o_isect *X;
+    int mirrored;
+    int64_t n, cap;
+    float *pos, *uv, *nrm;
+    double *st6;
+    int *interior;
+} o_texel_out;
+
+/* append_face / append_vertex (displaced_tessellation.cpp:60-95): three
+ * unshared vertices per face, the normal oriented along the base face's
+ * winding, b and c swapped under a mirrored chart. */
+static void texel_face(o_texel_out *o, v2 a, v2 b, v2 c, int interior)
+{
+    if (o->mirrored) {
+        v2 x = b;
+        b = c;
+        c = x;
+    }
+    if (o->n < o->cap) {
+        const o_tri *T = o->X->tri;
+        v2 v[3] = {a, b, c};
+        for (int q = 0; q < 3; ++q) {
+            int64_t k = 3 * o->n + q;
+            v3 S = displaced_position(T, o->X->field, v[q].x, v[q].y);
+            v3 nr = eigen_normalized(pointwise_normal(T, o->X->field, v[q].x, v[q].y));
+            if (o->mirrored)
+                nr = V3(-nr.x, -nr.y, -nr.z);
+            put_vertex(S, v[q], nr, o->pos + 3 * k, o->uv + 2 * k, o->nrm + 3 * k);
+            o->st6[6 * o->n + 2 * q] = v[q].x;
+            o->st6[6 * o->n + 2 * q + 1] = v[q].y;
+        }
+        o->interior[o->n] = interior;
+    }
+    ++o->n;
+}
+
+int64_t o_tessellate_texel(const o_scene *s, int tri, int m, int64_t cap, float *pos, float *uv, float *nrm,
+                           double *st6, int *interior)
+{
+    /* append_texel_tessellation (displaced_tessellation.cpp:97-137) */
+    const o_isect *X = find_tri(s, tri, NULL);
+    const o_uvtri *U = &X->domain;
+    o_texel_out o = {X, chart_mirrored(X->tri), 0, cap, pos, uv, nrm, st6, interior};
+    double w = 1.0 / X->pyr->n_leaf;
+    int64_t i_lo = (int64_t)floor(U->lo.x / w), i_hi = (int64_t)ceil(U->hi.x / w) - 1;
+    int64_t j_lo = (int64_t)floor(U->lo.y / w), j_hi = (int64_t)ceil(U->hi.y / w) - 1;
+    for (int64_t j = j_lo; j <= j_hi; ++j)
+        for (int64_t i = i_lo; i <= i_hi; ++i) {
+            v2 c = V2((i + 0.5) * w, (j + 0.5) * w);
+            int overlap = classify_square(U, c, 0.5 * w);
+            if (overlap == OUTSIDE)
+                continue;
+            double ws = w / m;
+            for (int b = 0; b < m; ++b)
+                for (int a = 0; a < m; ++a) {
+                    v2 p00 = V2(i * w + a * ws, j * w + b * ws);
+                    v2 p10 = add2(p00, V2(ws, 0.0)), p01 = add2(p00, V2(0.0, ws)), p11 = add2(p00, V2(ws, ws));
+                    v2 sc = add2(p00, V2(0.5 * ws, 0.5 * ws));
+                    int sub = overlap == INSIDE ? INSIDE : classify_square(U, sc, 0.5 * ws);
+                    if (sub == OUTSIDE)
+                        continue;
+                    if (sub == STRADDLE) {
+                        o_clip poly = clip_square(U, sc, 0.5 * ws);
+                        for (int k = 1; k + 1 < poly.n; ++k)
+                            texel_face(&o, poly.p[0], poly.p[k], poly.p[k + 1], 0);
+                        continue;
+                    }
+                    texel_face(&o, p00, p10, p01, 1);
+                    texel_face(&o, p10, p11, p01, 1);
+                }
+        }
+    return o.n;
+}

@@ -104,6 +104,18 @@ void o_triangle_param(const o_scene *s, int tri, double u, double v, double *out
 void o_surface_point(const o_scene *s, int tri, double u, double v, const double *uv_scale, const double *uv_offset,
                      int flip_v, double *out14);
 
+/* Oracle meshes (displaced_tessellation.cpp). Uniform barycentric grid at
+ * subdivision n (tessellation_grid + append_displaced_triangle, :11-56):
+ * (n+1)(n+2)/2 vertices (pos 3 floats, uv 2, normal 3) and n*n faces
+ * (3 uint32 indices, relative to the triangle's first vertex). */
+void o_tessellate_uniform(const o_scene *s, int tri, int n, float *pos, float *uv, float *nrm, uint32_t *idx);
+/* Texel-aligned tessellation with m x m sub-cells per leaf cell
+ * (append_texel_tessellation, :97-137): returns the face count and writes
+ * the first cap faces, three unshared vertices each (pos 9 floats, uv 6,
+ * normals 9), the TexelFace st (6 doubles) and its interior flag. */
+int64_t o_tessellate_texel(const o_scene *s, int tri, int m, int64_t cap, float *pos, float *uv, float *nrm,
+                           double *st6, int *interior);
+
 #ifdef __cplusplus
 }
 #endif

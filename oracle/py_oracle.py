@@ -71,6 +71,11 @@ class _Lib:
         self._node_bound = f("node_bound", None, C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int64, _dp, C.c_int,
                              C.c_int, _dp)
         self._disp = f("displaced_position", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp)
+        _fp = C.POINTER(C.c_float)
+        self._tess_uniform = f("tessellate_uniform", None, C.c_void_p, C.c_int, C.c_int, _fp, _fp, _fp,
+                               C.POINTER(C.c_uint32))
+        self._tess_texel = f("tessellate_texel", C.c_int64, C.c_void_p, C.c_int, C.c_int, C.c_int64, _fp, _fp, _fp,
+                             _dp, C.POINTER(C.c_int))
         if self.prefix == "o_":
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
                                _dp, _lp, _lp, C.c_int)
@@ -184,4 +189,31 @@ class CpuScene:
         sc = np.array(uv_scale, np.float64)
         of = np.array(uv_offset, np.float64)
         self.lib._surf(self.h, tri, u, v, _ptr(sc), _ptr(of), int(flip_v), _ptr(out))
+        return out
+
+    def tessellate_uniform(self, tri, n):
+        """append_displaced_triangle at subdivision n: dict of positions
+        (V, 3), texcoords (V, 2), normals (V, 3) float32 and indices (n*n, 3)
+        uint32 relative to the triangle's first vertex."""
+        V = (n + 1) * (n + 2) // 2
+        out = {"positions": np.empty((V, 3), np.float32), "texcoords": np.empty((V, 2), np.float32),
+               "normals": np.empty((V, 3), np.float32), "indices": np.empty((n * n, 3), np.uint32)}
+        fp = C.POINTER(C.c_float)
+        self.lib._tess_uniform(self.h, tri, n, _ptr(out["positions"], fp), _ptr(out["texcoords"], fp),
+                               _ptr(out["normals"], fp), _ptr(out["indices"], C.POINTER(C.c_uint32)))
+        return out
+
+    def tessellate_texel(self, tri, m):
+        """append_texel_tessellation with m x m sub-cells: dict of per-face
+        positions (F, 3, 3), texcoords (F, 3, 2), normals (F, 3, 3) float32,
+        st (F, 3, 2) double and interior (F,) int32."""
+        fp = C.POINTER(C.c_float)
+        n = self.lib._tess_texel(self.h, tri, m, 0, None, None, None, None, None)
+        out = {"positions": np.empty((n, 3, 3), np.float32), "texcoords": np.empty((n, 3, 2), np.float32),
+               "normals": np.empty((n, 3, 3), np.float32), "st": np.empty((n, 3, 2)),
+               "interior": np.empty(n, np.int32)}
+        got = self.lib._tess_texel(self.h, tri, m, n, _ptr(out["positions"], fp), _ptr(out["texcoords"], fp),
+                                   _ptr(out["normals"], fp), _ptr(out["st"]),
+                                   _ptr(out["interior"], C.POINTER(C.c_int)))
+        assert got == n
         return out

@@ -5,6 +5,7 @@
 #include "displaced_intersector.h"
 #include "node_bounds.h"
 #include "taylor_pyramid.h"
+#include "displaced_tessellation.h"
 
 #include "../dmap_oracle.h"
 
@@ -281,6 +282,44 @@ void r_displaced_position(const r_scene *s, int tri, double sp, double tp, doubl
     out[0] = S[0];
     out[1] = S[1];
     out[2] = S[2];
+}
+
+void r_tessellate_uniform(const r_scene *s, int tri, int n, float *pos, float *uv, float *nrm, uint32_t *idx)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    ks::MeshData m;
+    dmap::append_displaced_triangle(m, *X->tri, X->field, n);
+    std::copy(m.vertices.begin(), m.vertices.end(), pos);
+    std::copy(m.texcoords.begin(), m.texcoords.end(), uv);
+    std::copy(m.vertex_normals.begin(), m.vertex_normals.end(), nrm);
+    std::copy(m.indices.begin(), m.indices.end(), idx);
+}
+
+int64_t r_tessellate_texel(const r_scene *s, int tri, int m, int64_t cap, float *pos, float *uv, float *nrm,
+                           double *st6, int *interior)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    ks::MeshData md;
+    std::vector<dmap::TexelFace> faces;
+    dmap::append_texel_tessellation(md, *X->tri, X->field, X->pyramid->n_leaf, m, tri, faces);
+    int64_t n = (int64_t)faces.size();
+    for (int64_t f = 0; f < n && f < cap; ++f) {
+        for (int q = 0; q < 3; ++q) {
+            uint32_t v = md.indices[3 * f + q];
+            for (int c = 0; c < 3; ++c) {
+                pos[9 * f + 3 * q + c] = md.vertices[3 * v + c];
+                nrm[9 * f + 3 * q + c] = md.vertex_normals[3 * v + c];
+            }
+            uv[6 * f + 2 * q] = md.texcoords[2 * v];
+            uv[6 * f + 2 * q + 1] = md.texcoords[2 * v + 1];
+            st6[6 * f + 2 * q] = faces[f].st[q][0];
+            st6[6 * f + 2 * q + 1] = faces[f].st[q][1];
+        }
+        interior[f] = faces[f].interior ? 1 : 0;
+    }
+    return n;
 }
 
 } // extern "C"

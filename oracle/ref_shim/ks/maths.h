@@ -324,6 +324,7 @@ typedef Matrix<double, 2, 2> Matrix2d;
 typedef Matrix<double, 3, 3> Matrix3d;
 typedef Matrix<double, 2, 1> Vector2d;
 typedef Matrix<double, 3, 1> Vector3d;
+typedef Matrix<int, 3, 1> Vector3i;
 
 } // namespace Eigen
 

@@ -67,3 +67,27 @@ def aimed_rays(cpu, n, seed=2028):
 
 def small_sphere(n=32, patches=(0, 1, 5, 16, 40, 95)):
     return scenes.cube_sphere_scene(n, 4, patches=list(patches))
+
+
+def chart_scene(n=32, seed=7):
+    """Triangles with general charts (texture coordinates off the cell
+    lattice), one of them mirrored, and a repeat-wrapped object whose chart
+    leaves the unit tile: the cases the texel tessellation clips."""
+    rng = np.random.default_rng(seed)
+    h0 = scenes.sine_noise_heights(n, seed, 0.06)
+    h1 = scenes.sine_noise_heights(n, seed + 1, 0.04)
+    a0 = scenes.Asset(scenes.close_tile(h0, repeat=False).astype(np.float32))
+    a1 = scenes.Asset(scenes.close_tile(h1, repeat=True).astype(np.float32), scale=1.0, offset=0.01, repeat=True)
+    P = [np.array([0.0, 0.0, 0.0]), np.array([1.2, 0.1, 0.05]), np.array([0.2, 1.1, -0.1])]
+    N = [v / np.linalg.norm(v) for v in (np.array([0.05, -0.1, 1.0]), np.array([0.1, 0.0, 1.0]),
+                                          np.array([-0.08, 0.1, 1.0]))]
+
+    def rec(t0, t1, t2, shift=np.zeros(3)):
+        return np.concatenate([P[0] + shift, P[1] + shift, P[2] + shift, N[0], N[1], N[2], t0, t1, t2])
+
+    tris = [rec([0.13, 0.21], [0.87, 0.30], [0.25, 0.91]),
+            rec([0.13, 0.21], [0.25, 0.91], [0.87, 0.30], np.array([0.0, 0.0, 0.6])),   # mirrored chart
+            rec([-0.31, 0.42], [1.27, -0.18], [0.52, 1.61], np.array([1.5, 0.0, 0.0]))]  # repeat, off the tile
+    tris = np.stack(tris)
+    tris[:, 18:24] += rng.random(6) * 1e-3  # off the dyadic lattice
+    return scenes.Scene([a0, a1], tris, np.array([0, 0, 1], np.int32), name=f"charts{n}", extent=3.0)
