@@ -194,7 +194,7 @@ def cpu_sample(sc, rays, hits_t, budget_s: float, use_ref: bool):
     cpu = py_oracle.CpuScene(lib, sub)
     threads = os.cpu_count() or 1
     t = time.perf_counter()
-    h, _ = cpu.intersect(sample, threads=threads)
+    h, _ = cpu.intersect(sample, threads=threads, order="index")
     dt = time.perf_counter() - t
     # the bounce rays of the sample's hits
     hit = np.isfinite(h[:, 0])
@@ -212,7 +212,7 @@ def run_cpu(args, rank, world):
     times = []
     for s in range(args.warmup + args.steps):
         t = time.perf_counter()
-        cpu.intersect(allr, threads=threads)
+        cpu.intersect(allr, threads=threads, order="index")
         dt = time.perf_counter() - t
         if s >= args.warmup:
             times.append(dt)
@@ -256,6 +256,8 @@ def main():
                     help="keep --rounds / --blocks-per-sm instead of the autotuner's choice")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
+    ap.add_argument("--order", default="nearest", choices=["nearest", "index"],
+                    help="triangle order: nearest box entry first, or the reference's flat loop")
     ap.add_argument("--rounds", type=int, default=6)
     ap.add_argument("--blocks-per-sm", type=int, default=5)
     ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
@@ -298,10 +300,11 @@ def main():
     keep64 = args.precision == "f64" or True   # the FP64 path counts the reference algorithm's work
     dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=keep64)
     opt = dm.TraversalOptions(precision=args.precision, schedule=args.schedule, rounds=args.rounds,
-                              blocks_per_sm=args.blocks_per_sm)
-    ref_opt = dm.TraversalOptions(precision="f64")
-    # bounce rays from the FP64 (reference-arithmetic) hits, frozen
-    h0 = dev.intersect(prim, ref_opt, np.float64)
+                              blocks_per_sm=args.blocks_per_sm, order=args.order)
+    ref_opt = dm.TraversalOptions(precision="f64", order=args.order)
+    flat_opt = dm.TraversalOptions(precision="f64", order="index")
+    # bounce rays from the FP64 hits of the reference's flat loop, frozen
+    h0 = dev.intersect(prim, flat_opt, np.float64)
     hit = h0["tri"] >= 0
     bounce = scenes.bounce_rays(prim[hit], h0["t"][hit], h0["ng"][hit])
     rays_all = np.concatenate([prim, bounce, extra_rays(args.config, sc, args.small)]).astype(np.float32)
@@ -311,9 +314,11 @@ def main():
     lo, hi = shard_range(n_all, rank, world)
     my = np.ascontiguousarray(rays_all[lo:hi])
     n = len(my)
-    # algorithmic work of the reference algorithm on these rays (FP64 path counters)
+    # algorithmic work of the query on these rays (FP64 path counters, same triangle order)
     _, st = dev.intersect(my, ref_opt, np.float64, stats=True)
     flops_ray, bytes_ray, counts = work_per_ray(st)
+    # and of the reference's flat loop (index order), for comparison
+    counts_flat = work_per_ray(dev.intersect(my, flat_opt, np.float64, stats=True)[1])[2]
     # the measured path's own counters (its bounds are wider: more cells may pass)
     _, st_path = dev.intersect(my, opt, np.float64, stats=True)
     counts_path = work_per_ray(st_path)[2]
@@ -397,7 +402,7 @@ def main():
             "config": {"workload": workload_name(args), "rays_per_step": n_all, "precision": args.precision,
                        "l2": "flushed between steps (256 MB write); pyramids 17 GB exceed L2",
                        "parallelism": f"replicated scene, rays split over {world} rank(s)",
-                       "schedule": args.schedule, "autotuned": tuned,
+                       "schedule": args.schedule, "order": args.order, "autotuned": tuned,
                        "rounds": opt.rounds, "blocks_per_sm": opt.blocks_per_sm},
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": int(my.nbytes),
                     "d2h_bytes_per_step": int(n * 48)},
@@ -409,7 +414,8 @@ def main():
             "roofline_fp32": {"achieved": flops_ray * n / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                               "flops_per_ray": flops_ray, "nominal_peak": 74.4,
                               "note": "FP32 CUDA-core issue is the path's bound; no measured FP32 peak on file"},
-            "work_per_ray": counts, "work_per_ray_path": counts_path, "setup_s": setup_s}
+            "work_per_ray": counts, "work_per_ray_path": counts_path, "work_per_ray_flat_loop": counts_flat,
+            "setup_s": setup_s}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
@@ -418,7 +424,7 @@ def main():
             cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, rays_all, np.where(hit, 1.0, np.inf), 10.0, True)
             t = time.perf_counter()
             for _ in range(reps):
-                cpu.intersect(allr, threads=threads)
+                cpu.intersect(allr, threads=threads, order="index")
             dt = (time.perf_counter() - t) / reps
             line["cpu_baseline"] = {"value": len(allr) / dt / 1e6, "unit": "Mrays/s", "cores": threads,
                                     "kind": kind, "sample": f"{len(allr)} rays (64x64 primary block at the image "
@@ -445,7 +451,8 @@ def run_pathtrace(args, rank, world, local, dist):
     dev = dm.Scene.from_synthetic(ctx, sc)
     w, h, spp = (320, 180, 4) if args.small else (1280, 720, 16)
     view = scenes.path_tracer_view(w, h)
-    opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm)
+    opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm,
+                              order=args.order)
 
     def render(seed):
         return dev.render(view, sc.emitter, spp=spp, max_depth=5, rr_depth=3, seed=seed, options=opt, use_graph=True)
@@ -719,7 +726,8 @@ def run_serve(args, rank, world, local, dist):
         return v
 
     rkw = dict(spp=4, max_depth=3, rr_depth=3)
-    opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm)
+    opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm,
+                              order=args.order)
     # warm-up: every path once
     srv = dm.Server(ctx, hbm_budget_bytes=120 * 10 ** 9, slots=2, options=opt)
     for k in range(args.warmup):
@@ -762,7 +770,7 @@ def run_serve(args, rank, world, local, dist):
 
     plain = None
     if not args.no_plain:
-        popt = dm.TraversalOptions(schedule="simple")
+        popt = dm.TraversalOptions(schedule="simple", order=args.order)
         lat, queries = [], 0
         t0 = time.perf_counter()
         for r in trace:
@@ -776,7 +784,7 @@ def run_serve(args, rank, world, local, dist):
             else:
                 rays = request_rays(r)
                 d = devs[r["scene"]] if r["kind"] == 0 else d_pt
-                d.intersect(rays, dm.TraversalOptions(schedule="simple",
+                d.intersect(rays, dm.TraversalOptions(schedule="simple", order=args.order,
                                                       mode="occluded" if r["kind"] == 2 else "closest"), np.float32)
                 queries += len(rays)
             lat.append((time.perf_counter() - t0 - r["t"]) * 1e3)

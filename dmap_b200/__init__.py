@@ -40,6 +40,7 @@ LEAF = {"newton": 0, "two_triangle": 1}
 PRECISION = {"f64": 0, "f32": 1}
 MODE = {"closest": 0, "occluded": 1}
 SCHEDULE = {"wavefront": 0, "simple": 1}
+ORDER = {"index": 0, "nearest": 1}
 KEEP_F64, BUILD_DIRECT = 1, 2
 OK, ERR_INVALID, ERR_CUDA, ERR_OOM = 0, 1, 2, 3  # dmap_status
 
@@ -61,7 +62,7 @@ class DmapError(RuntimeError):
 class _Options(C.Structure):
     _fields_ = [("bound", C.c_int), ("slab_max_level", C.c_int), ("leaf", C.c_int), ("precision", C.c_int),
                 ("mode", C.c_int), ("polish_cond", C.c_double), ("schedule", C.c_int), ("rounds", C.c_int),
-                ("blocks_per_sm", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("order", C.c_int)]
 
 
 class _Camera(C.Structure):
@@ -184,11 +185,12 @@ class TraversalOptions:
     schedule: str = "wavefront"
     rounds: int = 6
     blocks_per_sm: int = 5
+    order: str = "nearest"
 
     def c(self) -> _Options:
         return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],
                         MODE[self.mode], self.polish_cond, SCHEDULE[self.schedule], self.rounds,
-                        self.blocks_per_sm)
+                        self.blocks_per_sm, ORDER[self.order])
 
 
 class Context:

@@ -86,6 +86,7 @@ void dmap_options_default(dmap_options *opt)
     opt->schedule = DMAP_SCHEDULE_WAVEFRONT;
     opt->rounds = 6;
     opt->blocks_per_sm = 5;
+    opt->order = DMAP_ORDER_NEAREST;
 }
 
 // ---- assets ---------------------------------------------------------------
@@ -299,6 +300,7 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
         cudaFree(s->tris_dev);
         cudaFree(s->tris32_dev);
         cudaFree(s->block_box_dev);
+        cudaFree(s->block_tree_dev);
         delete s;
         return st;
     };
@@ -341,6 +343,34 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
         if ((e = cudaMalloc((void **)&s->block_box_dev, sizeof(float) * bb.size())) ||
             (e = cudaMemcpy(s->block_box_dev, bb.data(), sizeof(float) * bb.size(), cudaMemcpyHostToDevice)))
             return cleanup(cuda_fail(ctx, e, "dmap_scene_create: block boxes"));
+        if (nb > 256) {
+            // more than 8192 triangles: a complete binary tree over the block
+            // boxes, heap layout, unions bottom-up (exact in float); leaves
+            // past the last block stay empty and are never entered
+            int L = 0;
+            while ((1 << L) < nb)
+                ++L;
+            const int P = 1 << L;
+            std::vector<float> tree((size_t)12 * P);
+            for (int v = 0; v < 2 * P; ++v)
+                for (int a3 = 0; a3 < 3; ++a3) {
+                    tree[6 * v + a3] = INFINITY;
+                    tree[6 * v + 3 + a3] = -INFINITY;
+                }
+            for (int b = 0; b < nb; ++b)
+                for (int q = 0; q < 6; ++q)
+                    tree[6 * (P + b) + q] = bb[6 * b + q];
+            for (int v = P - 1; v >= 1; --v)
+                for (int a3 = 0; a3 < 3; ++a3) {
+                    tree[6 * v + a3] = std::min(tree[6 * (2 * v) + a3], tree[6 * (2 * v + 1) + a3]);
+                    tree[6 * v + 3 + a3] = std::max(tree[6 * (2 * v) + 3 + a3], tree[6 * (2 * v + 1) + 3 + a3]);
+                }
+            if ((e = cudaMalloc((void **)&s->block_tree_dev, sizeof(float) * tree.size())) ||
+                (e = cudaMemcpy(s->block_tree_dev, tree.data(), sizeof(float) * tree.size(), cudaMemcpyHostToDevice)))
+                return cleanup(cuda_fail(ctx, e, "dmap_scene_create: block tree"));
+            s->tree_leaves = P;
+            s->tree_log2 = L;
+        }
     }
     s->tris_host.resize(n_tri);
     if ((e = cudaMemcpy(s->tris_host.data(), s->tris_dev, sizeof(TriDev) * n_tri, cudaMemcpyDeviceToHost)))
@@ -363,6 +393,7 @@ void dmap_scene_destroy(dmap_scene *s)
     cudaFree(s->tris_dev);
     cudaFree(s->tris32_dev);
     cudaFree(s->block_box_dev);
+    cudaFree(s->block_tree_dev);
     delete s;
 }
 
@@ -411,10 +442,16 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     if (o.schedule < 0 || o.schedule > 1 || o.rounds < 0 || o.rounds > dmapk::kMaxRounds || o.blocks_per_sm < 0 ||
         o.blocks_per_sm > 16)
         return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad schedule options");
+    if (o.order < 0 || o.order > 1)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad order");
+    q.order = o.order;
     q.schedule = o.schedule;
     q.rounds = o.rounds;
     q.blocks_per_sm = o.blocks_per_sm;
     q.block_box = s->block_box_dev;
+    q.block_tree = s->block_tree_dev;
+    q.tree_leaves = s->tree_leaves;
+    q.tree_log2 = s->tree_log2;
     return DMAP_OK;
 }
 

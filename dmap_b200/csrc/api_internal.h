@@ -62,6 +62,8 @@ struct dmap_scene
     TriDev *tris_dev = nullptr;
     TriDev32 *tris32_dev = nullptr;
     float *block_box_dev = nullptr; // more than 256 triangles: boxes of blocks of 32 (QueryOpts::block_box)
+    float *block_tree_dev = nullptr; // more than 8192 triangles: the tree over those boxes (QueryOpts::block_tree)
+    int tree_leaves = 0, tree_log2 = 0;
     std::vector<TriDev> tris_host;
     bool all_f64 = true;
 };

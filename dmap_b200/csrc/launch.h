@@ -18,6 +18,7 @@ struct QueryOpts
     int schedule;             // DMAP_SCHEDULE_*
     int rounds;               // wavefront: walk/leaf rounds before the inline-leaf drain
     int blocks_per_sm;        // wavefront walk: resident 128-thread CTAs per SM
+    int order = 1;            // DMAP_ORDER_*: 0 index order, 1 nearest box entry first
     // When set, the number of rays is read here on the device when the query
     // runs (at most the n the launch is given, which sizes grids and scratch):
     // stages of a device-driven pipeline pass counts they produced themselves.
@@ -25,6 +26,11 @@ struct QueryOpts
     // Scenes of more than 256 triangles: the object box of every block of 32
     // consecutive triangles (6 floats, outward), for the walk's candidate mask.
     const float *block_box = nullptr;
+    // Scenes of more than 8192 triangles: the complete binary tree over those
+    // block boxes in heap layout (node 1 the root, 6 floats per node, leaves
+    // tree_leaves .. 2 tree_leaves - 1 in block order; tree_leaves = 2^tree_log2).
+    const float *block_tree = nullptr;
+    int tree_leaves = 0, tree_log2 = 0;
 };
 
 constexpr int kMaxRounds = 32;

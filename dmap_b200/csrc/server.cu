@@ -229,6 +229,9 @@ struct dmap_server
             dmapk::QueryOpts qq = q;
             qq.mode = first->mode;
             qq.block_box = first->scene->block_box_dev;
+            qq.block_tree = first->scene->block_tree_dev;
+            qq.tree_leaves = first->scene->tree_leaves;
+            qq.tree_log2 = first->scene->tree_log2;
             qq.ray_dtype = qq.hit_dtype = 0;
             dmap_scene *s = first->scene;
             if (e == cudaSuccess)

@@ -35,6 +35,7 @@
 // This translation unit is compiled with -fmad=false (the FP64 leaf must
 // round like the reference); FP32 code uses explicit fmaf where it wants one.
 #include "f32_node.cuh"
+#include "order.cuh"
 
 namespace
 {
@@ -63,8 +64,11 @@ constexpr unsigned FULL = 0xffffffffu;
 // the caller's): where the exact ray is inside the box, |t d| <= |o| + |box|,
 // so the float ray is within u (2|o| + |box|) of it. On a pass t1 is the
 // exit parameter, rounded up.
-__device__ __forceinline__ bool box_pass(const float *box_lo, const float *box_hi, const float *of, const float *df,
-                                         const float *invf, float t0, float &t1)
+// box_pass that also returns the entry distance t0: the box is widened
+// outward by more than the float rounding of the slab products, so t0 is a
+// lower bound of the exact entry of any box inside it.
+__device__ __forceinline__ bool box_range(const float *box_lo, const float *box_hi, const float *of, const float *df,
+                                          const float *invf, float &t0, float &t1)
 {
     bool ok = true;
 #pragma unroll
@@ -83,10 +87,46 @@ __device__ __forceinline__ bool box_pass(const float *box_lo, const float *box_h
     return ok && !(t0 > t1 + tol32(fmaxf(fabsf(t0), fabsf(t1))));
 }
 
+__device__ __forceinline__ bool box_pass(const float *box_lo, const float *box_hi, const float *of, const float *df,
+                                         const float *invf, float t0, float &t1)
+{
+    return box_range(box_lo, box_hi, of, df, invf, t0, t1);
+}
+
 __device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, const float *df, const float *invf,
                                            float t0, float &t1)
 {
     return box_pass(T.box_lo, T.box_hi, of, df, invf, t0, t1);
+}
+
+// Scenes of more than 8192 triangles: the first block >= b, in index
+// order, whose box the ray meets within [t0, t1]. A left-to-right walk of
+// the complete binary tree over the block boxes (heap layout, node 1 the
+// root, leaves P..2P-1 in block order) that skips every subtree whose box
+// the ray misses and every subtree past the last block; each node is
+// entered at most once per call. Blocks come out in index order, so the
+// flat loop's semantics hold (the boxes only prune). -1 when there is none.
+__device__ inline int tree_next(const float *__restrict__ tree, int P, int log2P, int nb, int b, const float *of,
+                                const float *df, const float *invf, float t0, float t1)
+{
+    int v = P + b;
+    for (int guard = 0; guard <= 2 * P; ++guard) {
+        const int depth = 31 - __clz(v);
+        const int start = (v << (log2P - depth)) - P; // the subtree's first block
+        float tt = t1;
+        if (start < nb && box_pass(tree + 6 * v, tree + 6 * v + 3, of, df, invf, t0, tt)) {
+            if (v >= P)
+                return v - P;
+            v = 2 * v;
+        } else {
+            while (v & 1)
+                v >>= 1;
+            if (v == 0)
+                return -1;
+            ++v;
+        }
+    }
+    return -1;
 }
 
 // The tangent-space ray of a triangle: transformed in double, rounded to
@@ -212,11 +252,38 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
     d64::hit64 best;
     int best_tri = -1;
     bool found = false;
-    for (int t = 0; t < n_tri; ++t) {
-        const TriDev32 &T = tris32[t];
+    // the next triangle: index order, or (nearest) the smallest (key, index)
+    // past the cursor among the candidates the ray still reaches
+    double inv[3], ckey = -INFINITY;
+    int cidx = -1;
+    d64::ray_inverse(d, inv);
+    for (int step = 0; step < n_tri; ++step) {
+        int t = step;
         float t1 = __double2float_ru(t_max);
-        if (!object_box(T, of, df, invf, __double2float_rd(t_min), t1))
+        if (opt.order == 1) {
+            const float tmf = t1;
+            double bk = 0.0;
+            int bt = -1;
+            for (int q = 0; q < n_tri; ++q) {
+                const double key = d64::entry_key(tris64[q], o, d, inv, t_min);
+                if (!d64::after_cursor(key, q, ckey, cidx) || !d64::before_best(key, q, bk, bt))
+                    continue;
+                float tt = tmf;
+                if (!object_box(tris32[q], of, df, invf, __double2float_rd(t_min), tt))
+                    continue;
+                bk = key;
+                bt = q;
+                t1 = tt;
+            }
+            if (bt < 0)
+                break;
+            t = bt;
+            ckey = bk;
+            cidx = bt;
+        } else if (!object_box(tris32[t], of, df, invf, __double2float_rd(t_min), t1)) {
             continue;
+        }
+        const TriDev32 &T = tris32[t];
         if (sp)
             ++st[DMAP_ST_TRI];
         double tm = t_max;
@@ -244,6 +311,8 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
 struct RayState
 {
     double t_max;
+    double ckey; // nearest-first order: the cursor (key, index) of the last triangle taken
+    int cidx;
     int tri, root, best_tri, flags;
     int cl, ci, cj, el, ei, ej;
     int nah, lah;
@@ -280,7 +349,7 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // One lane's walk from its parked or fresh state to the next leaf (parked,
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
-template <bool ST, bool INLINE_LEAF, bool BLOCKS, typename R, typename H, typename Fp>
+template <bool ST, bool INLINE_LEAF, int TOPM, typename R, typename H, typename Fp>
 __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
@@ -291,10 +360,10 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     enum : int { NEED = 0, TOP = 1, WALK = 2, DONE = 3 };
     const int lane = threadIdx.x & 31;
     // the candidate mask: one bit per triangle (up to 256 triangles), or
-    // (BLOCKS) one bit per block of 32 consecutive triangles (up to 8192),
-    // visited in order
-    constexpr bool use_blocks = BLOCKS;
-    const bool use_mask = BLOCKS || n_tri <= 32 * kMaskWords;
+    // (TOPM 1) one bit per block of 32 consecutive triangles (up to 8192),
+    // visited in order; (TOPM 2) no mask, the block tree instead
+    constexpr bool use_blocks = TOPM == 1;
+    const bool use_mask = TOPM == 1 || (TOPM == 0 && n_tri <= 32 * kMaskWords);
     const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
@@ -306,6 +375,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     double o[3], d[3], t_min = 0.0, t_max = 0.0;
     float of[3], df[3], invf[3], tmin_f = 0.0f;
     int tri = 0, best_tri = -1, root = 0, si = 0, sj = 0, nah = 0, lah = 0, flags = 0, guard = 0;
+    double ckey = -INFINITY;
+    int cidx = -1;
     Ray32 r;
     Cell32 cur = {0, 0, 0}, end = {0, 0, 0};
     unsigned mask[kMaskWords];
@@ -328,6 +399,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     auto park = [&](bool here) {
         RayState &s = states[ray];
         s.t_max = t_max;
+        s.ckey = ckey;
+        s.cidx = cidx;
         s.tri = tri;
         s.root = root;
         s.best_tri = best_tri;
@@ -383,6 +456,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                             stl[q] = 0;
                     if (round == 0) {
                         tri = 0;
+                        ckey = -INFINITY;
+                        cidx = -1;
                         best_tri = -1;
                         flags = 0;
                         nah = lah = 0;
@@ -391,6 +466,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     } else {
                         const RayState &s = states[ray];
                         t_max = s.t_max;
+                        ckey = s.ckey;
+                        cidx = s.cidx;
                         tri = s.tri;
                         root = s.root;
                         best_tri = s.best_tri;
@@ -458,7 +535,114 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
         if (phase == TOP) {
             float t1 = 0.0f;
             bool hit_box = false;
-            if (use_blocks) {
+            if (opt.order == 1) {
+                // nearest box entry first: the smallest (key, index) past the
+                // cursor among the candidates the ray still reaches
+                double inv[3];
+                d64::ray_inverse(d, inv);
+                double bk = 0.0;
+                int bt = -1;
+                const float tmf = __double2float_ru(t_max);
+                auto consider = [&](int t) {
+                    const double key = d64::entry_key(tris64[t], o, d, inv, t_min);
+                    if (!d64::after_cursor(key, t, ckey, cidx) || !d64::before_best(key, t, bk, bt))
+                        return;
+                    float tt = tmf;
+                    if (!object_box(tris32[t], of, df, invf, tmin_f, tt))
+                        return;
+                    bk = key;
+                    bt = t;
+                    t1 = tt;
+                };
+                if (TOPM >= 1) {
+                    // blocks: first the candidate block with the nearest
+                    // entry, then the others unless their entry (a lower
+                    // bound of their triangles' keys) is beyond the best key
+                    const int nb = (n_tri + 31) >> 5;
+                    auto blocks = [&](auto &&fn) {
+                        if (TOPM == 2) {
+                            for (int b = 0; b < nb; ++b) {
+                                b = tree_next(opt.block_tree, opt.tree_leaves, opt.tree_log2, nb, b, of, df, invf,
+                                              tmin_f, tmf);
+                                if (b < 0)
+                                    break;
+                                fn(b);
+                            }
+                        } else {
+#pragma unroll 1
+                            for (int w = 0; w < kMaskWords; ++w) {
+                                unsigned bits = mask[0];
+#pragma unroll
+                                for (int q = 1; q < kMaskWords; ++q)
+                                    bits = w == q ? mask[q] : bits;
+                                while (bits) {
+                                    const int b = 32 * w + __ffs(bits) - 1;
+                                    bits &= bits - 1;
+                                    if (b < nb)
+                                        fn(b);
+                                }
+                            }
+                        }
+                    };
+                    auto entry = [&](int b, float &e) {
+                        float t0 = tmin_f, t1b = tmf;
+                        const bool ok = box_range(opt.block_box + 6 * b, opt.block_box + 6 * b + 3, of, df, invf, t0,
+                                                  t1b);
+                        e = t0;
+                        return ok;
+                    };
+                    int b0 = -1;
+                    float e0 = INFINITY;
+                    blocks([&](int b) {
+                        float e;
+                        if (entry(b, e) && (b0 < 0 || e < e0)) {
+                            b0 = b;
+                            e0 = e;
+                        }
+                    });
+                    if (b0 >= 0) {
+                        for (int t = 32 * b0, stop = min(n_tri, 32 * b0 + 32); t < stop; ++t)
+                            consider(t);
+                        blocks([&](int b) {
+                            float e;
+                            if (b == b0 || !entry(b, e) || (bt >= 0 && (double)e > bk))
+                                return;
+                            for (int t = 32 * b, stop = min(n_tri, 32 * b + 32); t < stop; ++t)
+                                consider(t);
+                        });
+                    }
+                } else if (use_mask) {
+#pragma unroll 1
+                    for (int w = 0; w < kMaskWords; ++w) {
+                        unsigned bits = mask[0];
+#pragma unroll
+                        for (int q = 1; q < kMaskWords; ++q)
+                            bits = w == q ? mask[q] : bits;
+                        while (bits) {
+                            const int item = 32 * w + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if (use_blocks) {
+                                const int stop = min(n_tri, 32 * item + 32);
+                                for (int t = 32 * item; t < stop; ++t)
+                                    consider(t);
+                            } else if (item < n_tri) {
+                                consider(item);
+                            }
+                        }
+                    }
+                } else {
+                    for (int t = 0; t < n_tri; ++t)
+                        consider(t);
+                }
+                if (bt >= 0) {
+                    tri = bt;
+                    ckey = bk;
+                    cidx = bt;
+                    hit_box = true;
+                } else {
+                    tri = n_tri;
+                }
+            } else if (use_blocks) {
                 // the next block whose box the ray met, then its triangles in order
                 while (tri < n_tri) {
                     int blk = tri >> 5, w = blk >> 5;
@@ -475,6 +659,30 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     if (nb != blk)
                         tri = nb << 5;
                     const int stop = min(n_tri, (nb + 1) << 5);
+                    for (; tri < stop; ++tri) {
+                        t1 = __double2float_ru(t_max);
+                        if (object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
+                            hit_box = true;
+                            break;
+                        }
+                    }
+                    if (hit_box)
+                        break;
+                }
+            } else if (TOPM == 2) {
+                // blocks in order from the tree, then their triangles in order
+                const int nb = (n_tri + 31) >> 5;
+                while (tri < n_tri) {
+                    if ((tri & 31) == 0) {
+                        const int blk = tree_next(opt.block_tree, opt.tree_leaves, opt.tree_log2, nb, tri >> 5, of, df,
+                                                  invf, tmin_f, __double2float_ru(t_max));
+                        if (blk < 0) {
+                            tri = n_tri;
+                            break;
+                        }
+                        tri = blk << 5;
+                    }
+                    const int stop = min(n_tri, (tri | 31) + 1);
                     for (; tri < stop; ++tri) {
                         t1 = __double2float_ru(t_max);
                         if (object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
@@ -906,22 +1114,28 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
         bool last = rd == rounds;
         // the block mask has its own instances so that scenes of up to 256
         // triangles keep the smaller kernel
-        const bool blocks = n_tri > 32 * kMaskWords && opt.block_box && n_tri <= 32 * 32 * kMaskWords;
-#define DMAP_WALK_LAUNCH(ST_, IL_, BL_)                                                                             \
-    wave_walk<ST_, IL_, BL_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,           \
+        // (and scenes of more than 8192 triangles walk the block tree)
+        const int topm = n_tri > 32 * kMaskWords && opt.block_box && n_tri <= 32 * 32 * kMaskWords ? 1
+                         : n_tri > 32 * 32 * kMaskWords && opt.block_tree                          ? 2
+                                                                                                    : 0;
+#define DMAP_WALK_LAUNCH(ST_, IL_, TM_)                                                                             \
+    wave_walk<ST_, IL_, TM_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,           \
                                                                  ST_ ? stats : nullptr, states, q_in, rd, leaves, \
                                                                  ws.counters, status)
+#define DMAP_WALK_TOPM(ST_, IL_)                                                                                    \
+    (topm == 1 ? DMAP_WALK_LAUNCH(ST_, IL_, 1) : topm == 2 ? DMAP_WALK_LAUNCH(ST_, IL_, 2) : DMAP_WALK_LAUNCH(ST_, IL_, 0))
         if (stats) {
             if (last)
-                blocks ? DMAP_WALK_LAUNCH(true, true, true) : DMAP_WALK_LAUNCH(true, true, false);
+                DMAP_WALK_TOPM(true, true);
             else
-                blocks ? DMAP_WALK_LAUNCH(true, false, true) : DMAP_WALK_LAUNCH(true, false, false);
+                DMAP_WALK_TOPM(true, false);
         } else {
             if (last)
-                blocks ? DMAP_WALK_LAUNCH(false, true, true) : DMAP_WALK_LAUNCH(false, true, false);
+                DMAP_WALK_TOPM(false, true);
             else
-                blocks ? DMAP_WALK_LAUNCH(false, false, true) : DMAP_WALK_LAUNCH(false, false, false);
+                DMAP_WALK_TOPM(false, false);
         }
+#undef DMAP_WALK_TOPM
 #undef DMAP_WALK_LAUNCH
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;

@@ -10,6 +10,7 @@
 #include "f64_math.cuh"
 #include "f64_leaf.cuh"
 #include "f64_node.cuh"
+#include "order.cuh"
 #include "launch.h"
 
 namespace
@@ -159,7 +160,37 @@ __global__ void __launch_bounds__(128) walk64_kernel(const TriDev *__restrict__ 
     hit64 best;
     int best_tri = -1;
     bool found = false;
-    for (int t = 0; t < n_tri; ++t) {
+    // the next triangle: index order (the flat loop), or (nearest) the
+    // smallest (key, index) past the cursor whose box the ray still meets
+    const double od[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+    double inv[3], ckey = -INFINITY;
+    int cidx = -1;
+    ray_inverse(dd, inv);
+    for (int step = 0; step < n_tri; ++step) {
+        int t = step;
+        if (opt.order == 1) {
+            double bk = 0.0;
+            int bt = -1;
+            for (int q = 0; q < n_tri; ++q) {
+                const TriDev &Q = tris[q];
+                if (Q.status != 0)
+                    continue;
+                const double key = entry_key(Q, od, dd, inv, t_min);
+                if (!after_cursor(key, q, ckey, cidx) || !before_best(key, q, bk, bt))
+                    continue;
+                box3 box = {L3(Q.box_lo), L3(Q.box_hi)};
+                double t0 = t_min, t1 = t_max;
+                if (!box_clip(box, o, d, t0, t1))
+                    continue;
+                bk = key;
+                bt = q;
+            }
+            if (bt < 0)
+                break;
+            t = bt;
+            ckey = bk;
+            cidx = bt;
+        }
         const TriDev &T = tris[t];
         box3 box = {L3(T.box_lo), L3(T.box_hi)};
         double t0 = t_min, t1 = t_max;

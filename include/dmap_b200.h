@@ -155,6 +155,22 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *o
 #define DMAP_SCHEDULE_WAVEFRONT 0 /* rounds of a persistent walk kernel and a leaf kernel (default) */
 #define DMAP_SCHEDULE_SIMPLE 1    /* one thread per ray, one launch: the plain per-request kernel */
 
+/*
+ * The order in which a ray visits the triangles whose boxes it meets.
+ * INDEX is ObjectIntersector::intersect's flat loop (displaced_intersector.cpp:
+ * 778-799): triangles in index order, each walked with the t_max the ones
+ * before it left. NEAREST visits them by box entry distance (the FP64 slab
+ * entry max(t_min, max_a min(ta, tb)), ta = (lo_a - o_a) * (1 / d_a), ties
+ * to the lower index), as a BVH over the embree callbacks
+ * (displaced_geometry.cpp:49-106) does, and skips a triangle whose box lies
+ * beyond the current hit: the walk starts with a tight t_max, so far
+ * triangles cost a box test instead of a walk. Both find the nearest
+ * certified root; the returned t may differ in the last bits where the walks
+ * run with different t_max.
+ */
+#define DMAP_ORDER_INDEX 0
+#define DMAP_ORDER_NEAREST 1
+
 typedef struct dmap_options {
     int bound;          /* DMAP_BOUND_*, default BOTH */
     int slab_max_level; /* default 1 */
@@ -167,6 +183,7 @@ typedef struct dmap_options {
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
                            default 6; 0 = one walk with every leaf inline) */
     int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 5, at most 5 resident) */
+    int order;          /* DMAP_ORDER_*, default NEAREST */
 } dmap_options;
 
 /* Fills the defaults above. */

@@ -52,6 +52,9 @@ struct TraversalOptions
     int slab_max_level = 1;
     LeafMode leaf = LeafMode::Newton;
     bool fp64 = false; // the reference's double arithmetic throughout (needs assets kept in FP64)
+    // false: ObjectIntersector's flat loop, triangles in index order (the
+    // drop-in default); true: nearest box entry first (DMAP_ORDER_NEAREST)
+    bool nearest = false;
 
     dmap_options c() const
     {
@@ -61,6 +64,7 @@ struct TraversalOptions
         o.slab_max_level = slab_max_level;
         o.leaf = (int)leaf;
         o.precision = fp64 || leaf == LeafMode::TwoTriangle ? DMAP_PRECISION_F64 : DMAP_PRECISION_F32;
+        o.order = nearest ? DMAP_ORDER_NEAREST : DMAP_ORDER_INDEX;
         return o;
     }
 };

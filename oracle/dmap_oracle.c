@@ -1465,14 +1465,79 @@ static void write_miss(double *out)
     out[11] = -1.0;
 }
 
-/* The flat loop of ObjectIntersector::intersect_flat (:778-799) over every object. */
+/* A candidate of the nearest-first order: the triangle's box entry key and
+ * its scene-global index. */
+typedef struct {
+    double key;
+    int ob, k, g;
+} o_cand;
+
+static int cand_cmp(const void *pa, const void *pb)
+{
+    const o_cand *a = (const o_cand *)pa, *b = (const o_cand *)pb;
+    if (a->key != b->key)
+        return a->key < b->key ? -1 : 1;
+    return (a->g > b->g) - (a->g < b->g);
+}
+
+/* The nearest-first key (not in the reference: the order a BVH over the
+ * embree callbacks gives, displaced_geometry.cpp:49-106, made exact):
+ * max(t_min, max over axes with d != 0 of min(ta, tb)), ta = (lo - o) * (1 / d). */
+static double entry_key(const o_box *B, v3 o, v3 d, const double *inv, double t_min)
+{
+    double key = t_min;
+    for (int a = 0; a < 3; ++a)
+        if (comp3(d, a) != 0.0) {
+            double ta = (comp3(B->lo, a) - comp3(o, a)) * inv[a], tb = (comp3(B->hi, a) - comp3(o, a)) * inv[a];
+            key = dmax(key, dmin(ta, tb));
+        }
+    return key;
+}
+
+/* The flat loop of ObjectIntersector::intersect_flat (:778-799) over every
+ * object (order O_ORDER_INDEX); or (O_ORDER_NEAREST) the same loop over the
+ * triangles whose boxes the ray meets, sorted by (key, index), each still
+ * box-tested with the t_max of the ones before it. cand: n_tri scratch. */
 static int scene_intersect1(const o_scene *s, const double *ray, int bound, int slab_max_level, int leaf,
-                            double *out, int64_t *st, int64_t *level_stats)
+                            double *out, int64_t *st, int64_t *level_stats, int order, o_cand *cand)
 {
     v3 o = V3(ray[0], ray[1], ray[2]), d = V3(ray[3], ray[4], ray[5]);
     double t_min = ray[6], t_max = ray[7];
     int found = 0;
     write_miss(out);
+    if (order == O_ORDER_NEAREST) {
+        double inv[3];
+        for (int a = 0; a < 3; ++a)
+            inv[a] = comp3(d, a) != 0.0 ? 1.0 / comp3(d, a) : 0.0;
+        int nc = 0;
+        for (int ob = 0; ob < s->n_obj; ++ob) {
+            const o_object *O = &s->obj[ob];
+            for (int k = 0; k < O->n_tri; ++k) {
+                double t0 = t_min, t1 = t_max;
+                if (!box_clip(&O->isects[k].box, o, d, &t0, &t1))
+                    continue;
+                o_cand c = {entry_key(&O->isects[k].box, o, d, inv, t_min), ob, k, O->first_tri + k};
+                cand[nc++] = c;
+            }
+        }
+        qsort(cand, (size_t)nc, sizeof(o_cand), cand_cmp);
+        for (int c = 0; c < nc; ++c) {
+            const o_object *O = &s->obj[cand[c].ob];
+            const o_isect *X = &O->isects[cand[c].k];
+            double t0 = t_min, t1 = t_max;
+            if (!box_clip(&X->box, o, d, &t0, &t1))
+                continue;
+            if (st)
+                ++st[O_ST_TRIANGLE_TESTS];
+            o_hit h;
+            if (isect_intersect(X, o, d, t_min, t_max, bound, slab_max_level, leaf, &h, st, level_stats)) {
+                write_hit(out, &h, cand[c].g, cand[c].ob);
+                t_max = h.t;
+                found = 1;
+            }
+        }
+        return found;
+    }
     for (int ob = 0; ob < s->n_obj; ++ob) {
         const o_object *O = &s->obj[ob];
         for (int k = 0; k < O->n_tri; ++k) {
@@ -1497,7 +1562,7 @@ typedef struct {
     const o_scene *s;
     const double *rays;
     int64_t n;
-    int bound, slab_max_level, leaf;
+    int bound, slab_max_level, leaf, order;
     double *hits;
     int64_t *stats;
     atomic_llong next;
@@ -1513,6 +1578,7 @@ static void *worker(void *arg)
     int64_t local_levels[32] = {0};
     int64_t local_hits = 0;
     const int64_t chunk = 4096;
+    o_cand *cand = (o_cand *)malloc(sizeof(o_cand) * (size_t)(J->s->n_tri > 0 ? J->s->n_tri : 1));
     for (;;) {
         int64_t b = atomic_fetch_add(&J->next, chunk);
         if (b >= J->n)
@@ -1523,9 +1589,11 @@ static void *worker(void *arg)
             if (st)
                 memset(st, 0, O_ST_COUNT * sizeof(int64_t));
             local_hits += scene_intersect1(J->s, J->rays + 8 * r, J->bound, J->slab_max_level, J->leaf,
-                                           J->hits + O_HIT_DOUBLES * r, st, J->level_out ? local_levels : NULL);
+                                           J->hits + O_HIT_DOUBLES * r, st, J->level_out ? local_levels : NULL,
+                                           J->order, cand);
         }
     }
+    free(cand);
     atomic_fetch_add(&J->n_hit, local_hits);
     if (J->level_out) {
         pthread_mutex_lock(&J->mu);
@@ -1537,7 +1605,7 @@ static void *worker(void *arg)
 }
 
 int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
-                          double *hits, int64_t *stats, int64_t *level_stats, int threads)
+                          double *hits, int64_t *stats, int64_t *level_stats, int threads, int order)
 {
     if (threads <= 0)
         threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
@@ -1551,6 +1619,7 @@ int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int b
     J.bound = bound;
     J.slab_max_level = slab_max_level;
     J.leaf = leaf;
+    J.order = order;
     J.hits = hits;
     J.stats = stats;
     J.level_out = level_stats;

@@ -36,6 +36,9 @@ enum { O_BUILD_FOLD = 0, O_BUILD_DIRECT = 1 };
 /* Traversal options (traversal_options.h:587-608). */
 enum { O_BOUND_BOX = 0, O_BOUND_SLAB = 1, O_BOUND_BOTH = 2 };
 enum { O_LEAF_NEWTON = 0, O_LEAF_TWO_TRIANGLE = 1 };
+/* Triangle order of a scene query: the reference's flat loop, or nearest box
+ * entry first (the library's DMAP_ORDER_NEAREST). */
+enum { O_ORDER_INDEX = 0, O_ORDER_NEAREST = 1 };
 
 /* Per-ray statistics (TraversalStats, displaced_intersector.h:89-105), plus a
  * Newton-iteration counter that the reference does not keep. */
@@ -83,10 +86,12 @@ void o_scene_triangle_frame(const o_scene *s, int tri, double *out12);
 /* rays: n x 8 doubles (o, d, t_min, t_max). hits: n x O_HIT_DOUBLES.
  * stats: n x O_ST_COUNT int64 (may be NULL); level_stats: 32 int64 summed (may be NULL).
  * Flat loop over every triangle of every object, the walk of
- * ObjectIntersector::intersect_flat (displaced_intersector.cpp:778-799).
- * threads <= 0 uses every host core. Returns the number of hits. */
+ * ObjectIntersector::intersect_flat (displaced_intersector.cpp:778-799)
+ * (order O_ORDER_INDEX), or the same triangles nearest box entry first
+ * (O_ORDER_NEAREST). threads <= 0 uses every host core. Returns the number
+ * of hits. */
 int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
-                          double *hits, int64_t *stats, int64_t *level_stats, int threads);
+                          double *hits, int64_t *stats, int64_t *level_stats, int threads, int order);
 
 /* Single-triangle entry points for validation. */
 int o_triangle_intersect(const o_scene *s, int tri, const double *ray8, int bound, int slab_max_level, int leaf,

@@ -22,6 +22,7 @@ ST_NAMES = ("triangle_tests", "node_tests", "leaf_tests", "sub_squares", "newton
 
 BOUND = {"box": 0, "slab": 1, "both": 2}
 LEAF = {"newton": 0, "two_triangle": 1}
+ORDER = {"index": 0, "nearest": 1}
 
 _dp = C.POINTER(C.c_double)
 _lp = C.POINTER(C.c_int64)
@@ -78,7 +79,7 @@ class _Lib:
                              _dp, C.POINTER(C.c_int))
         if self.prefix == "o_":
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
-                               _dp, _lp, _lp, C.c_int)
+                               _dp, _lp, _lp, C.c_int, C.c_int)
             self._param = f("triangle_param", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp)
             self._surf = f("surface_point", None, C.c_void_p, C.c_int, C.c_double, C.c_double, _dp, _dp, C.c_int,
                            _dp)
@@ -147,16 +148,21 @@ class CpuScene:
             self.lib._sc_free(self.h)
             self.h = None
 
-    def intersect(self, rays, bound="both", slab_max_level=1, leaf="newton", stats=False, threads=0):
-        """rays: (n, 8) o, d, t_min, t_max. Returns (hits (n, 12), stats (n, 8) or None)."""
+    def intersect(self, rays, bound="both", slab_max_level=1, leaf="newton", stats=False, threads=0,
+                  order="nearest"):
+        """rays: (n, 8) o, d, t_min, t_max. Returns (hits (n, 12), stats (n, 8) or None).
+        order: "index" (the reference's flat loop) or "nearest" (box entry
+        first, the library's default); the reference build has the flat loop only."""
         r = np.ascontiguousarray(rays, np.float64)
         n = len(r)
         hits = np.empty((n, HIT))
         st = np.zeros((n, ST), np.int64) if stats else None
         if isinstance(self.lib, Oracle):
             self.lib._sc_isect(self.h, _ptr(r), n, BOUND[bound], slab_max_level, LEAF[leaf], _ptr(hits),
-                               _ptr(st, _lp), None, threads)
+                               _ptr(st, _lp), None, threads, ORDER[order])
         else:
+            if order != "index":
+                raise ValueError("the reference build runs the flat loop (order='index') only")
             self.lib._sc_isect(self.h, _ptr(r), n, BOUND[bound], slab_max_level, LEAF[leaf], _ptr(hits),
                                _ptr(st, _lp), threads)
         return hits, st

@@ -19,9 +19,10 @@ def ctx():
     return dm.Context(0)
 
 
-def _check(cpu, dev, rays, bound="both", k=1, **kw):
-    ho, so = cpu.intersect(rays, bound, k, stats=True)
-    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, precision="f32", **kw), np.float64, stats=True)
+def _check(cpu, dev, rays, bound="both", k=1, order="nearest", **kw):
+    ho, so = cpu.intersect(rays, bound, k, stats=True, order=order)
+    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, precision="f32", order=order, **kw), np.float64,
+                           stats=True)
     assert np.array_equal(hd["tri"] >= 0, ho[:, 10] >= 0), "hit/miss set differs"
     hit = ho[:, 10] >= 0
     assert np.array_equal(hd["tri"][hit], ho[hit, 10].astype(np.int32))
@@ -47,16 +48,19 @@ def test_f32_quad(ctx, oracle, bound, k):
     assert n > 1000 and ratio < 1.5
 
 
-@pytest.mark.parametrize("schedule,rounds,bps", [("wavefront", 6, 4), ("wavefront", 0, 1), ("wavefront", 1, 2),
-                                                 ("wavefront", 32, 4), ("simple", 6, 4)])
-def test_f32_sphere(ctx, oracle, schedule, rounds, bps):
-    """Every schedule gives the oracle's hits; rounds = 0 runs everything in
-    the inline-leaf walk, rounds = 1 parks each ray once."""
+@pytest.mark.parametrize("schedule,rounds,bps,order", [("wavefront", 6, 4, "nearest"), ("wavefront", 0, 1, "nearest"),
+                                                       ("wavefront", 1, 2, "nearest"), ("wavefront", 32, 4, "nearest"),
+                                                       ("simple", 6, 4, "nearest"), ("wavefront", 6, 4, "index"),
+                                                       ("wavefront", 1, 2, "index"), ("simple", 6, 4, "index")])
+def test_f32_sphere(ctx, oracle, schedule, rounds, bps, order):
+    """Every schedule and both triangle orders give the oracle's hits;
+    rounds = 0 runs everything in the inline-leaf walk, rounds = 1 parks
+    each ray once."""
     sc = helpers.small_sphere(32)
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
     rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 2000),
                            helpers.aimed_rays(cpu, 2000)[0]])
-    n, ratio = _check(cpu, dev, rays, schedule=schedule, rounds=rounds, blocks_per_sm=bps)
+    n, ratio = _check(cpu, dev, rays, order=order, schedule=schedule, rounds=rounds, blocks_per_sm=bps)
     assert n > 1000 and ratio < 1.5
 
 
@@ -131,8 +135,30 @@ def test_f32_many_triangles_block_mask(ctx, oracle, n, k):
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
     rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 1500),
                            helpers.aimed_rays(cpu, 1500)[0]])
-    n_hit, _ = _check(cpu, dev, rays)
-    assert n_hit > 1000
-    a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront"), np.float64)
-    b = dev.intersect(rays, dm.TraversalOptions(schedule="simple"), np.float64)
-    assert a.tobytes() == b.tobytes()
+    for order in ("nearest", "index"):
+        n_hit, _ = _check(cpu, dev, rays, order=order)
+        assert n_hit > 1000
+        a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", order=order), np.float64)
+        b = dev.intersect(rays, dm.TraversalOptions(schedule="simple", order=order), np.float64)
+        assert a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("k", [30, 40])
+def test_f32_many_triangles_block_tree(ctx, oracle, k):
+    """Scenes of more than 8192 triangles (10800 and 19200: 338 and 600
+    blocks, trees of 512 and 1024 leaves with empty padding) walk the tree
+    over the 32-triangle blocks' boxes; hits equal the oracle's in both
+    triangle orders, and the simple schedule's."""
+    sc = scenes.cube_sphere_scene(8, k)
+    assert len(sc.tris) > 8192
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 1500),
+                           helpers.aimed_rays(cpu, 1500)[0]])
+    for order in ("nearest", "index"):
+        n_hit, _ = _check(cpu, dev, rays, order=order)
+        assert n_hit > 1000
+        a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", order=order), np.float64)
+        b = dev.intersect(rays, dm.TraversalOptions(schedule="simple", order=order), np.float64)
+        assert a.tobytes() == b.tobytes()
+    occ = dev.intersect(rays, dm.TraversalOptions(mode="occluded"), np.float64)
+    assert np.array_equal(occ["tri"] >= 0, a["tri"] >= 0)

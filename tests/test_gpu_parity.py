@@ -52,9 +52,10 @@ def test_device_pyramid_equals_oracle(ctx, oracle, dtype, scale, offset, repeat)
             assert np.array_equal(got[ch], lv[ch]), (k, ch)
 
 
-def _compare(cpu, dev, rays, bound="both", k=1, leaf="newton"):
-    ho, so = cpu.intersect(rays, bound, k, leaf, stats=True)
-    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, leaf, precision="f64"), np.float64, stats=True)
+def _compare(cpu, dev, rays, bound="both", k=1, leaf="newton", order="nearest"):
+    ho, so = cpu.intersect(rays, bound, k, leaf, stats=True, order=order)
+    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, leaf, precision="f64", order=order), np.float64,
+                           stats=True)
     assert np.array_equal(hd["tri"], ho[:, 10].astype(np.int32))
     hit = ho[:, 10] >= 0
     assert np.array_equal(hd["t"][hit], ho[hit, 0])
@@ -94,17 +95,20 @@ def test_f64_walk_equals_oracle_quad(quad_pair, bound, k):
     assert _compare(cpu, dev, rays, bound, k) > 1000
 
 
-def test_f64_walk_equals_oracle_sphere(sphere_pair):
+@pytest.mark.parametrize("order", ["nearest", "index"])
+def test_f64_walk_equals_oracle_sphere(sphere_pair, order):
+    """Both triangle orders: the nearest-first one and the reference's flat loop."""
     cpu, dev = sphere_pair
     rays = np.concatenate([scenes.sphere_camera_rays(96, 54), helpers.near_surface_rays(cpu, 1500),
                            helpers.aimed_rays(cpu, 1500)[0]])
-    assert _compare(cpu, dev, rays) > 1000
+    assert _compare(cpu, dev, rays, order=order) > 1000
 
 
 def test_f64_two_triangle_leaf_equals_oracle(quad_pair):
     cpu, dev = quad_pair
     rays = np.concatenate([scenes.quad_camera_rays(32, 32), helpers.near_surface_rays(cpu, 800)])
     _compare(cpu, dev, rays, leaf="two_triangle")
+    _compare(cpu, dev, rays, leaf="two_triangle", order="index")
 
 
 def test_f64_float64_rays(sphere_pair):

@@ -29,8 +29,8 @@ def test_oracle_equals_reference_quad(oracle, reference, quad, bound, k):
         assert np.array_equal(so.triangle_info(t), sr.triangle_info(t))
         assert np.array_equal(so.triangle_frame(t), sr.triangle_frame(t))
     rays = _all_rays(so, quad, scenes.quad_camera_rays(48, 48))
-    ho, sto = so.intersect(rays, bound, k, stats=True)
-    hr, st_r = sr.intersect(rays, bound, k, stats=True)
+    ho, sto = so.intersect(rays, bound, k, stats=True, order="index")
+    hr, st_r = sr.intersect(rays, bound, k, stats=True, order="index")
     assert np.array_equal(ho, hr)
     cols = [0, 1, 2, 3, 5, 6]
     assert np.array_equal(sto[:, cols], st_r[:, cols])
@@ -40,7 +40,8 @@ def test_oracle_equals_reference_quad(oracle, reference, quad, bound, k):
 def test_oracle_equals_reference_two_triangle_leaf(oracle, reference, quad):
     so, sr = py_oracle.CpuScene(oracle, quad), py_oracle.CpuScene(reference, quad)
     rays = _all_rays(so, quad, scenes.quad_camera_rays(32, 32))
-    assert np.array_equal(so.intersect(rays, leaf="two_triangle")[0], sr.intersect(rays, leaf="two_triangle")[0])
+    assert np.array_equal(so.intersect(rays, leaf="two_triangle", order="index")[0],
+                          sr.intersect(rays, leaf="two_triangle", order="index")[0])
 
 
 def test_oracle_equals_reference_sphere(oracle, reference, sphere):
@@ -49,8 +50,8 @@ def test_oracle_equals_reference_sphere(oracle, reference, sphere):
         assert np.array_equal(so.triangle_info(t), sr.triangle_info(t))
     rays = np.concatenate([scenes.sphere_camera_rays(64, 36), helpers.near_surface_rays(so, 600),
                            helpers.aimed_rays(so, 600)[0]])
-    ho, sto = so.intersect(rays, stats=True)
-    hr, st_r = sr.intersect(rays, stats=True)
+    ho, sto = so.intersect(rays, stats=True, order="index")
+    hr, st_r = sr.intersect(rays, stats=True, order="index")
     assert np.array_equal(ho, hr)
     assert np.array_equal(sto[:, [0, 1, 2, 3, 5, 6]], st_r[:, [0, 1, 2, 3, 5, 6]])
 
@@ -105,3 +106,24 @@ def test_never_miss_and_residual(oracle, sphere):
         S = so.displaced_position(tri, hits[r, 1], hits[r, 2])
         p = rays[r, 0:3].astype(np.float64) + hits[r, 0] * rays[r, 3:6].astype(np.float64)
         assert np.linalg.norm(S - p) <= 2 * tol[tri] + 1e-12
+
+
+@pytest.mark.parametrize("name", ["quad", "sphere"])
+def test_nearest_order_same_hits(oracle, quad, sphere, name):
+    """The nearest-first triangle order finds the flat loop's hits: the same
+    hit set and triangles, t within the Newton tolerance (bit-identical on
+    almost every ray), and it walks fewer triangles and nodes."""
+    sc = quad if name == "quad" else sphere
+    so = py_oracle.CpuScene(oracle, sc)
+    cam = scenes.quad_camera_rays(48, 48) if name == "quad" else scenes.sphere_camera_rays(64, 36)
+    rays = np.concatenate([cam, helpers.near_surface_rays(so, 800), helpers.aimed_rays(so, 800)[0]])
+    hi, si = so.intersect(rays, stats=True, order="index")
+    hn, sn = so.intersect(rays, stats=True, order="nearest")
+    hit = hi[:, 10] >= 0
+    assert np.array_equal(hit, hn[:, 10] >= 0)
+    assert np.array_equal(hi[hit, 10], hn[hit, 10])
+    tol = np.array([so.triangle_info(t)[2] for t in range(so.n_tri)])
+    tri = hi[hit, 10].astype(int)
+    assert (np.abs(hi[hit, 0] - hn[hit, 0]) <= 4 * tol[tri]).all()
+    assert (hi[hit, 0] == hn[hit, 0]).mean() > 0.99
+    assert sn[:, 0].sum() <= si[:, 0].sum() and sn[:, 1].sum() <= si[:, 1].sum()
