@@ -421,7 +421,7 @@ def main():
         line["clocks"] = clk_s
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, rays_all, np.where(hit, 1.0, np.inf), 10.0, True)
+            cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, prim, np.where(hit, 1.0, np.inf), 10.0, True)
             t = time.perf_counter()
             for _ in range(reps):
                 cpu.intersect(allr, threads=threads, order="index")

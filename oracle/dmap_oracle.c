@@ -1562,7 +1562,7 @@ typedef struct {
     const o_scene *s;
     const double *rays;
     int64_t n;
-    int bound, slab_max_level, leaf, order;
+    int bound, slab_max_level, leaf, order, threads;
     double *hits;
     int64_t *stats;
     atomic_llong next;
@@ -1577,7 +1577,9 @@ static void *worker(void *arg)
     o_job *J = (o_job *)arg;
     int64_t local_levels[32] = {0};
     int64_t local_hits = 0;
-    const int64_t chunk = 4096;
+    /* chunks of at most 4096 rays, small enough that every thread gets work */
+    int64_t chunk = J->n / (8 * (int64_t)J->threads);
+    chunk = chunk < 1 ? 1 : chunk > 4096 ? 4096 : chunk;
     o_cand *cand = (o_cand *)malloc(sizeof(o_cand) * (size_t)(J->s->n_tri > 0 ? J->s->n_tri : 1));
     for (;;) {
         int64_t b = atomic_fetch_add(&J->next, chunk);
@@ -1620,6 +1622,7 @@ int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int b
     J.slab_max_level = slab_max_level;
     J.leaf = leaf;
     J.order = order;
+    J.threads = threads;
     J.hits = hits;
     J.stats = stats;
     J.level_out = level_stats;

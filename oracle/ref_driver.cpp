@@ -177,7 +177,8 @@ static void fill_stats(int64_t *out, const dmap::TraversalStats &st)
 
 // The object loop carries t_max the way intersect_flat does. The reference's
 // intersect is const and re-entrant, so rays are split over `threads`
-// std::threads in chunks of 4096 (threads <= 0: every core).
+// std::threads in chunks of at most 4096, small enough that every thread gets
+// work (threads <= 0: every core).
 static int64_t intersect_range(const r_scene *s, const double *rays, int64_t b, int64_t e,
                                const dmap::TraversalOptions &opt, double *hits, int64_t *stats);
 
@@ -191,13 +192,14 @@ int64_t r_scene_intersect(const r_scene *s, const double *rays, int64_t n, int b
         return intersect_range(s, rays, 0, n, opt, hits, stats);
     std::atomic<int64_t> next{0}, n_hit{0};
     std::vector<std::thread> pool;
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(4096, n / (8 * (int64_t)threads)));
     for (int k = 0; k < threads; ++k)
         pool.emplace_back([&] {
             for (;;) {
-                int64_t b = next.fetch_add(4096);
+                int64_t b = next.fetch_add(chunk);
                 if (b >= n)
                     break;
-                n_hit += intersect_range(s, rays, b, std::min<int64_t>(n, b + 4096), opt, hits, stats);
+                n_hit += intersect_range(s, rays, b, std::min<int64_t>(n, b + chunk), opt, hits, stats);
             }
         });
     for (auto &t : pool)
