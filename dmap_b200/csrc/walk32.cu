@@ -362,8 +362,10 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     // the candidate mask: one bit per triangle (up to 256 triangles), or
     // (TOPM 1) one bit per block of 32 consecutive triangles (up to 8192),
     // visited in order; (TOPM 2) no mask, the block tree instead
+    // (the launcher takes TOPM 0 only for scenes of up to 256 triangles, so
+    // the flat loops below are never compiled into the hot kernels)
     constexpr bool use_blocks = TOPM == 1;
-    const bool use_mask = TOPM == 1 || (TOPM == 0 && n_tri <= 32 * kMaskWords);
+    constexpr bool use_mask = TOPM <= 1;
     const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
@@ -1118,6 +1120,8 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
         const int topm = n_tri > 32 * kMaskWords && opt.block_box && n_tri <= 32 * 32 * kMaskWords ? 1
                          : n_tri > 32 * 32 * kMaskWords && opt.block_tree                          ? 2
                                                                                                     : 0;
+        if (topm == 0 && n_tri > 32 * kMaskWords)
+            return cudaErrorInvalidValue; // a scene without its block boxes (every scene has them)
 #define DMAP_WALK_LAUNCH(ST_, IL_, TM_)                                                                             \
     wave_walk<ST_, IL_, TM_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,           \
                                                                  ST_ ? stats : nullptr, states, q_in, rd, leaves, \
