@@ -1920,3 +1920,483 @@ int64_t o_tessellate_texel(const o_scene *s, int tri, int m, int64_t cap, float 
         }
     return o.n;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Displaced-emitter sampling: emission_tile.cpp, descent_sampler.cpp.      */
+/* ------------------------------------------------------------------------ */
+
+/* EmissionTile over the texture's own tile (emission_tile.cpp:30-33,
+ * 43-78, 80-130; the repeating layout): per level the mean of the texels
+ * below each cell. */
+typedef struct {
+    int n_leaf, n_levels;
+    int *m;
+    double **mean;
+} o_tile;
+
+static void tile_build(o_tile *E, const double *texels, int n)
+{
+    E->n_leaf = n;
+    E->n_levels = 1;
+    while ((1 << E->n_levels) <= n)
+        ++E->n_levels;
+    E->m = (int *)malloc(sizeof(int) * (size_t)E->n_levels);
+    E->mean = (double **)malloc(sizeof(double *) * (size_t)E->n_levels);
+    E->m[0] = n;
+    E->mean[0] = (double *)malloc(sizeof(double) * (size_t)n * n);
+    memcpy(E->mean[0], texels, sizeof(double) * (size_t)n * n);
+    for (int l = 1; l < E->n_levels; ++l) {
+        int cm = E->m[l - 1], pm = cm / 2;
+        E->m[l] = pm;
+        E->mean[l] = (double *)malloc(sizeof(double) * (size_t)pm * pm);
+        for (int J = 0; J < pm; ++J)
+            for (int I = 0; I < pm; ++I) {
+                double sum = 0.0;
+                for (int a = 0; a < 2; ++a)
+                    for (int b = 0; b < 2; ++b)
+                        sum += E->mean[l - 1][(size_t)(2 * J + a) * cm + (2 * I + b)];
+                E->mean[l][(size_t)J * pm + I] = 0.25 * sum;
+            }
+    }
+}
+
+static void tile_free(o_tile *E)
+{
+    for (int l = 0; l < E->n_levels; ++l)
+        free(E->mean[l]);
+    free(E->mean);
+    free(E->m);
+}
+
+static int64_t wrap_index(int64_t i, int m)
+{
+    int64_t r = i % m;
+    return r < 0 ? r + m : r;
+}
+
+static double tile_mean(const o_tile *E, int level, int64_t i, int64_t j) /* emission_tile.cpp:91-110 */
+{
+    if (level >= E->n_levels)
+        return E->mean[E->n_levels - 1][0];
+    int m = E->m[level];
+    return E->mean[level][(size_t)wrap_index(j, m) * m + wrap_index(i, m)];
+}
+
+static double tile_sum(const o_tile *E, int level, int64_t i, int64_t j) /* emission_tile.h:73-74 */
+{
+    double w = ldexp(1.0, level) / E->n_leaf;
+    return tile_mean(E, level, i, j) * (w * w);
+}
+
+/* FootprintChild / FootprintNode (descent_sampler.h:67-80). */
+typedef struct {
+    int overlap;
+    double area, mass;
+    int32_t node;
+} o_fpchild;
+
+typedef struct {
+    o_fpchild child[4];
+} o_fpnode;
+
+enum { O_DESCENT_AREA = 0, O_DESCENT_PRODUCT = 1, O_DESCENT_PRODUCT_GEOMETRY = 2 };
+
+struct o_emitter {
+    const o_isect *X;
+    o_tile tile;
+    int variant, emitter_cosine;
+    double beta;
+    int root_level;
+    int64_t root_i0, root_j0;
+    o_fpchild roots[4];
+    o_fpnode *nodes;
+    int n_nodes, cap_nodes;
+    double total_area, total_mass;
+};
+
+static double clip_area(const o_clip *P) /* uv_clip.cpp:51-59 */
+{
+    double a = 0.0;
+    for (int k = 0; k < P->n; ++k) {
+        v2 p0 = P->p[k], p1 = P->p[(k + 1) % P->n];
+        a += p0.x * p1.y - p1.x * p0.y;
+    }
+    return 0.5 * fabs(a);
+}
+
+static o_fpchild build_child(o_emitter *e, int level, int64_t i, int64_t j) /* descent_sampler.cpp:33-63 */
+{
+    int n_leaf = e->tile.n_leaf;
+    double w = ldexp(1.0, level) / n_leaf;
+    v2 c = V2((i + 0.5) * w, (j + 0.5) * w);
+    o_fpchild out = {OUTSIDE, 0.0, 0.0, -1};
+    out.overlap = classify_square(&e->X->domain, c, 0.5 * w);
+    if (out.overlap == OUTSIDE)
+        return out;
+    if (out.overlap == INSIDE) {
+        out.area = w * w;
+        out.mass = tile_sum(&e->tile, level, i, j);
+        return out;
+    }
+    if (level == 0) {
+        o_clip poly = clip_square(&e->X->domain, c, 0.5 * w);
+        out.area = clip_area(&poly);
+        out.mass = tile_mean(&e->tile, 0, i, j) * out.area;
+        return out;
+    }
+    int32_t index = e->n_nodes;
+    if (e->n_nodes == e->cap_nodes) {
+        e->cap_nodes = e->cap_nodes ? 2 * e->cap_nodes : 64;
+        e->nodes = (o_fpnode *)realloc(e->nodes, sizeof(o_fpnode) * (size_t)e->cap_nodes);
+    }
+    ++e->n_nodes;
+    o_fpnode node;
+    for (int ch = 0; ch < 4; ++ch) {
+        node.child[ch] = build_child(e, level - 1, 2 * i + (ch & 1), 2 * j + (ch >> 1));
+        out.area += node.child[ch].area;
+        out.mass += node.child[ch].mass;
+    }
+    e->nodes[index] = node;
+    out.node = index;
+    return out;
+}
+
+o_emitter *o_emitter_create(const o_scene *s, int tri, const double *texels, int n, int variant, double beta,
+                            int emitter_cosine)
+{
+    /* DescentSampler's constructor and build_footprint (descent_sampler.cpp:85-113) */
+    const o_isect *X = find_tri(s, tri, NULL);
+    if (!X || n != X->pyr->n_leaf)
+        return NULL;
+    o_emitter *e = (o_emitter *)calloc(1, sizeof(o_emitter));
+    e->X = X;
+    tile_build(&e->tile, texels, n);
+    e->variant = variant;
+    e->beta = beta;
+    e->emitter_cosine = emitter_cosine;
+    footprint_roots(&X->domain, n, &e->root_level, &e->root_i0, &e->root_j0);
+    for (int ch = 0; ch < 4; ++ch) {
+        e->roots[ch] = build_child(e, e->root_level, e->root_i0 + (ch & 1), e->root_j0 + (ch >> 1));
+        e->total_area += e->roots[ch].area;
+        e->total_mass += e->roots[ch].mass;
+    }
+    return e;
+}
+
+void o_emitter_free(o_emitter *e)
+{
+    if (!e)
+        return;
+    tile_free(&e->tile);
+    free(e->nodes);
+    free(e);
+}
+
+void o_emitter_info(const o_emitter *e, double *out)
+{
+    out[0] = e->root_level;
+    out[1] = (double)e->root_i0;
+    out[2] = (double)e->root_j0;
+    out[3] = e->total_area;
+    out[4] = e->total_mass;
+    out[5] = e->n_nodes;
+}
+
+/* pointwise_fields(tri, s, t, h, hu, hv) (displaced_surface.cpp:116-158):
+ * the metric's sqrt(det G) and the unnormalized normal Su x Sv. */
+static void pointwise_metric(const o_tri *T, double s, double t, double h, double hu, double hv, double *sqrt_det,
+                             v3 *n)
+{
+    o_nframe f = normal_frame_at(T, s, t);
+    v3 e1 = T->e1, e2 = T->e2;
+    double bt00 = -dot3(f.Nu, e1), bt01 = -dot3(f.Nv, e1);
+    double bt10 = -dot3(f.Nu, e2), bt11 = -dot3(f.Nv, e2);
+    double B00 = bt00, B01 = 0.5 * (bt01 + bt10), B11 = bt11;
+    double C00 = dot3(f.Nu, f.Nu), C01 = dot3(f.Nu, f.Nv), C11 = dot3(f.Nv, f.Nv);
+    double a0 = dot3(f.N, e1), a1 = dot3(f.N, e2);
+    double G0_00 = dot3(e1, e1), G0_01 = dot3(e1, e2), G0_11 = dot3(e2, e2); /* displaced_surface.cpp:87-90 */
+    double G00 = (((G0_00 - 2.0 * h * B00) + h * h * C00) + hu * hu) + 2.0 * hu * a0;
+    double G01 = ((((G0_01 - 2.0 * h * B01) + h * h * C01) + hu * hv) + hu * a1) + hv * a0;
+    double G11 = (((G0_11 - 2.0 * h * B11) + h * h * C11) + hv * hv) + 2.0 * hv * a1;
+    double det = G00 * G11 - G01 * G01;
+    *sqrt_det = sqrt(dmax(det, 0.0));
+    v3 Su = add3(add3(e1, mul3(hu, f.N)), mul3(h, f.Nu));
+    v3 Sv = add3(add3(e2, mul3(hv, f.N)), mul3(h, f.Nv));
+    *n = cross3(Su, Sv);
+}
+
+static int admissible(const o_emitter *e, const o_fpchild *info) /* descent_sampler.cpp:115-122 */
+{
+    if (info->overlap == OUTSIDE)
+        return 0;
+    return e->variant == O_DESCENT_AREA ? info->area > 0.0 : info->mass > 0.0;
+}
+
+static o_fpchild child_info(const o_emitter *e, int level, int64_t pi, int64_t pj, const o_fpchild *parent, int c)
+{
+    /* descent_sampler.cpp:124-138 */
+    o_fpchild out = {OUTSIDE, 0.0, 0.0, -1};
+    if (parent->node >= 0)
+        return e->nodes[parent->node].child[c];
+    if (parent->overlap != INSIDE)
+        return out;
+    int64_t i = 2 * pi + (c & 1), j = 2 * pj + (c >> 1);
+    double w = cell_width(e->X->pyr, level);
+    out.overlap = INSIDE;
+    out.area = w * w;
+    out.mass = tile_sum(&e->tile, level, i, j);
+    return out;
+}
+
+typedef struct {
+    v3 x, n;
+} o_receiver;
+
+static double node_weight(const o_emitter *e, int level, int64_t i, int64_t j, const o_fpchild *info,
+                          const o_receiver *rcv) /* descent_sampler.cpp:140-170 */
+{
+    const o_tri *T = e->X->tri;
+    o_node nd = pyramid_node(e->X->pyr, level, i, j);
+    double w = ldexp(1.0, level) / e->X->pyr->n_leaf;
+    double u0 = (i + 0.5) * w, v0 = (j + 0.5) * w;
+    double sqrt_det;
+    v3 fn;
+    pointwise_metric(T, u0, v0, nd.h0, nd.gu, nd.gv, &sqrt_det, &fn);
+    double base = e->variant == O_DESCENT_AREA ? info->area : info->mass;
+    double weight = base * sqrt_det;
+    if (e->variant == O_DESCENT_PRODUCT_GEOMETRY && rcv) {
+        o_nframe nf = normal_frame_at(T, u0, v0);
+        v3 y = add3(tri_P(T, u0, v0), mul3(nd.h0, nf.N));
+        v3 d = sub3(y, rcv->x);
+        double r2 = dmax(dot3(d, d), 1e-12);
+        v3 omega = div3(d, sqrt(r2));
+        double cos_r = dmax(dot3(rcv->n, omega), 0.0);
+        double cos_e = e->emitter_cosine ? fabs(dot3(eigen_normalized(fn), omega)) : 1.0;
+        weight *= cos_r * cos_e / r2;
+    }
+    return weight;
+}
+
+static void child_probs(const o_emitter *e, int level, int64_t pi, int64_t pj, const o_fpchild *parent,
+                        const o_receiver *rcv, double p[4], o_fpchild info[4]) /* descent_sampler.cpp:172-206 */
+{
+    double w[4];
+    int adm[4];
+    int n_adm = 0;
+    double sumw = 0.0;
+    int virtual_root = level > e->root_level;
+    for (int c = 0; c < 4; ++c) {
+        int child_level = level - 1;
+        int64_t i, j;
+        if (virtual_root) {
+            info[c] = e->roots[c];
+            i = e->root_i0 + (c & 1);
+            j = e->root_j0 + (c >> 1);
+        } else {
+            info[c] = child_info(e, child_level, pi, pj, parent, c);
+            i = 2 * pi + (c & 1);
+            j = 2 * pj + (c >> 1);
+        }
+        adm[c] = admissible(e, &info[c]);
+        w[c] = adm[c] ? node_weight(e, child_level, i, j, &info[c], rcv) : 0.0;
+        if (adm[c])
+            ++n_adm;
+        sumw += w[c];
+    }
+    for (int c = 0; c < 4; ++c) {
+        if (!adm[c])
+            p[c] = 0.0;
+        else if (sumw > 0.0)
+            p[c] = (1.0 - e->beta) * w[c] / sumw + e->beta / n_adm;
+        else
+            p[c] = 1.0 / n_adm;
+    }
+}
+
+typedef struct {
+    const float *u;
+    int n, k;
+} o_rng;
+
+static double rng_next(o_rng *r) { return r->k < r->n ? (double)r->u[r->k++] : 0.5; }
+
+static v2 sample_polygon(const o_clip *poly, double xi_tri, double xi1, double xi2) /* uv_clip.cpp:92-115 */
+{
+    double areas[8];
+    double total = 0.0;
+    for (int k = 1; k + 1 < poly->n; ++k) {
+        v2 a = sub2(poly->p[k], poly->p[0]), b = sub2(poly->p[k + 1], poly->p[0]);
+        areas[k] = 0.5 * fabs(a.x * b.y - a.y * b.x);
+        total += areas[k];
+    }
+    double target = xi_tri * total, acc = 0.0;
+    int chosen = poly->n - 2;
+    for (int k = 1; k + 1 < poly->n; ++k) {
+        acc += areas[k];
+        if (target < acc) {
+            chosen = k;
+            break;
+        }
+    }
+    double r = sqrt(xi1);
+    double b1 = 1.0 - r, b2 = r * xi2;
+    return add2(add2(poly->p[0], mul2(b1, sub2(poly->p[chosen], poly->p[0]))),
+                mul2(b2, sub2(poly->p[chosen + 1], poly->p[0])));
+}
+
+int o_emitter_sample(const o_emitter *e, const float *u, int n_u, const double *recv, double *out)
+{
+    /* DescentSampler::sample (descent_sampler.cpp:208-290) */
+    o_rng rng = {u, n_u, 0};
+    o_receiver R, *rcv = NULL;
+    if (recv) {
+        R.x = V3(recv[0], recv[1], recv[2]);
+        R.n = V3(recv[3], recv[4], recv[5]);
+        rcv = &R;
+    }
+    int level = e->root_level + 1;
+    int64_t i = 0, j = 0;
+    o_fpchild cur = {OUTSIDE, 0.0, 0.0, -1};
+    double P = 1.0;
+    for (; level >= 1; --level) {
+        double p[4];
+        o_fpchild info[4];
+        child_probs(e, level, i, j, &cur, rcv, p, info);
+        double xi = rng_next(&rng);
+        int c = -1;
+        double cum = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            cum += p[k];
+            if (xi < cum) {
+                c = k;
+                break;
+            }
+        }
+        if (c < 0 || p[c] == 0.0) {
+            for (int k = 3; k >= 0; --k)
+                if (p[k] > 0.0) {
+                    c = k;
+                    break;
+                }
+        }
+        P *= p[c];
+        if (level > e->root_level) {
+            i = e->root_i0 + (c & 1);
+            j = e->root_j0 + (c >> 1);
+        } else {
+            i = 2 * i + (c & 1);
+            j = 2 * j + (c >> 1);
+        }
+        cur = info[c];
+    }
+    int n = e->X->pyr->n_leaf;
+    double wl = 1.0 / n;
+    double uu, vv;
+    int inside_leaf = cur.overlap == INSIDE;
+    for (int tries = 0;;) {
+        uu = (i + rng_next(&rng)) * wl;
+        vv = (j + rng_next(&rng)) * wl;
+        if (inside_leaf || uvtri_inside(&e->X->domain, V2(uu, vv)))
+            break;
+        if (++tries == 32) {
+            o_clip poly = clip_square(&e->X->domain, V2((i + 0.5) * wl, (j + 0.5) * wl), 0.5 * wl);
+            /* sample_polygon(poly, rng.next(), rng.next(), rng.next()): g++
+             * evaluates these arguments right to left */
+            double x3 = rng_next(&rng), x2 = rng_next(&rng), x1 = rng_next(&rng);
+            v2 s = sample_polygon(&poly, x1, x2, x3);
+            uu = s.x;
+            vv = s.y;
+            break;
+        }
+    }
+    const o_tri *T = e->X->tri;
+    double h = grid_h(e->X->field, uu, vv);
+    v2 gh = grid_grad(e->X->field, uu, vv);
+    double sqrt_det;
+    v3 fn;
+    pointwise_metric(T, uu, vv, h, gh.x, gh.y, &sqrt_det, &fn);
+    v3 p = add3(tri_P(T, uu, vv), mul3(h, normal_frame_at(T, uu, vv).N));
+    v3 nn = eigen_normalized(fn);
+    double pdf_uv = P / cur.area;
+    double o[11] = {uu, vv, p.x, p.y, p.z, nn.x, nn.y, nn.z, sqrt_det, pdf_uv, pdf_uv / sqrt_det};
+    memcpy(out, o, sizeof(o));
+    return rng.k;
+}
+
+static o_receiver *receiver_of(const double *recv, o_receiver *R)
+{
+    if (!recv)
+        return NULL;
+    R->x = V3(recv[0], recv[1], recv[2]);
+    R->n = V3(recv[3], recv[4], recv[5]);
+    return R;
+}
+
+static double leaf_prob(const o_emitter *e, int64_t i, int64_t j, const o_receiver *rcv, o_fpchild *leaf)
+{
+    /* DescentSampler::leaf_prob (descent_sampler.cpp:292-326) */
+    int L = e->root_level;
+    int64_t ri = i >> L, rj = j >> L;
+    int64_t di = ri - e->root_i0, dj = rj - e->root_j0;
+    if (di < 0 || di > 1 || dj < 0 || dj > 1)
+        return 0.0;
+    o_fpchild cur = {OUTSIDE, 0.0, 0.0, -1};
+    double P = 1.0;
+    int64_t pi = 0, pj = 0;
+    for (int level = L + 1; level >= 1; --level) {
+        double p[4];
+        o_fpchild info[4];
+        child_probs(e, level, pi, pj, &cur, rcv, p, info);
+        int c;
+        if (level > L) {
+            c = (int)(di | (dj << 1));
+            pi = ri;
+            pj = rj;
+        } else {
+            int64_t ci = i >> (level - 1), cj = j >> (level - 1);
+            c = (int)((ci - 2 * pi) | ((cj - 2 * pj) << 1));
+            pi = ci;
+            pj = cj;
+        }
+        P *= p[c];
+        cur = info[c];
+        if (P == 0.0)
+            return 0.0;
+    }
+    if (leaf)
+        *leaf = cur;
+    return P;
+}
+
+double o_emitter_leaf_prob(const o_emitter *e, int64_t i, int64_t j, const double *recv)
+{
+    o_receiver R;
+    return leaf_prob(e, i, j, receiver_of(recv, &R), NULL);
+}
+
+double o_emitter_pdf_uv(const o_emitter *e, double u, double v, const double *recv)
+{
+    /* DescentSampler::pdf_uv (descent_sampler.cpp:344-354) */
+    int n = e->X->pyr->n_leaf;
+    int64_t i = (int64_t)floor(u / (1.0 / n)), j = (int64_t)floor(v / (1.0 / n));
+    o_receiver R;
+    o_fpchild leaf;
+    double P = leaf_prob(e, i, j, receiver_of(recv, &R), &leaf);
+    if (P == 0.0)
+        return 0.0;
+    return P / leaf.area;
+}
+
+double o_emitter_pdf_area(const o_emitter *e, double u, double v, const double *recv)
+{
+    /* DescentSampler::pdf_area (descent_sampler.cpp:356-362) */
+    double p = o_emitter_pdf_uv(e, u, v, recv);
+    if (p == 0.0)
+        return 0.0;
+    double h = grid_h(e->X->field, u, v);
+    v2 gh = grid_grad(e->X->field, u, v);
+    double sqrt_det;
+    v3 fn;
+    pointwise_metric(e->X->tri, u, v, h, gh.x, gh.y, &sqrt_det, &fn);
+    return p / sqrt_det;
+}

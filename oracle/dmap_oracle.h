@@ -121,6 +121,26 @@ void o_tessellate_uniform(const o_scene *s, int tri, int n, float *pos, float *u
 int64_t o_tessellate_texel(const o_scene *s, int tri, int m, int64_t cap, float *pos, float *uv, float *nrm,
                            double *st6, int *interior);
 
+/* Displaced-emitter sampling (descent_sampler.h:105-160, emission_tile.h):
+ * the DescentSampler of scene triangle `tri` over its object's height grid
+ * and pyramid, with an emission tile of n x n texels (n = the pyramid's
+ * leaf count, the repeating tile layout), variant 0 AreaOnly, 1 Product,
+ * 2 ProductGeometry, blend floor beta. NULL when n does not match. */
+typedef struct o_emitter o_emitter;
+o_emitter *o_emitter_create(const o_scene *s, int tri, const double *texels, int n, int variant, double beta,
+                            int emitter_cosine);
+void o_emitter_free(o_emitter *e);
+/* root_level, root_i0, root_j0, total_area, total_mass, footprint nodes */
+void o_emitter_info(const o_emitter *e, double *out6);
+/* One sample drawing its random numbers from u[0..n_u) in order (0.5 past
+ * the end); recv6 = receiver position and normal for ProductGeometry (or
+ * NULL). out11 = u, v, p, n, sqrt_det, pdf_uv, pdf_area. Returns the number
+ * of draws used. */
+int o_emitter_sample(const o_emitter *e, const float *u, int n_u, const double *recv6, double *out11);
+double o_emitter_pdf_uv(const o_emitter *e, double u, double v, const double *recv6);
+double o_emitter_pdf_area(const o_emitter *e, double u, double v, const double *recv6);
+double o_emitter_leaf_prob(const o_emitter *e, int64_t i, int64_t j, const double *recv6);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,14 @@ class _Lib:
                                C.POINTER(C.c_uint32))
         self._tess_texel = f("tessellate_texel", C.c_int64, C.c_void_p, C.c_int, C.c_int, C.c_int64, _fp, _fp, _fp,
                              _dp, C.POINTER(C.c_int))
+        self._em_create = f("emitter_create", C.c_void_p, C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, C.c_double,
+                            C.c_int)
+        self._em_free = f("emitter_free", None, C.c_void_p)
+        self._em_info = f("emitter_info", None, C.c_void_p, _dp)
+        self._em_sample = f("emitter_sample", C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_int, _dp, _dp)
+        self._em_pdf_uv = f("emitter_pdf_uv", C.c_double, C.c_void_p, C.c_double, C.c_double, _dp)
+        self._em_pdf_area = f("emitter_pdf_area", C.c_double, C.c_void_p, C.c_double, C.c_double, _dp)
+        self._em_leaf_prob = f("emitter_leaf_prob", C.c_double, C.c_void_p, C.c_int64, C.c_int64, _dp)
         if self.prefix == "o_":
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
                                _dp, _lp, _lp, C.c_int, C.c_int)
@@ -223,3 +231,51 @@ class CpuScene:
                                    _ptr(out["interior"], C.POINTER(C.c_int)))
         assert got == n
         return out
+
+
+VARIANT = {"area": 0, "product": 1, "product_geometry": 2}
+
+
+class CpuEmitter:
+    """DescentSampler of one scene triangle (descent_sampler.h:105-160) on
+    one of the CPU checkers, with an n_leaf x n_leaf emission texel grid."""
+
+    def __init__(self, cpu: CpuScene, tri: int, texels, variant="product", beta=0.05, emitter_cosine=True):
+        self.lib = cpu.lib
+        self.cpu = cpu  # keeps the scene alive
+        t = np.ascontiguousarray(texels, np.float64)
+        self.h = self.lib._em_create(cpu.h, tri, _ptr(t), t.shape[0], VARIANT[variant], beta, int(emitter_cosine))
+        if not self.h:
+            raise ValueError("emission grid does not match the pyramid's leaf count")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib._em_free(self.h)
+            self.h = None
+
+    def info(self):
+        out = np.empty(6)
+        self.lib._em_info(self.h, _ptr(out))
+        return out
+
+    @staticmethod
+    def _recv(receiver):
+        return None if receiver is None else np.ascontiguousarray(receiver, np.float64)
+
+    def sample(self, u, receiver=None):
+        """u: float32 uniforms; returns (11 values u, v, p, n, sqrt_det,
+        pdf_uv, pdf_area, draws used)."""
+        uu = np.ascontiguousarray(u, np.float32)
+        out = np.empty(11)
+        r = self._recv(receiver)
+        k = self.lib._em_sample(self.h, _ptr(uu, C.POINTER(C.c_float)), len(uu), _ptr(r), _ptr(out))
+        return out, k
+
+    def pdf_uv(self, u, v, receiver=None):
+        return self.lib._em_pdf_uv(self.h, u, v, _ptr(self._recv(receiver)))
+
+    def pdf_area(self, u, v, receiver=None):
+        return self.lib._em_pdf_area(self.h, u, v, _ptr(self._recv(receiver)))
+
+    def leaf_prob(self, i, j, receiver=None):
+        return self.lib._em_leaf_prob(self.h, i, j, _ptr(self._recv(receiver)))

@@ -6,6 +6,7 @@
 #include "node_bounds.h"
 #include "taylor_pyramid.h"
 #include "displaced_tessellation.h"
+#include "descent_sampler.h"
 
 #include "../dmap_oracle.h"
 
@@ -322,6 +323,86 @@ int64_t r_tessellate_texel(const r_scene *s, int tri, int m, int64_t cap, float 
         interior[f] = faces[f].interior ? 1 : 0;
     }
     return n;
+}
+
+struct r_emitter
+{
+    std::unique_ptr<dmap::EmissionTile> tile;
+    std::unique_ptr<dmap::DescentSampler> s;
+};
+
+static dmap::Receiver receiver_of(const double *r)
+{
+    dmap::Receiver out;
+    out.x = vec3d(r[0], r[1], r[2]);
+    out.n = vec3d(r[3], r[4], r[5]);
+    return out;
+}
+
+r_emitter *r_emitter_create(const r_scene *s, int tri, const double *texels, int n, int variant, double beta,
+                            int emitter_cosine)
+{
+    int ob, local;
+    const dmap::DisplacedIntersector *X = find_tri(s, tri, &ob, &local);
+    auto *e = new r_emitter;
+    dmap::TextureGrid tg;
+    tg.W = tg.H = n;
+    tg.values.assign(texels, texels + (size_t)n * n);
+    e->tile = std::make_unique<dmap::EmissionTile>(tg);
+    dmap::DescentWeight w = variant == 0   ? dmap::DescentWeight::AreaOnly
+                            : variant == 1 ? dmap::DescentWeight::Product
+                                           : dmap::DescentWeight::ProductGeometry;
+    e->s = std::make_unique<dmap::DescentSampler>(*X->tri, X->field, *X->pyramid, *e->tile, w, beta);
+    e->s->emitter_cosine = emitter_cosine != 0;
+    return e;
+}
+
+void r_emitter_free(r_emitter *e) { delete e; }
+
+void r_emitter_info(const r_emitter *e, double *out)
+{
+    const dmap::Footprint &fp = e->s->footprint;
+    double v[6] = {(double)fp.root_level, (double)fp.root_i0, (double)fp.root_j0, fp.total_area, fp.total_mass,
+                   (double)fp.nodes.size()};
+    std::memcpy(out, v, sizeof(v));
+}
+
+int r_emitter_sample(const r_emitter *e, const float *u, int n_u, const double *recv, double *out)
+{
+    ks::RNG rng;
+    rng.u = u;
+    rng.n = n_u;
+    dmap::Receiver r;
+    if (recv)
+        r = receiver_of(recv);
+    dmap::DescentSample d = e->s->sample(rng, recv ? &r : nullptr);
+    double v[11] = {d.u, d.v, d.p[0], d.p[1], d.p[2], d.n[0], d.n[1], d.n[2], d.sqrt_det, d.pdf_uv, d.pdf_area};
+    std::memcpy(out, v, sizeof(v));
+    return rng.k;
+}
+
+double r_emitter_pdf_uv(const r_emitter *e, double u, double v, const double *recv)
+{
+    dmap::Receiver r;
+    if (recv)
+        r = receiver_of(recv);
+    return e->s->pdf_uv(u, v, recv ? &r : nullptr);
+}
+
+double r_emitter_pdf_area(const r_emitter *e, double u, double v, const double *recv)
+{
+    dmap::Receiver r;
+    if (recv)
+        r = receiver_of(recv);
+    return e->s->pdf_area(u, v, recv ? &r : nullptr);
+}
+
+double r_emitter_leaf_prob(const r_emitter *e, int64_t i, int64_t j, const double *recv)
+{
+    dmap::Receiver r;
+    if (recv)
+        r = receiver_of(recv);
+    return e->s->leaf_prob(i, j, recv ? &r : nullptr);
 }
 
 } // extern "C"

@@ -184,6 +184,13 @@ struct Matrix
             m = std::max(m, v[k]);
         return m;
     }
+    T minCoeff() const
+    {
+        T m = v[0];
+        for (int k = 1; k < R * C; ++k)
+            m = std::min(m, v[k]);
+        return m;
+    }
     bool allFinite() const
     {
         for (int k = 0; k < R * C; ++k)
