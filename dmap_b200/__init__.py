@@ -91,6 +91,11 @@ class _UvMap(C.Structure):
     _fields_ = [("uv_scale", C.c_double * 2), ("uv_offset", C.c_double * 2), ("flip_v", C.c_int)]
 
 
+# dmap_emitter_point
+EMITTER_POINT = np.dtype([("u", "<f8"), ("v", "<f8"), ("p", "<f8", 3), ("n", "<f8", 3), ("sqrt_det", "<f8"),
+                          ("pdf_uv", "<f8"), ("pdf_area", "<f8"), ("tri", "<i4"), ("draws", "<i4")])
+DESCENT = {"area": 0, "product": 1, "product_geometry": 2}
+
 # dmap_texel_face: triangle, interior, st[3][2]
 TEXEL_FACE = np.dtype([("triangle", np.int32), ("interior", np.int32), ("st", np.float64, (3, 2))])
 
@@ -148,6 +153,13 @@ def lib() -> C.CDLL:
             "dmap_tessellate_uniform_host": (i32, [vp, i32, vp, vp, vp, vp]),
             "dmap_tessellate_texel": (i32, [vp, i32, i64, vp, vp, vp, vp, C.POINTER(i64), vp]),
             "dmap_tessellate_texel_host": (i32, [vp, i32, i64, vp, vp, vp, vp, C.POINTER(i64)]),
+            "dmap_emitter_create": (i32, [vp, vp, i32, dbl, i32, C.POINTER(vp)]),
+            "dmap_emitter_destroy": (None, [vp]),
+            "dmap_emitter_triangle_info": (i32, [vp, i32, vp]),
+            "dmap_emitter_sample": (i32, [vp, vp, vp, i32, vp, i64, vp, vp]),
+            "dmap_emitter_pdf": (i32, [vp, vp, vp, vp, i64, vp, vp, vp]),
+            "dmap_emitter_sample_host": (i32, [vp, vp, vp, i32, vp, i64, vp]),
+            "dmap_emitter_pdf_host": (i32, [vp, vp, vp, vp, i64, vp, vp]),
             "dmap_server_create": (i32, [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]),
             "dmap_server_destroy": (None, [vp]),
             "dmap_server_submit_rays": (i32, [vp, vp, vp, i64, i32, vp, C.POINTER(C.c_uint64)]),
@@ -520,6 +532,72 @@ class Server:
             lib().dmap_server_destroy(self.h)
         self.h = None
         self._bufs.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Emitter:
+    """DescentSampler for every triangle of a scene (dmap_emitter_*):
+    texels is one n_leaf x n_leaf emission grid per scene asset (None: a
+    uniform emission of 1 everywhere, or None entries per asset)."""
+
+    def __init__(self, scene: Scene, texels=None, variant: str = "product", beta: float = 0.05,
+                 emitter_cosine: bool = True):
+        self.scene = scene
+        self.ctx = scene.ctx
+        keep = []
+        arr = None
+        if texels is not None:
+            ptrs = []
+            for t in texels:
+                if t is None:
+                    ptrs.append(None)
+                else:
+                    a = np.ascontiguousarray(t, np.float64)
+                    keep.append(a)
+                    ptrs.append(a.ctypes.data)
+            arr = (C.c_void_p * len(ptrs))(*ptrs)
+        h = C.c_void_p()
+        self.ctx.check(lib().dmap_emitter_create(scene.h, arr, DESCENT[variant], beta, int(emitter_cosine),
+                                                 C.byref(h)), "dmap_emitter_create")
+        self.h = h
+
+    def triangle_info(self, tri: int) -> np.ndarray:
+        out = np.empty(6)
+        self.ctx.check(lib().dmap_emitter_triangle_info(self.h, tri, out.ctypes.data), "dmap_emitter_triangle_info")
+        return out
+
+    def sample(self, tri, uniforms, receivers=None) -> np.ndarray:
+        """Samples on triangles tri (n,) from float32 uniforms (n, K):
+        EMITTER_POINT records."""
+        t = np.ascontiguousarray(tri, np.int32)
+        u = np.ascontiguousarray(uniforms, np.float32).reshape(len(t), -1)
+        r = None if receivers is None else np.ascontiguousarray(receivers, np.float64).reshape(len(t), 6)
+        out = np.empty(len(t), EMITTER_POINT)
+        self.ctx.check(lib().dmap_emitter_sample_host(self.h, t.ctypes.data, u.ctypes.data, u.shape[1],
+                                                      None if r is None else r.ctypes.data, len(t),
+                                                      out.ctypes.data), "dmap_emitter_sample_host")
+        return out
+
+    def pdf(self, tri, uv, receivers=None):
+        """(pdf_uv, pdf_area) at points uv (n, 2) of triangles tri (n,)."""
+        t = np.ascontiguousarray(tri, np.int32)
+        q = np.ascontiguousarray(uv, np.float64).reshape(len(t), 2)
+        r = None if receivers is None else np.ascontiguousarray(receivers, np.float64).reshape(len(t), 6)
+        pu, pa = np.empty(len(t)), np.empty(len(t))
+        self.ctx.check(lib().dmap_emitter_pdf_host(self.h, t.ctypes.data, q.ctypes.data,
+                                                   None if r is None else r.ctypes.data, len(t), pu.ctypes.data,
+                                                   pa.ctypes.data), "dmap_emitter_pdf_host")
+        return pu, pa
+
+    def close(self):
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
+            lib().dmap_emitter_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         try:

@@ -2,7 +2,7 @@
 
 The translation units with FP64 arithmetic that must round like the
 reference (pyramid.cu, setup.cu, walk64.cu, walk32.cu for its FP64 leaf,
-shade.cu, tess.cu)
+shade.cu, tess.cu, emitter.cu)
 are compiled with -fmad=false so that each double operation rounds on its
 own, as the reference's CPU build does; FP32 code there asks for fused
 multiply-adds explicitly (fmaf, __fmaf_ru).
@@ -25,7 +25,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libdmap_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-I", str(CSRC)]
-EXACT_FP64 = {"pyramid.cu", "setup.cu", "walk64.cu", "walk32.cu", "shade.cu", "tess.cu"}
+EXACT_FP64 = {"pyramid.cu", "setup.cu", "walk64.cu", "walk32.cu", "shade.cu", "tess.cu", "emitter.cu"}
 
 
 def nvcc() -> str:

@@ -128,44 +128,6 @@ struct TexelRange
     int64_t tile_first, tiles_x; // tiles of the m = 1 emit pass, row-major over the range
 };
 
-struct ClipPoly
-{
-    int n;
-    v2 p[8];
-};
-
-// clip_square (uv_clip.cpp:61-90): Sutherland-Hodgman of the square (c, s)
-// against the domain's three inward half-planes.
-__device__ inline ClipPoly clip_square(const TriDev &T, v2 c, double s)
-{
-    ClipPoly in;
-    in.n = 4;
-    in.p[0] = add2(c, V2(-s, -s));
-    in.p[1] = add2(c, V2(s, -s));
-    in.p[2] = add2(c, V2(s, s));
-    in.p[3] = add2(c, V2(-s, s));
-    for (int k = 0; k < 3; ++k) {
-        ClipPoly out;
-        out.n = 0;
-        v2 nk = L2(T.un[k]);
-        double dk = T.ud[k];
-        for (int a = 0; a < in.n; ++a) {
-            v2 pa = in.p[a], pb = in.p[a + 1 == in.n ? 0 : a + 1];
-            double fa = dot2(nk, pa) - dk, fb = dot2(nk, pb) - dk;
-            if (fa >= 0.0)
-                out.p[out.n++] = pa;
-            if ((fa >= 0.0) != (fb >= 0.0)) {
-                double t = fa / (fa - fb);
-                out.p[out.n++] = add2(pa, mul2(t, sub2(pb, pa)));
-            }
-        }
-        in = out;
-        if (in.n == 0)
-            break;
-    }
-    return in;
-}
-
 __device__ __forceinline__ int find_triangle(const TexelRange *__restrict__ ranges, int n_tri, int64_t cell)
 {
     int lo = 0, hi = n_tri - 1; // last range with first <= cell

@@ -304,6 +304,65 @@ dmap_status dmap_tessellate_texel_host(dmap_scene *scene, int m, int64_t capacit
                                        float *texcoords, float *normals, dmap_texel_face *faces, int64_t *n_faces);
 
 /*
+ * Displaced-emitter sampling: DescentSampler (descent_sampler.h:105-160,
+ * descent_sampler.cpp:85-362) for every triangle of a scene, over an
+ * EmissionTile per asset (emission_tile.h:40-88, the texture's own
+ * repeating tile: texels_host[a] is the asset's n_leaf x n_leaf texel grid,
+ * row major, or NULL for a uniform emission of 1). variant: AreaOnly,
+ * Product or ProductGeometry (DescentWeight); beta: the uniform blend floor;
+ * emitter_cosine: ProductGeometry's |emitter cosine| factor. The descent
+ * weights read the FP64 pyramid, so the scene's assets need
+ * DMAP_ASSET_KEEP_F64. Built once on the host (each triangle's footprint:
+ * root block and straddling tree with exact clipped areas and masses) and
+ * uploaded.
+ */
+#define DMAP_DESCENT_AREA 0
+#define DMAP_DESCENT_PRODUCT 1
+#define DMAP_DESCENT_PRODUCT_GEOMETRY 2
+typedef struct dmap_emitter dmap_emitter;
+dmap_status dmap_emitter_create(dmap_scene *scene, const double *const *texels_host, int variant, double beta,
+                                int emitter_cosine, dmap_emitter **out);
+/* An emitter borrows its scene for queries: destroy it before the scene's
+ * context (destroying it after the scene is allowed). */
+void dmap_emitter_destroy(dmap_emitter *emitter);
+/* Footprint of one triangle: root_level, root_i0, root_j0, total clipped
+ * area, total clipped mass, straddling nodes (6 doubles). */
+dmap_status dmap_emitter_triangle_info(const dmap_emitter *emitter, int tri, double *out6);
+/*
+ * DescentSampler::sample for n samples: sample k on triangle tri_dev[k]
+ * draws its random numbers, in the reference's order (one per descent level,
+ * two per leaf try, three for the clipped-polygon fallback after 32 misses),
+ * from uniforms_dev[k * uniforms_per_sample ...] (0.5 past the end; 2^L + 70
+ * covers every path), and receivers_dev (6 doubles per sample: position,
+ * unit normal; NULL = none) steers ProductGeometry. draws = the uniforms
+ * used, -1 for a bad triangle or one without mass. Asynchronous on stream.
+ */
+typedef struct dmap_emitter_point {
+    double u, v;     /* texture coordinates */
+    double p[3];     /* S(u, v) */
+    double n[3];     /* unit surface normal */
+    double sqrt_det; /* pointwise sqrt(det G) */
+    double pdf_uv;   /* per unit parameter area */
+    double pdf_area; /* per unit surface area */
+    int32_t tri, draws;
+} dmap_emitter_point;
+dmap_status dmap_emitter_sample(dmap_emitter *emitter, const int32_t *tri_dev, const float *uniforms_dev,
+                                int uniforms_per_sample, const double *receivers_dev, int64_t n,
+                                dmap_emitter_point *out_dev, void *stream);
+/* DescentSampler::pdf_uv / pdf_area (descent_sampler.cpp:344-362) at n
+ * points (uv_dev: 2 doubles each) of triangles tri_dev; pdf_area_dev may be
+ * NULL. The re-walk equals the sampled pdf at sampled points. */
+dmap_status dmap_emitter_pdf(dmap_emitter *emitter, const int32_t *tri_dev, const double *uv_dev,
+                             const double *receivers_dev, int64_t n, double *pdf_uv_dev, double *pdf_area_dev,
+                             void *stream);
+/* The same two on host buffers (synchronous). */
+dmap_status dmap_emitter_sample_host(dmap_emitter *emitter, const int32_t *tri, const float *uniforms,
+                                     int uniforms_per_sample, const double *receivers, int64_t n,
+                                     dmap_emitter_point *out);
+dmap_status dmap_emitter_pdf_host(dmap_emitter *emitter, const int32_t *tri, const double *uv,
+                                  const double *receivers, int64_t n, double *pdf_uv, double *pdf_area);
+
+/*
  * Schedule autotuner (no counterpart in the reference). Times the wavefront
  * schedule's launch shapes (rounds x blocks_per_sm) with `base`'s other
  * options on the first min(n, 2^22) of the caller's device rays and returns
