@@ -64,6 +64,9 @@ struct dmap_scene
     float *block_box_dev = nullptr; // more than 256 triangles: boxes of blocks of 32 (QueryOpts::block_box)
     float *block_tree_dev = nullptr; // more than 8192 triangles: the tree over those boxes (QueryOpts::block_tree)
     int tree_leaves = 0, tree_log2 = 0;
+    int *cluster_tri_dev = nullptr;    // more than 256 triangles: spatial clusters for the nearest-first order
+    float *cluster_box_dev = nullptr;
+    float *cluster_tree_dev = nullptr;
     std::vector<TriDev> tris_host;
     bool all_f64 = true;
 };

@@ -31,6 +31,12 @@ struct QueryOpts
     // tree_leaves .. 2 tree_leaves - 1 in block order; tree_leaves = 2^tree_log2).
     const float *block_tree = nullptr;
     int tree_leaves = 0, tree_log2 = 0;
+    // The same for the nearest-first order over spatial clusters: cluster c
+    // holds triangles cluster_tri[32c .. 32c + 31] (Morton order of their box
+    // centres), with its box and, past 8192 triangles, the tree over them.
+    const int *cluster_tri = nullptr;
+    const float *cluster_box = nullptr;
+    const float *cluster_tree = nullptr;
 };
 
 constexpr int kMaxRounds = 32;

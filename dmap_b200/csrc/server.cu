@@ -232,6 +232,9 @@ struct dmap_server
             qq.block_tree = first->scene->block_tree_dev;
             qq.tree_leaves = first->scene->tree_leaves;
             qq.tree_log2 = first->scene->tree_log2;
+            qq.cluster_tri = first->scene->cluster_tri_dev;
+            qq.cluster_box = first->scene->cluster_box_dev;
+            qq.cluster_tree = first->scene->cluster_tree_dev;
             qq.ray_dtype = qq.hit_dtype = 0;
             dmap_scene *s = first->scene;
             if (e == cudaSuccess)

@@ -366,6 +366,12 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     // the flat loops below are never compiled into the hot kernels)
     constexpr bool use_blocks = TOPM == 1;
     constexpr bool use_mask = TOPM <= 1;
+    // the nearest-first order takes its candidates by spatial clusters (the
+    // triangles of cluster c: cluster_tri[32c ..]), the index order by blocks
+    // of consecutive triangles
+    const bool clustered = opt.order == 1 && opt.cluster_tri != nullptr;
+    const float *const item_box = clustered ? opt.cluster_box : opt.block_box;
+    const float *const item_tree = clustered ? opt.cluster_tree : opt.block_tree;
     const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
@@ -518,7 +524,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     int t = 32 * w + lane;
                     float t1 = s_tmax;
                     bool pass = t < n_items &&
-                                (use_blocks ? box_pass(opt.block_box + 6 * t, opt.block_box + 6 * t + 3, so, sd, sv,
+                                (use_blocks ? box_pass(item_box + 6 * t, item_box + 6 * t + 3, so, sd, sv,
                                                        s_tmin, t1)
                                             : object_box(tris32[t], so, sd, sv, s_tmin, t1));
                     unsigned bits = __ballot_sync(FULL, pass);
@@ -564,7 +570,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     auto blocks = [&](auto &&fn) {
                         if (TOPM == 2) {
                             for (int b = 0; b < nb; ++b) {
-                                b = tree_next(opt.block_tree, opt.tree_leaves, opt.tree_log2, nb, b, of, df, invf,
+                                b = tree_next(item_tree, opt.tree_leaves, opt.tree_log2, nb, b, of, df, invf,
                                               tmin_f, tmf);
                                 if (b < 0)
                                     break;
@@ -588,7 +594,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     };
                     auto entry = [&](int b, float &e) {
                         float t0 = tmin_f, t1b = tmf;
-                        const bool ok = box_range(opt.block_box + 6 * b, opt.block_box + 6 * b + 3, of, df, invf, t0,
+                        const bool ok = box_range(item_box + 6 * b, item_box + 6 * b + 3, of, df, invf, t0,
                                                   t1b);
                         e = t0;
                         return ok;
@@ -602,15 +608,17 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                             e0 = e;
                         }
                     });
+                    auto scan = [&](int b) {
+                        for (int q = 32 * b, stop = min(n_tri, 32 * b + 32); q < stop; ++q)
+                            consider(clustered ? opt.cluster_tri[q] : q);
+                    };
                     if (b0 >= 0) {
-                        for (int t = 32 * b0, stop = min(n_tri, 32 * b0 + 32); t < stop; ++t)
-                            consider(t);
+                        scan(b0);
                         blocks([&](int b) {
                             float e;
                             if (b == b0 || !entry(b, e) || (bt >= 0 && (double)e > bk))
                                 return;
-                            for (int t = 32 * b, stop = min(n_tri, 32 * b + 32); t < stop; ++t)
-                                consider(t);
+                            scan(b);
                         });
                     }
                 } else if (use_mask) {
