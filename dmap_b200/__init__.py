@@ -552,8 +552,12 @@ class Emitter:
         keep = []
         arr = None
         if texels is not None:
+            if len(texels) != len(scene.assets):
+                raise ValueError(f"one emission grid per scene asset: {len(texels)} for {len(scene.assets)}")
             ptrs = []
-            for t in texels:
+            for a_, t in zip(scene.assets, texels):
+                if t is not None and np.shape(t) != (a_.n_leaf, a_.n_leaf):
+                    raise ValueError(f"emission grid {np.shape(t)} does not match {a_.n_leaf}^2 leaf cells")
                 if t is None:
                     ptrs.append(None)
                 else:

@@ -349,7 +349,7 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // One lane's walk from its parked or fresh state to the next leaf (parked,
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
-template <bool ST, bool INLINE_LEAF, int TOPM, typename R, typename H, typename Fp>
+template <bool ST, bool INLINE_LEAF, int TOPM, bool NEAR, typename R, typename H, typename Fp>
 __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     // the nearest-first order takes its candidates by spatial clusters (the
     // triangles of cluster c: cluster_tri[32c ..]), the index order by blocks
     // of consecutive triangles
-    const bool clustered = opt.order == 1 && opt.cluster_tri != nullptr;
+    const bool clustered = NEAR && opt.cluster_tri != nullptr;
     const float *const item_box = clustered ? opt.cluster_box : opt.block_box;
     const float *const item_tree = clustered ? opt.cluster_tree : opt.block_tree;
     const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
         if (phase == TOP) {
             float t1 = 0.0f;
             bool hit_box = false;
-            if (opt.order == 1) {
+            if (NEAR) {
                 // nearest box entry first: the smallest (key, index) past the
                 // cursor among the candidates the ray still reaches
                 double inv[3];
@@ -1130,12 +1130,17 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
                                                                                                     : 0;
         if (topm == 0 && n_tri > 32 * kMaskWords)
             return cudaErrorInvalidValue; // a scene without its block boxes (every scene has them)
-#define DMAP_WALK_LAUNCH(ST_, IL_, TM_)                                                                             \
-    wave_walk<ST_, IL_, TM_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,           \
-                                                                 ST_ ? stats : nullptr, states, q_in, rd, leaves, \
-                                                                 ws.counters, status)
+        // (the triangle order is a template argument too, so each instance
+        // carries the code of one order only)
+        const bool nearest = opt.order == 1;
+#define DMAP_WALK_LAUNCH(ST_, IL_, TM_, NR_)                                                                        \
+    wave_walk<ST_, IL_, TM_, NR_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,      \
+                                                                      ST_ ? stats : nullptr, states, q_in, rd,    \
+                                                                      leaves, ws.counters, status)
+#define DMAP_WALK_ORDER(ST_, IL_, TM_)                                                                              \
+    (nearest ? DMAP_WALK_LAUNCH(ST_, IL_, TM_, true) : DMAP_WALK_LAUNCH(ST_, IL_, TM_, false))
 #define DMAP_WALK_TOPM(ST_, IL_)                                                                                    \
-    (topm == 1 ? DMAP_WALK_LAUNCH(ST_, IL_, 1) : topm == 2 ? DMAP_WALK_LAUNCH(ST_, IL_, 2) : DMAP_WALK_LAUNCH(ST_, IL_, 0))
+    (topm == 1 ? DMAP_WALK_ORDER(ST_, IL_, 1) : topm == 2 ? DMAP_WALK_ORDER(ST_, IL_, 2) : DMAP_WALK_ORDER(ST_, IL_, 0))
         if (stats) {
             if (last)
                 DMAP_WALK_TOPM(true, true);
@@ -1148,6 +1153,7 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
                 DMAP_WALK_TOPM(false, false);
         }
 #undef DMAP_WALK_TOPM
+#undef DMAP_WALK_ORDER
 #undef DMAP_WALK_LAUNCH
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
