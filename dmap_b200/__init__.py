@@ -138,6 +138,7 @@ def lib() -> C.CDLL:
             "dmap_asset_build_ms": (dbl, [vp]),
             "dmap_asset_pyramid_level": (i32, [vp, i32, i32, vp]),
             "dmap_scene_create": (i32, [vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
+            "dmap_scene_create_instanced": (i32, [vp, vp, i32, vp, vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
             "dmap_scene_destroy": (None, [vp]),
             "dmap_scene_triangle_count": (i32, [vp]),
             "dmap_scene_triangle_info": (i32, [vp, i32, vp]),
@@ -314,6 +315,29 @@ class Scene:
                                           C.byref(h)), "dmap_scene_create")
         self.h = h
         self.n_tri = len(t)
+
+    @classmethod
+    def instanced(cls, ctx: Context, assets: Sequence[Asset], tris: np.ndarray, tri_asset: np.ndarray,
+                  object_first: Sequence[int], instance_object: Sequence[int], to_world: np.ndarray):
+        """dmap_scene_create_instanced: objects are triangle ranges
+        (object_first, n_objects + 1 offsets), instances (object, 3x4 rigid
+        to_world) expanded in order."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.assets = list(assets)
+        t = np.ascontiguousarray(tris, np.float64).reshape(-1, 24)
+        ta = np.ascontiguousarray(tri_asset, np.int32)
+        of = np.ascontiguousarray(object_first, np.int32)
+        io = np.ascontiguousarray(instance_object, np.int32)
+        M = np.ascontiguousarray(to_world, np.float64).reshape(-1, 12)
+        arr = (C.c_void_p * len(self.assets))(*[a.h.value for a in self.assets])
+        h = C.c_void_p()
+        ctx.check(lib().dmap_scene_create_instanced(ctx.h, arr, len(self.assets), ta.ctypes.data, t.ctypes.data,
+                                                    of.ctypes.data, len(of) - 1, io.ctypes.data, M.ctypes.data,
+                                                    len(io), C.byref(h)), "dmap_scene_create_instanced")
+        self.h = h
+        self.n_tri = lib().dmap_scene_triangle_count(h)
+        return self
 
     @classmethod
     def from_synthetic(cls, ctx: Context, scene, keep_f64: bool = False, build: str = "fold"):

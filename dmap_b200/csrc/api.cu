@@ -440,6 +440,58 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
     return DMAP_OK;
 }
 
+dmap_status dmap_scene_create_instanced(dmap_context *ctx, dmap_asset *const *assets, int n_assets,
+                                        const int *tri_asset, const double *tris, const int *object_first,
+                                        int n_objects, const int *instance_object, const double *to_world,
+                                        int n_instances, dmap_scene **out)
+{
+    if (!ctx || !tri_asset || !tris || !object_first || n_objects <= 0 || !instance_object || !to_world ||
+        n_instances <= 0 || !out)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: bad argument");
+    for (int o = 0; o < n_objects; ++o)
+        if (object_first[o] < 0 || object_first[o + 1] < object_first[o])
+            return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: object ranges must be ordered");
+    std::vector<double> wt;
+    std::vector<int> wa;
+    for (int k = 0; k < n_instances; ++k) {
+        const int o = instance_object[k];
+        if (o < 0 || o >= n_objects)
+            return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: instance object out of range");
+        const double *M = to_world + 12 * (size_t)k;
+        for (int q = 0; q < 12; ++q)
+            if (!std::isfinite(M[q]))
+                return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: non-finite transform");
+        // rigid: the rotation part is orthogonal (R R^T = I within 1e-9)
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                const double dot = (M[4 * a] * M[4 * b] + M[4 * a + 1] * M[4 * b + 1]) + M[4 * a + 2] * M[4 * b + 2];
+                if (std::fabs(dot - (a == b ? 1.0 : 0.0)) > 1e-9)
+                    return fail(ctx, DMAP_ERR_UNSUPPORTED,
+                                "dmap_scene_create_instanced: only rigid transforms move the displaced surface "
+                                "exactly (a scale or shear would scale the heights)");
+            }
+        auto point = [&](const double *p, double *q, bool translate) {
+            for (int a = 0; a < 3; ++a)
+                q[a] = ((M[4 * a] * p[0] + M[4 * a + 1] * p[1]) + M[4 * a + 2] * p[2]) + (translate ? M[4 * a + 3] : 0.0);
+        };
+        for (int t = object_first[o]; t < object_first[o + 1]; ++t) {
+            const double *r = tris + 24 * (size_t)t;
+            double w[24];
+            for (int v = 0; v < 3; ++v) {
+                point(r + 3 * v, w + 3 * v, true);      // p0, p1, p2
+                point(r + 9 + 3 * v, w + 9 + 3 * v, false); // m0, m1, m2
+            }
+            for (int q = 18; q < 24; ++q)
+                w[q] = r[q];
+            wt.insert(wt.end(), w, w + 24);
+            wa.push_back(tri_asset[t]);
+        }
+    }
+    if (wa.empty())
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: no triangles");
+    return dmap_scene_create(ctx, assets, n_assets, wa.data(), wt.data(), (int)wa.size(), out);
+}
+
 void dmap_scene_destroy(dmap_scene *s)
 {
     if (!s)

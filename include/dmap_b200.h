@@ -126,6 +126,26 @@ dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dtype dtype, 
  */
 dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset_host,
                               const double *tris_host, int n_tri, dmap_scene **out);
+/*
+ * Scene-level instancing: the reference's scene objects placed by their
+ * to_world transforms as embree instances (displaced_scene.cpp:79-87,
+ * Builder::add_instance). Objects are consecutive ranges of the base
+ * triangles: object o holds triangles object_first[o] .. object_first[o+1]-1
+ * of tris_host / tri_asset_host (n_objects + 1 offsets). Instance k places
+ * object instance_object[k] by the row-major 3x4 matrix instance_to_world +
+ * 12 k (rotation R, translation t). The scene holds, for every instance in
+ * order, its object's triangles moved to world space (positions R p + t,
+ * vertex normals R m; texture coordinates and assets unchanged), so the
+ * instances share the assets' pyramids; hit.tri counts through the
+ * instances' triangles in that order. Only rigid transforms (R orthogonal
+ * within 1e-9, mirrors included) are taken: a rigid motion moves the
+ * displaced surface exactly, S = R (P + h N) + t = (R P + t) + h (R N); a
+ * scale or shear would also scale the heights (DMAP_ERR_UNSUPPORTED).
+ */
+dmap_status dmap_scene_create_instanced(dmap_context *ctx, dmap_asset *const *assets, int n_assets,
+                                        const int *tri_asset_host, const double *tris_host,
+                                        const int *object_first, int n_objects, const int *instance_object,
+                                        const double *instance_to_world, int n_instances, dmap_scene **out);
 void dmap_scene_destroy(dmap_scene *scene);
 int dmap_scene_triangle_count(const dmap_scene *scene);
 /*
