@@ -599,20 +599,49 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                         e = t0;
                         return ok;
                     };
+                    // the groups the ray reaches, sorted by entry bound (up to
+                    // kGroupList of them); then scanned nearest first until
+                    // a group's bound passes the best key. Past kGroupList
+                    // candidates: the nearest group first, then every group
+                    // whose bound is not beyond the best key.
+                    constexpr int kGroupList = 24;
+                    int gl_b[kGroupList];
+                    float gl_e[kGroupList];
+                    int n_gl = 0;
+                    bool overflow = false;
                     int b0 = -1;
                     float e0 = INFINITY;
                     blocks([&](int b) {
                         float e;
-                        if (entry(b, e) && (b0 < 0 || e < e0)) {
+                        if (!entry(b, e))
+                            return;
+                        if (b0 < 0 || e < e0) {
                             b0 = b;
                             e0 = e;
                         }
+                        if (n_gl == kGroupList) {
+                            overflow = true;
+                            return;
+                        }
+                        int k = n_gl++;
+                        for (; k > 0 && gl_e[k - 1] > e; --k) {
+                            gl_e[k] = gl_e[k - 1];
+                            gl_b[k] = gl_b[k - 1];
+                        }
+                        gl_e[k] = e;
+                        gl_b[k] = b;
                     });
                     auto scan = [&](int b) {
                         for (int q = 32 * b, stop = min(n_tri, 32 * b + 32); q < stop; ++q)
                             consider(clustered ? opt.cluster_tri[q] : q);
                     };
-                    if (b0 >= 0) {
+                    if (!overflow) {
+                        for (int k = 0; k < n_gl; ++k) {
+                            if (bt >= 0 && (double)gl_e[k] > bk)
+                                break;
+                            scan(gl_b[k]);
+                        }
+                    } else if (b0 >= 0) {
                         scan(b0);
                         blocks([&](int b) {
                             float e;
