@@ -72,3 +72,19 @@ def test_sampler_properties(oracle):
         total = sum(e.leaf_prob(int(i0) * (1 << int(root_level)) + a, int(j0) * (1 << int(root_level)) + b)
                     for a in range(span) for b in range(span))
         assert abs(total - 1.0) < 1e-12
+
+
+def test_sampler_without_emitter_cosine(oracle, reference):
+    """ProductGeometry without the |emitter cosine| factor."""
+    sc = helpers.chart_scene(32)
+    so, sr = py_oracle.CpuScene(oracle, sc), py_oracle.CpuScene(reference, sc)
+    rng = np.random.default_rng(4)
+    for t in range(so.n_tri):
+        tex = _texels(sc.assets[sc.tri_asset[t]].n_leaf, 50 + t)
+        eo = py_oracle.CpuEmitter(so, t, tex, "product_geometry", beta=0.2, emitter_cosine=False)
+        er = py_oracle.CpuEmitter(sr, t, tex, "product_geometry", beta=0.2, emitter_cosine=False)
+        for _ in range(60):
+            u = rng.random(64).astype(np.float32)
+            a, ka = eo.sample(u, RECV)
+            b, kb = er.sample(u, RECV)
+            assert ka == kb and np.array_equal(a, b)
