@@ -198,7 +198,7 @@ typedef struct dmap_options {
     int precision;      /* DMAP_PRECISION_*, default F32 */
     int mode;           /* DMAP_MODE_*, default CLOSEST */
     double polish_cond; /* reserved for an FP32 leaf with FP64 refinement above this cond(J) (default
-                           1e4); this build's leaves are FP64 throughout and ignore it */
+                           1e4); the library's leaves are FP64 throughout and ignore it */
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
                            default 6; 0 = one walk with every leaf inline) */
@@ -224,7 +224,7 @@ typedef struct dmap_hit64 {
     int32_t tri, i, j, flags;
 } dmap_hit64;
 /* dmap_hit*.flags bits */
-#define DMAP_HIT_FP64_LEAF 1 /* the root came from the FP64 certified Newton leaf (every hit of this build) */
+#define DMAP_HIT_FP64_LEAF 1 /* the root came from the FP64 certified Newton leaf (every hit the library returns) */
 #define DMAP_HIT_CAPPED 2   /* a device iteration cap ran out for this ray */
 
 /* Per-ray counters (TraversalStats, displaced_intersector.h:89-105), 8 int64 per ray. */
