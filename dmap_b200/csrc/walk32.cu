@@ -57,6 +57,12 @@ using dmapdev::TriDev32;
 #define DMAP_STALE_CAP 32
 #endif
 
+// The smallest candidate-mode (TOPM below) whose nearest-order picks test a
+// triangle's float box before its FP64 key.
+#ifndef DMAP_BOX_FIRST_TOPM
+#define DMAP_BOX_FIRST_TOPM 1
+#endif
+
 constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the object-box candidate mask
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -373,6 +379,9 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     const float *const item_box = clustered ? opt.cluster_box : opt.block_box;
     const float *const item_tree = clustered ? opt.cluster_tree : opt.block_tree;
     const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
+    // nearest order: test a candidate's float box before its FP64 key (the
+    // group scans of large scenes, where most of a group's boxes miss)
+    constexpr bool kBoxFirst = TOPM >= DMAP_BOX_FIRST_TOPM;
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
     if (round == 0 && opt.n_dev && (unsigned long long)*opt.n_dev < count)
@@ -552,11 +561,19 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 int bt = -1;
                 const float tmf = __double2float_ru(t_max);
                 auto consider = [&](int t) {
+                    float tt = tmf;
+                    if (kBoxFirst) {
+                        // the float box first: its entry e is a lower bound of
+                        // the key, so past the best key the FP64 key is not needed
+                        float e = tmin_f;
+                        if (!box_range(tris32[t].box_lo, tris32[t].box_hi, of, df, invf, e, tt) ||
+                            (bt >= 0 && (double)e > bk))
+                            return;
+                    }
                     const double key = d64::entry_key(tris64[t], o, d, inv, t_min);
                     if (!d64::after_cursor(key, t, ckey, cidx) || !d64::before_best(key, t, bk, bt))
                         return;
-                    float tt = tmf;
-                    if (!object_box(tris32[t], of, df, invf, tmin_f, tt))
+                    if (!kBoxFirst && !object_box(tris32[t], of, df, invf, tmin_f, tt))
                         return;
                     bk = key;
                     bt = t;
