@@ -43,6 +43,7 @@ SCHEDULE = {"wavefront": 0, "simple": 1}
 ORDER = {"index": 0, "nearest": 1}
 KEEP_F64, BUILD_DIRECT = 1, 2
 OK, ERR_INVALID, ERR_CUDA, ERR_OOM = 0, 1, 2, 3  # dmap_status
+ERR_UNSUPPORTED = 8
 
 HIT32 = np.dtype([("t", "<f4"), ("st", "<f4", 2), ("bary", "<f4", 2), ("ng", "<f4", 3), ("tri", "<i4"),
                   ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
@@ -150,6 +151,7 @@ def lib() -> C.CDLL:
                                     C.POINTER(dbl)]),
             "dmap_surface_points": (i32, [vp, vp, i32, i64, C.POINTER(_UvMap), vp, vp]),
             "dmap_surface_points_host": (i32, [vp, vp, i32, i64, C.POINTER(_UvMap), vp]),
+            "dmap_scene_set_opacity": (i32, [vp, vp, i32, i32, C.POINTER(_UvMap), vp]),
             "dmap_tessellate_uniform": (i32, [vp, i32, vp, vp, vp, vp, vp]),
             "dmap_tessellate_uniform_host": (i32, [vp, i32, vp, vp, vp, vp]),
             "dmap_tessellate_texel": (i32, [vp, i32, i64, vp, vp, vp, vp, C.POINTER(i64), vp]),
@@ -384,6 +386,27 @@ class Scene:
         self.ctx.check(lib().dmap_surface_points_host(self.h, h.ctypes.data, dt, len(h), C.byref(m),
                                                       out.ctypes.data), "dmap_surface_points_host")
         return out
+
+    def set_opacity(self, mask: Optional[np.ndarray] = None, uv_scale=(1.0, 1.0), uv_offset=(0.0, 0.0),
+                    flip_v: bool = False, tri_flags: Optional[np.ndarray] = None):
+        """dmap_scene_set_opacity: ks's opacity map as the scene's hit filter
+        (embree's filter functions in DisplacedGeometry's callbacks), a (h, w)
+        uint8 mask over the object's texture coordinates, 0 transparent;
+        tri_flags (n_tri,) marks the triangles it covers (None: all). mask
+        None removes it. Filtered scenes run precision "f64" or schedule
+        "simple"."""
+        if mask is None:
+            self.ctx.check(lib().dmap_scene_set_opacity(self.h, None, 0, 0, None, None), "dmap_scene_set_opacity")
+            return
+        m = np.ascontiguousarray(mask, np.uint8)
+        if m.ndim != 2:
+            raise ValueError("the opacity mask is (h, w)")
+        tf = None if tri_flags is None else np.ascontiguousarray(tri_flags, np.uint8)
+        if tf is not None and tf.shape != (self.n_tri,):
+            raise ValueError("tri_flags needs one byte per triangle")
+        uvm = _UvMap((C.c_double * 2)(*uv_scale), (C.c_double * 2)(*uv_offset), int(flip_v))
+        self.ctx.check(lib().dmap_scene_set_opacity(self.h, m.ctypes.data, m.shape[1], m.shape[0], C.byref(uvm),
+                                                    None if tf is None else tf.ctypes.data), "dmap_scene_set_opacity")
 
     def tessellate_uniform(self, n: int) -> dict:
         """dmap_tessellate_uniform_host (append_displaced_triangle over the

@@ -506,7 +506,53 @@ void dmap_scene_destroy(dmap_scene *s)
     cudaFree(s->cluster_tri_dev);
     cudaFree(s->cluster_box_dev);
     cudaFree(s->cluster_tree_dev);
+    cudaFree(s->op_mask_dev);
+    cudaFree(s->op_tri_dev);
     delete s;
+}
+
+dmap_status dmap_scene_set_opacity(dmap_scene *s, const uint8_t *mask_host, int w, int h, const dmap_uv_map *map,
+                                   const uint8_t *tri_flags_host)
+{
+    if (!s)
+        return DMAP_ERR_INVALID;
+    dmap_context *ctx = s->ctx;
+    if (mask_host && (w <= 0 || h <= 0 || (int64_t)w * h > (1ll << 30)))
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_set_opacity: the mask needs 1 <= w h <= 2^30 texels");
+    dmap_uv_map m = {{1.0, 1.0}, {0.0, 0.0}, 0};
+    if (map)
+        m = *map;
+    if (mask_host && !(m.uv_scale[0] != 0.0 && m.uv_scale[1] != 0.0 && std::isfinite(m.uv_scale[0]) &&
+                       std::isfinite(m.uv_scale[1]) && std::isfinite(m.uv_offset[0]) && std::isfinite(m.uv_offset[1])))
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_set_opacity: uv_scale must be finite and non-zero");
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    // queries in flight, on any stream, may read the old mask
+    DMAP_CUDA(ctx, cudaDeviceSynchronize());
+    cudaFree(s->op_mask_dev);
+    cudaFree(s->op_tri_dev);
+    s->op_mask_dev = s->op_tri_dev = nullptr;
+    s->op_w = s->op_h = 0;
+    if (!mask_host)
+        return DMAP_OK;
+    const size_t mb = (size_t)w * h, tb = tri_flags_host ? (size_t)s->n_tri : 0;
+    unsigned char *md = nullptr, *td = nullptr;
+    DMAP_CUDA(ctx, cudaMalloc(&md, mb));
+    if (tb && cudaMalloc(&td, tb) != cudaSuccess) {
+        cudaFree(md);
+        return fail(ctx, DMAP_ERR_OOM, "dmap_scene_set_opacity: cudaMalloc");
+    }
+    if (cudaMemcpy(md, mask_host, mb, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (tb && cudaMemcpy(td, tri_flags_host, tb, cudaMemcpyHostToDevice) != cudaSuccess)) {
+        cudaFree(md);
+        cudaFree(td);
+        return fail(ctx, DMAP_ERR_CUDA, "dmap_scene_set_opacity: copy");
+    }
+    s->op_mask_dev = md;
+    s->op_tri_dev = td;
+    s->op_w = w;
+    s->op_h = h;
+    s->op_map = m;
+    return DMAP_OK;
 }
 
 int dmap_scene_triangle_count(const dmap_scene *s) { return s ? s->n_tri : 0; }
@@ -567,6 +613,20 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.cluster_tri = s->cluster_tri_dev;
     q.cluster_box = s->cluster_box_dev;
     q.cluster_tree = s->cluster_tree_dev;
+    if (s->op_mask_dev) {
+        if (o.precision == DMAP_PRECISION_F32 && o.schedule == DMAP_SCHEDULE_WAVEFRONT)
+            return fail(ctx, DMAP_ERR_UNSUPPORTED,
+                        "dmap_intersect: a scene with an opacity filter runs DMAP_SCHEDULE_SIMPLE or FP64 precision");
+        q.op_mask = s->op_mask_dev;
+        q.op_tri = s->op_tri_dev;
+        q.op_w = s->op_w;
+        q.op_h = s->op_h;
+        q.op_flip = s->op_map.flip_v;
+        q.op_scale[0] = s->op_map.uv_scale[0];
+        q.op_scale[1] = s->op_map.uv_scale[1];
+        q.op_offset[0] = s->op_map.uv_offset[0];
+        q.op_offset[1] = s->op_map.uv_offset[1];
+    }
     return DMAP_OK;
 }
 

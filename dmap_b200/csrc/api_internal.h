@@ -69,6 +69,11 @@ struct dmap_scene
     float *cluster_tree_dev = nullptr;
     std::vector<TriDev> tris_host;
     bool all_f64 = true;
+    // the opacity filter (dmap_scene_set_opacity); op_mask_dev null: none
+    unsigned char *op_mask_dev = nullptr;
+    unsigned char *op_tri_dev = nullptr;
+    int op_w = 0, op_h = 0;
+    dmap_uv_map op_map = {{1.0, 1.0}, {0.0, 0.0}, 0};
 };
 
 namespace dmapi

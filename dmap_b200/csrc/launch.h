@@ -37,6 +37,13 @@ struct QueryOpts
     const int *cluster_tri = nullptr;
     const float *cluster_box = nullptr;
     const float *cluster_tree = nullptr;
+    // The scene's opacity filter (dmap_scene_set_opacity): op_h rows of op_w
+    // mask texels, 0 transparent; op_tri flags the triangles it covers
+    // (nullptr: every one); the object uv map of the crossings' coordinates.
+    const unsigned char *op_mask = nullptr;
+    const unsigned char *op_tri = nullptr;
+    int op_w = 0, op_h = 0, op_flip = 0;
+    double op_scale[2] = {1.0, 1.0}, op_offset[2] = {0.0, 0.0};
 };
 
 constexpr int kMaxRounds = 32;

@@ -461,6 +461,8 @@ dmap_status dmap_server_submit_rays(dmap_server *S, dmap_scene *scene, const flo
     if (!S || !scene || !id || n < 0 || (n > 0 && (!rays_host || !hits_host)) ||
         (mode != DMAP_MODE_CLOSEST && mode != DMAP_MODE_OCCLUDED) || scene->ctx != S->ctx)
         return DMAP_ERR_INVALID;
+    if (scene->op_mask_dev) // the server's wavefront launches do not run the filter
+        return DMAP_ERR_UNSUPPORTED;
     auto r = std::make_unique<Request>();
     r->kind = Kind::Rays;
     r->scene = scene;
@@ -490,6 +492,8 @@ dmap_status dmap_server_submit_render(dmap_server *S, dmap_scene *scene, const d
 {
     if (!S || !scene || !desc || !rgb_host || !id || scene->ctx != S->ctx)
         return DMAP_ERR_INVALID;
+    if (scene->op_mask_dev)
+        return DMAP_ERR_UNSUPPORTED;
     const dmap_camera &C = desc->camera;
     if (C.width <= 0 || C.height <= 0 || desc->spp <= 0 || desc->max_depth < 1)
         return DMAP_ERR_INVALID;

@@ -36,6 +36,7 @@
 // round like the reference); FP32 code uses explicit fmaf where it wants one.
 #include "f32_node.cuh"
 #include "order.cuh"
+#include "filter.cuh"
 
 namespace
 {
@@ -222,7 +223,7 @@ __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const Asse
                 t_max = lh.t;
                 found = true;
                 nah = lah = 0;
-                if (opt.mode == 1)
+                if (opt.mode == 1 && !opt.op_mask) // a filter judges the nearest crossing
                     return true;
             }
             cell_next(cur, si, sj, T.root_level);
@@ -292,9 +293,21 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
         const TriDev32 &T = tris32[t];
         if (sp)
             ++st[DMAP_ST_TRI];
-        double tm = t_max;
         d64::hit64 h;
-        if (triangle_walk32(T, tris64[t], assets[T.asset], o, d, t_min, tm, opt, h, sp, far_bound(t1), status)) {
+        bool got = false;
+        // the callbacks' filter passes (displaced_geometry.cpp:53-106); no filter: one walk
+        double t_lo = t_min;
+        for (int pass = 0; pass < (opt.op_mask ? dmapdev::kFilterPasses : 1); ++pass) {
+            double tm = t_max;
+            if (!triangle_walk32(T, tris64[t], assets[T.asset], o, d, t_lo, tm, opt, h, sp, far_bound(t1), status))
+                break;
+            if (dmapdev::crossing_opaque(opt, tris64[t], t, h.bary.x, h.bary.y)) {
+                got = true;
+                break;
+            }
+            t_lo = h.t;
+        }
+        if (got) {
             best = h;
             best_tri = t;
             t_max = h.t;

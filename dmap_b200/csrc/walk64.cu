@@ -11,6 +11,7 @@
 #include "f64_leaf.cuh"
 #include "f64_node.cuh"
 #include "order.cuh"
+#include "filter.cuh"
 #include "launch.h"
 
 namespace
@@ -93,8 +94,8 @@ __device__ bool triangle_intersect(const TriDev &T, const AssetDev &g, v3 o, v3 
                 t_max = lh.t;
                 found = true;
                 nah = lah = 0;
-                if (opt.mode == 1)
-                    return true; // occlusion: any hit answers the query
+                if (opt.mode == 1 && !opt.op_mask)
+                    return true; // occlusion: any hit answers the query (a filter judges the nearest)
             }
             cell_next(cur, si, sj, T.root_level);
         }
@@ -104,6 +105,25 @@ __device__ bool triangle_intersect(const TriDev &T, const AssetDev &g, v3 o, v3 
         st[DMAP_ST_LAH] += lah;
     }
     return found;
+}
+
+// The intersect / occluded callback's passes over DisplacedIntersector::intersect
+// (displaced_geometry.cpp:53-106): a crossing the scene's filter rejects
+// raises t_min to its t and the triangle is walked again. No filter: one walk.
+__device__ bool triangle_filtered(const TriDev &T, int tri, const AssetDev &g, v3 o, v3 d, double t_min,
+                                  double t_max, const dmapk::QueryOpts &opt, hit64 &hit, int64_t *st)
+{
+    if (!opt.op_mask)
+        return triangle_intersect(T, g, o, d, t_min, t_max, opt, hit, st);
+    double t_lo = t_min;
+    for (int pass = 0; pass < dmapdev::kFilterPasses; ++pass) {
+        if (!triangle_intersect(T, g, o, d, t_lo, t_max, opt, hit, st))
+            return false;
+        if (dmapdev::crossing_opaque(opt, T, tri, hit.bary.x, hit.bary.y))
+            return true;
+        t_lo = hit.t; // the walk accepts t > t_min only
+    }
+    return false;
 }
 
 template <typename R>
@@ -199,7 +219,7 @@ __global__ void __launch_bounds__(128) walk64_kernel(const TriDev *__restrict__ 
         if (sp)
             ++st[DMAP_ST_TRI];
         hit64 h;
-        if (triangle_intersect(T, assets[T.asset], o, d, t_min, t_max, opt, h, sp)) {
+        if (triangle_filtered(T, t, assets[T.asset], o, d, t_min, t_max, opt, h, sp)) {
             best = h;
             best_tri = t;
             t_max = h.t;

@@ -278,6 +278,30 @@ dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, d
                                      const dmap_uv_map *map, double *out_host);
 
 /*
+ * Hit filter: ks's opacity map behind embree's filter functions, as
+ * DisplacedGeometry's intersect and occluded callbacks run them
+ * (displaced_geometry.cpp:53-106). The crossing a triangle's walk returns
+ * goes to the filter; a crossing it rejects is skipped and the triangle is
+ * walked again from t_min = that crossing's t, at most 64 times
+ * (max_filter_passes, displaced_geometry.h:62); an occlusion query takes
+ * the nearest crossing of each triangle for the filter to judge. The
+ * filter: the crossing's texture coordinate (compute_hit_texcoord,
+ * displaced_geometry.cpp:189-193: the float barycentrics the filter sees,
+ * BaseTriangle::param, the object uv of `map` (NULL = identity), rounded to
+ * float) picks texel (floor(u w) mod w, floor(v h) mod h) of a w x h mask,
+ * row-major with rows along v; 0 is transparent and rejects the crossing.
+ * tri_flags_host (n_tri bytes, NULL = every triangle) marks the triangles
+ * the map covers (the object whose material carries it); the others accept
+ * every crossing. mask_host NULL removes the filter. The mask is copied.
+ * Queries on a filtered scene run the one-thread-per-ray schedules
+ * (DMAP_PRECISION_F64, or DMAP_PRECISION_F32 with DMAP_SCHEDULE_SIMPLE);
+ * the wavefront schedule, dmap_render and the server return
+ * DMAP_ERR_UNSUPPORTED for it.
+ */
+dmap_status dmap_scene_set_opacity(dmap_scene *scene, const uint8_t *mask_host, int w, int h, const dmap_uv_map *map,
+                                   const uint8_t *tri_flags_host);
+
+/*
  * Oracle meshes (displaced_tessellation.h:17-53): the displaced surface of
  * every scene triangle as a float mesh, for mesh-based cross-checks.
  * Positions S = P + h N, texture coordinates (s, t) and unit vertex normals

@@ -1332,6 +1332,10 @@ struct o_scene {
     int n_obj, cap;
     o_object *obj;
     int n_tri;
+    /* the opacity filter (o_scene_set_opacity); op_mask NULL: none */
+    uint8_t *op_mask, *op_tri;
+    int op_w, op_h, op_flip;
+    double op_scale[2], op_offset[2];
 };
 
 o_scene *o_scene_create(void) { return (o_scene *)calloc(1, sizeof(o_scene)); }
@@ -1348,7 +1352,31 @@ void o_scene_free(o_scene *s)
         free(s->obj[k].isects);
     }
     free(s->obj);
+    free(s->op_mask);
+    free(s->op_tri);
     free(s);
+}
+
+void o_scene_set_opacity(o_scene *s, const uint8_t *mask, int w, int h, const double *map5, const uint8_t *tri_flags)
+{
+    free(s->op_mask);
+    free(s->op_tri);
+    s->op_mask = s->op_tri = NULL;
+    if (!mask || w <= 0 || h <= 0)
+        return;
+    s->op_mask = (uint8_t *)malloc((size_t)w * h);
+    memcpy(s->op_mask, mask, (size_t)w * h);
+    if (tri_flags) {
+        s->op_tri = (uint8_t *)malloc((size_t)(s->n_tri > 0 ? s->n_tri : 1));
+        memcpy(s->op_tri, tri_flags, (size_t)s->n_tri);
+    }
+    s->op_w = w;
+    s->op_h = h;
+    s->op_scale[0] = map5 ? map5[0] : 1.0;
+    s->op_scale[1] = map5 ? map5[1] : 1.0;
+    s->op_offset[0] = map5 ? map5[2] : 0.0;
+    s->op_offset[1] = map5 ? map5[3] : 0.0;
+    s->op_flip = map5 ? map5[4] != 0.0 : 0;
 }
 
 int o_scene_add_object(o_scene *s, const double *values, int W, double scale, double offset, int repeat, int build,
@@ -1494,6 +1522,53 @@ static double entry_key(const o_box *B, v3 o, v3 d, const double *inv, double t_
     return key;
 }
 
+/* The opacity filter (not in the reference's sources: ks's opacity map
+ * behind embree's filter functions, reduced to a binary texel mask): the
+ * crossing's texture coordinate as compute_hit_texcoord forms it
+ * (displaced_geometry.cpp:189-193) from the float barycentrics of
+ * potential_hit (:21-34), BaseTriangle::param (displaced_surface.h:88) and
+ * DisplacedObject::object_uv (scene_spec.cpp:382-388) rounded to float,
+ * then the mask texel under it with repeat; 0 rejects. */
+static int crossing_opaque(const o_scene *s, const o_tri *T, int g, const o_hit *h)
+{
+    if (!s->op_mask || (s->op_tri && !s->op_tri[g]))
+        return 1;
+    double u = (double)(float)h->bary.x, v = (double)(float)h->bary.y;
+    double ps = (T->t0.x + u * (T->t1.x - T->t0.x)) + v * (T->t2.x - T->t0.x);
+    double pt = (T->t0.y + u * (T->t1.y - T->t0.y)) + v * (T->t2.y - T->t0.y);
+    double x = (ps - s->op_offset[0]) / s->op_scale[0], y = (pt - s->op_offset[1]) / s->op_scale[1];
+    if (s->op_flip)
+        y = 1.0 - y;
+    double fx = (double)(float)x * s->op_w, fy = (double)(float)y * s->op_h;
+    if (!(fabs(fx) < 1e15 && fabs(fy) < 1e15))
+        return 1;
+    long long i = (long long)floor(fx) % s->op_w, j = (long long)floor(fy) % s->op_h;
+    if (i < 0)
+        i += s->op_w;
+    if (j < 0)
+        j += s->op_h;
+    return s->op_mask[j * s->op_w + i] != 0;
+}
+
+/* The intersect / occluded callback's passes (displaced_geometry.cpp:53-106):
+ * a crossing the filter rejects raises t_min to its t and the triangle is
+ * walked again, at most max_filter_passes = 64 times (displaced_geometry.h:62). */
+static int isect_filtered(const o_scene *s, const o_isect *X, int g, v3 o, v3 d, double t_min, double t_max,
+                          int bound, int slab_max_level, int leaf, o_hit *h, int64_t *st, int64_t *level_stats)
+{
+    if (!s->op_mask)
+        return isect_intersect(X, o, d, t_min, t_max, bound, slab_max_level, leaf, h, st, level_stats);
+    double t_lo = t_min;
+    for (int pass = 0; pass < 64; ++pass) {
+        if (!isect_intersect(X, o, d, t_lo, t_max, bound, slab_max_level, leaf, h, st, level_stats))
+            return 0;
+        if (crossing_opaque(s, X->tri, g, h))
+            return 1;
+        t_lo = h->t; /* the walk accepts t > t_min only */
+    }
+    return 0;
+}
+
 /* The flat loop of ObjectIntersector::intersect_flat (:778-799) over every
  * object (order O_ORDER_INDEX); or (O_ORDER_NEAREST) the same loop over the
  * triangles whose boxes the ray meets, sorted by (key, index), each still
@@ -1530,7 +1605,8 @@ static int scene_intersect1(const o_scene *s, const double *ray, int bound, int 
             if (st)
                 ++st[O_ST_TRIANGLE_TESTS];
             o_hit h;
-            if (isect_intersect(X, o, d, t_min, t_max, bound, slab_max_level, leaf, &h, st, level_stats)) {
+            if (isect_filtered(s, X, cand[c].g, o, d, t_min, t_max, bound, slab_max_level, leaf, &h, st,
+                               level_stats)) {
                 write_hit(out, &h, cand[c].g, cand[c].ob);
                 t_max = h.t;
                 found = 1;
@@ -1547,8 +1623,8 @@ static int scene_intersect1(const o_scene *s, const double *ray, int bound, int 
             if (st)
                 ++st[O_ST_TRIANGLE_TESTS];
             o_hit h;
-            if (isect_intersect(&O->isects[k], o, d, t_min, t_max, bound, slab_max_level, leaf, &h, st,
-                                level_stats)) {
+            if (isect_filtered(s, &O->isects[k], O->first_tri + k, o, d, t_min, t_max, bound, slab_max_level, leaf,
+                               &h, st, level_stats)) {
                 write_hit(out, &h, O->first_tri + k, ob);
                 t_max = h.t;
                 found = 1;

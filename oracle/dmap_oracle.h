@@ -93,6 +93,12 @@ void o_scene_triangle_frame(const o_scene *s, int tri, double *out12);
 int64_t o_scene_intersect(const o_scene *s, const double *rays, int64_t n, int bound, int slab_max_level, int leaf,
                           double *hits, int64_t *stats, int64_t *level_stats, int threads, int order);
 
+/* The opacity filter of dmap_scene_set_opacity for o_scene_intersect: an h x w
+ * mask (0 transparent) over the crossings' texture coordinates; map5 = uv_scale
+ * u, v, uv_offset u, v, flip_v (NULL identity); tri_flags n_tri bytes (NULL
+ * every triangle). mask NULL removes it. Both buffers are copied. */
+void o_scene_set_opacity(o_scene *s, const uint8_t *mask, int w, int h, const double *map5, const uint8_t *tri_flags);
+
 /* Single-triangle entry points for validation. */
 int o_triangle_intersect(const o_scene *s, int tri, const double *ray8, int bound, int slab_max_level, int leaf,
                          double *hit, int64_t *stats);

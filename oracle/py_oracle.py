@@ -65,6 +65,8 @@ class _Lib:
         self._sc_add = f("scene_add_object", C.c_int, C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_int,
                          C.c_int, _dp, C.c_int)
         self._sc_ntri = f("scene_triangle_count", C.c_int, C.c_void_p)
+        _u8 = C.POINTER(C.c_uint8)
+        self._sc_opacity = f("scene_set_opacity", None, C.c_void_p, _u8, C.c_int, C.c_int, _dp, _u8)
         self._sc_info = f("scene_triangle_info", None, C.c_void_p, C.c_int, _dp)
         self._sc_frame = f("scene_triangle_frame", None, C.c_void_p, C.c_int, _dp)
         self._tri_isect = f("triangle_intersect", C.c_int, C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, C.c_int,
@@ -174,6 +176,20 @@ class CpuScene:
             self.lib._sc_isect(self.h, _ptr(r), n, BOUND[bound], slab_max_level, LEAF[leaf], _ptr(hits),
                                _ptr(st, _lp), threads)
         return hits, st
+
+    def set_opacity(self, mask=None, uv_scale=(1.0, 1.0), uv_offset=(0.0, 0.0), flip_v=False, tri_flags=None):
+        """The opacity filter of dmap_scene_set_opacity: mask (h, w) uint8,
+        0 transparent; tri_flags (n_tri,) marks the triangles it covers
+        (None: all). mask None removes it."""
+        u8 = C.POINTER(C.c_uint8)
+        if mask is None:
+            self.lib._sc_opacity(self.h, None, 0, 0, None, None)
+            return
+        m = np.ascontiguousarray(mask, np.uint8)
+        mp = np.array([uv_scale[0], uv_scale[1], uv_offset[0], uv_offset[1], 1.0 if flip_v else 0.0])
+        tf = None if tri_flags is None else np.ascontiguousarray(tri_flags, np.uint8)
+        self.lib._sc_opacity(self.h, m.ctypes.data_as(u8), m.shape[1], m.shape[0], _ptr(mp),
+                             None if tf is None else tf.ctypes.data_as(u8))
 
     def triangle_info(self, tri):
         out = np.empty(11)

@@ -41,6 +41,10 @@ struct r_scene
 {
     std::vector<std::unique_ptr<RefObject>> objects;
     int n_tri = 0;
+    // the opacity filter (r_scene_set_opacity); empty mask: none
+    std::vector<uint8_t> op_mask, op_tri;
+    int op_w = 0, op_h = 0, op_flip = 0;
+    double op_scale[2] = {1.0, 1.0}, op_offset[2] = {0.0, 0.0};
 };
 
 struct r_pyramid
@@ -208,6 +212,63 @@ int64_t r_scene_intersect(const r_scene *s, const double *rays, int64_t n, int b
     return n_hit.load();
 }
 
+// The opacity filter standing in for rtcFilterIntersection: the crossing's
+// texture coordinate as DisplacedGeometry::compute_hit_texcoord forms it
+// (displaced_geometry.cpp:189-193, from potential_hit's float barycentrics,
+// :21-34) with the reference's BaseTriangle::param, the object uv
+// (scene_spec.cpp:382-388) rounded to float, and the mask texel under it.
+static bool crossing_opaque(const r_scene *s, const BaseTriangle &tri, int g, const dmap::DisplacedHit &h)
+{
+    if (s->op_mask.empty() || (!s->op_tri.empty() && !s->op_tri[g]))
+        return true;
+    float fu = (float)h.bary[0], fv = (float)h.bary[1];
+    vec2d st = tri.param(fu, fv);
+    double x = (st[0] - s->op_offset[0]) / s->op_scale[0], y = (st[1] - s->op_offset[1]) / s->op_scale[1];
+    if (s->op_flip)
+        y = 1.0 - y;
+    double fx = (double)(float)x * s->op_w, fy = (double)(float)y * s->op_h;
+    if (!(std::fabs(fx) < 1e15 && std::fabs(fy) < 1e15))
+        return true;
+    long long i = (long long)std::floor(fx) % s->op_w, j = (long long)std::floor(fy) % s->op_h;
+    if (i < 0)
+        i += s->op_w;
+    if (j < 0)
+        j += s->op_h;
+    return s->op_mask[(size_t)(j * s->op_w + i)] != 0;
+}
+
+// A filtered scene: intersect_flat's loop (displaced_intersector.cpp:578-599)
+// with each triangle behind intersect_callback's passes
+// (displaced_geometry.cpp:53-78, max_filter_passes = 64 at displaced_geometry.h:62).
+static bool intersect_filtered(const r_scene *s, const RefObject &ob, const vec3d &o, const vec3d &d, double t_min,
+                               double &t_max, const dmap::TraversalOptions &opt, dmap::DisplacedHit &hit, int &tri,
+                               dmap::TraversalStats *st)
+{
+    bool found = false;
+    for (size_t k = 0; k < ob.obj->triangles.size(); ++k) {
+        double t0 = t_min, t1 = t_max;
+        if (!ob.obj->boxes[k].clip(o, d, t0, t1))
+            continue;
+        if (st)
+            ++st->triangle_tests;
+        double t_lo = t_min;
+        for (int pass = 0; pass < 64; ++pass) {
+            dmap::DisplacedHit h;
+            if (!ob.obj->triangles[k].intersect(o, d, t_lo, t_max, opt, h, st))
+                break;
+            if (crossing_opaque(s, ob.tris[k], ob.first_tri + (int)k, h)) {
+                hit = h;
+                tri = (int)k;
+                t_max = h.t;
+                found = true;
+                break;
+            }
+            t_lo = h.t;
+        }
+    }
+    return found;
+}
+
 static int64_t intersect_range(const r_scene *s, const double *rays, int64_t b, int64_t e,
                                const dmap::TraversalOptions &opt, double *hits, int64_t *stats)
 {
@@ -224,6 +285,13 @@ static int64_t intersect_range(const r_scene *s, const double *rays, int64_t b, 
             const RefObject &ob = *s->objects[k];
             dmap::DisplacedHit h;
             int tri = -1;
+            if (!s->op_mask.empty()) {
+                if (intersect_filtered(s, ob, o, d, t_min, t_max, opt, h, tri, stats ? &st : nullptr)) {
+                    write_hit(out, h, ob.first_tri + tri, (int)k);
+                    found = true;
+                }
+                continue;
+            }
             if (ob.obj->intersect(o, d, t_min, t_max, opt, h, tri, stats ? &st : nullptr)) {
                 write_hit(out, h, ob.first_tri + tri, (int)k);
                 t_max = h.t;
@@ -235,6 +303,24 @@ static int64_t intersect_range(const r_scene *s, const double *rays, int64_t b, 
             fill_stats(stats + O_ST_COUNT * r, st);
     }
     return n_hit;
+}
+
+void r_scene_set_opacity(r_scene *s, const uint8_t *mask, int w, int h, const double *map5, const uint8_t *tri_flags)
+{
+    s->op_mask.clear();
+    s->op_tri.clear();
+    if (!mask || w <= 0 || h <= 0)
+        return;
+    s->op_mask.assign(mask, mask + (size_t)w * h);
+    if (tri_flags)
+        s->op_tri.assign(tri_flags, tri_flags + s->n_tri);
+    s->op_w = w;
+    s->op_h = h;
+    s->op_scale[0] = map5 ? map5[0] : 1.0;
+    s->op_scale[1] = map5 ? map5[1] : 1.0;
+    s->op_offset[0] = map5 ? map5[2] : 0.0;
+    s->op_offset[1] = map5 ? map5[3] : 0.0;
+    s->op_flip = map5 ? map5[4] != 0.0 : 0;
 }
 
 int r_triangle_intersect(const r_scene *s, int tri, const double *q, int bound, int slab_max_level, int leaf,
