@@ -64,6 +64,7 @@ using dmapdev::TriDev32;
 #define DMAP_BOX_FIRST_TOPM 1
 #endif
 
+constexpr int kGroupList = 24; // groups a ray's nearest-order list holds
 constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the object-box candidate mask
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -407,6 +408,11 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     int tri = 0, best_tri = -1, root = 0, si = 0, sj = 0, nah = 0, lah = 0, flags = 0, guard = 0;
     double ckey = -INFINITY;
     int cidx = -1;
+    // nearest order over groups (TOPM >= 1): the ray's sorted group list;
+    // n_gl -1: not built for this ray, kGroupList + 1: more groups than fit
+    int gl_b[kGroupList];
+    float gl_e[kGroupList];
+    int n_gl = -1;
     Ray32 r;
     Cell32 cur = {0, 0, 0}, end = {0, 0, 0};
     unsigned mask[kMaskWords];
@@ -474,6 +480,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 } else {
                     ray = round == 0 ? (int)item : q_in[item];
                     load_ray(rays, ray, o, d, t_min, t_max);
+                    n_gl = -1;
 #pragma unroll
                     for (int a = 0; a < 3; ++a) {
                         of[a] = (float)o[a];
@@ -630,55 +637,68 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                         return ok;
                     };
                     // the groups the ray reaches, sorted by entry bound (up to
-                    // kGroupList of them); then scanned nearest first until
-                    // a group's bound passes the best key. Past kGroupList
-                    // candidates: the nearest group first, then every group
-                    // whose bound is not beyond the best key.
-                    constexpr int kGroupList = 24;
-                    int gl_b[kGroupList];
-                    float gl_e[kGroupList];
-                    int n_gl = 0;
-                    bool overflow = false;
-                    int b0 = -1;
-                    float e0 = INFINITY;
-                    blocks([&](int b) {
-                        float e;
-                        if (!entry(b, e))
-                            return;
-                        if (b0 < 0 || e < e0) {
-                            b0 = b;
-                            e0 = e;
-                        }
-                        if (n_gl == kGroupList) {
-                            overflow = true;
-                            return;
-                        }
-                        int k = n_gl++;
-                        for (; k > 0 && gl_e[k - 1] > e; --k) {
-                            gl_e[k] = gl_e[k - 1];
-                            gl_b[k] = gl_b[k - 1];
-                        }
-                        gl_e[k] = e;
-                        gl_b[k] = b;
-                    });
+                    // kGroupList of them), built at the ray's first pick in
+                    // this launch and kept for its later picks: t_max only
+                    // shrinks, so no other group becomes reachable, and each
+                    // pick re-tests a listed group's box before it scans it.
+                    // Groups are scanned nearest first until a group's bound
+                    // passes the best key (the bound is a lower bound of its
+                    // triangles' keys). Past kGroupList groups: the nearest
+                    // group first, then every group whose bound is not beyond
+                    // the best key, enumerated at every pick.
+                    if (n_gl < 0) {
+                        n_gl = 0;
+                        blocks([&](int b) {
+                            float e;
+                            if (n_gl > kGroupList || !entry(b, e))
+                                return;
+                            if (n_gl == kGroupList) {
+                                n_gl = kGroupList + 1;
+                                return;
+                            }
+                            int k = n_gl++;
+                            for (; k > 0; --k) { // insertion: slots below n_gl are set
+                                const float prev = gl_e[k - 1];
+                                if (!(prev > e))
+                                    break;
+                                gl_e[k] = prev;
+                                gl_b[k] = gl_b[k - 1];
+                            }
+                            gl_e[k] = e;
+                            gl_b[k] = b;
+                        });
+                    }
                     auto scan = [&](int b) {
                         for (int q = 32 * b, stop = min(n_tri, 32 * b + 32); q < stop; ++q)
                             consider(clustered ? opt.cluster_tri[q] : q);
                     };
-                    if (!overflow) {
+                    if (n_gl <= kGroupList) {
                         for (int k = 0; k < n_gl; ++k) {
                             if (bt >= 0 && (double)gl_e[k] > bk)
                                 break;
-                            scan(gl_b[k]);
+                            float e;
+                            if (entry(gl_b[k], e)) // still reached with the current t_max
+                                scan(gl_b[k]);
                         }
-                    } else if (b0 >= 0) {
-                        scan(b0);
+                    } else {
+                        int b0 = -1;
+                        float e0 = INFINITY;
                         blocks([&](int b) {
                             float e;
-                            if (b == b0 || !entry(b, e) || (bt >= 0 && (double)e > bk))
-                                return;
-                            scan(b);
+                            if (entry(b, e) && (b0 < 0 || e < e0)) {
+                                b0 = b;
+                                e0 = e;
+                            }
                         });
+                        if (b0 >= 0) {
+                            scan(b0);
+                            blocks([&](int b) {
+                                float e;
+                                if (b == b0 || !entry(b, e) || (bt >= 0 && (double)e > bk))
+                                    return;
+                                scan(b);
+                            });
+                        }
                     }
                 } else if (use_mask) {
 #pragma unroll 1
