@@ -580,24 +580,30 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 double bk = 0.0;
                 int bt = -1;
                 const float tmf = __double2float_ru(t_max);
-                auto consider = [&](int t) {
+                // takes t when it is the best so far; true when t is still a
+                // candidate past the cursor (box-first order: its box passes)
+                auto consider = [&](int t) -> bool {
                     float tt = tmf;
                     if (kBoxFirst) {
                         // the float box first: its entry e is a lower bound of
                         // the key, so past the best key the FP64 key is not needed
                         float e = tmin_f;
-                        if (!box_range(tris32[t].box_lo, tris32[t].box_hi, of, df, invf, e, tt) ||
-                            (bt >= 0 && (double)e > bk))
-                            return;
+                        if (!box_range(tris32[t].box_lo, tris32[t].box_hi, of, df, invf, e, tt))
+                            return false;
+                        if (bt >= 0 && (double)e > bk)
+                            return true; // key > best key > cursor
                     }
                     const double key = d64::entry_key(tris64[t], o, d, inv, t_min);
-                    if (!d64::after_cursor(key, t, ckey, cidx) || !d64::before_best(key, t, bk, bt))
-                        return;
+                    if (!d64::after_cursor(key, t, ckey, cidx))
+                        return false;
+                    if (!d64::before_best(key, t, bk, bt))
+                        return true;
                     if (!kBoxFirst && !object_box(tris32[t], of, df, invf, tmin_f, tt))
-                        return;
+                        return false;
                     bk = key;
                     bt = t;
                     t1 = tt;
+                    return true;
                 };
                 if (TOPM >= 1) {
                     // blocks: first the candidate block with the nearest
@@ -668,17 +674,26 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                             gl_b[k] = b;
                         });
                     }
+                    // true when a triangle of group b is still a candidate
                     auto scan = [&](int b) {
+                        bool left = false;
                         for (int q = 32 * b, stop = min(n_tri, 32 * b + 32); q < stop; ++q)
-                            consider(clustered ? opt.cluster_tri[q] : q);
+                            if (consider(clustered ? opt.cluster_tri[q] : q))
+                                left = true;
+                        return left;
                     };
                     if (n_gl <= kGroupList) {
                         for (int k = 0; k < n_gl; ++k) {
+                            if (gl_b[k] < 0) // spent
+                                continue;
                             if (bt >= 0 && (double)gl_e[k] > bk)
                                 break;
+                            // a group no longer reached with the current t_max,
+                            // or without a candidate past the cursor, stays so:
+                            // t_max only shrinks and the cursor only advances
                             float e;
-                            if (entry(gl_b[k], e)) // still reached with the current t_max
-                                scan(gl_b[k]);
+                            if (!entry(gl_b[k], e) || !scan(gl_b[k]))
+                                gl_b[k] = -1;
                         }
                     } else {
                         int b0 = -1;
