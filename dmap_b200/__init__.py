@@ -34,7 +34,7 @@ _PKG = Path(__file__).resolve().parent
 # DMAP_B200_LIB names another build of the library (tuning variants)
 LIB_PATH = Path(os.environ.get("DMAP_B200_LIB") or _PKG / "libdmap_b200.so")
 
-F32, F16, F64 = 0, 1, 2
+F32, F16, F64, BF16 = 0, 1, 2, 3
 BOUND = {"box": 0, "slab": 1, "both": 2}
 LEAF = {"newton": 0, "two_triangle": 1}
 PRECISION = {"f64": 0, "f32": 1}
@@ -243,13 +243,34 @@ _DT = {np.dtype(np.float32): F32, np.dtype(np.float16): F16, np.dtype(np.float64
 CHANNELS = ("h0", "gu", "gv", "r", "ru", "rv", "h_min", "h_max")
 
 
+def to_bf16(values: np.ndarray) -> np.ndarray:
+    """Rounds values to bfloat16 (to nearest, ties to even) and returns the
+    16-bit patterns (uint16), the texel layout of a DMAP_BF16 asset."""
+    f = np.ascontiguousarray(values, np.float32)
+    if not np.isfinite(f).all():
+        raise ValueError("bfloat16 texels must be finite")
+    u = f.view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def from_bf16(bits: np.ndarray) -> np.ndarray:
+    """The values of bfloat16 patterns, exactly, as float64."""
+    return (np.ascontiguousarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+
+
 class Asset:
-    """HeightGrid + TaylorPyramid of one node grid on the device."""
+    """HeightGrid + TaylorPyramid of one node grid on the device. texel
+    "bf16" stores the grid as bfloat16 (the values rounded by to_bf16);
+    otherwise the array's own float32 / float16 / float64 type is kept."""
 
     def __init__(self, ctx: Context, nodes: np.ndarray, scale: float = 1.0, offset: float = 0.0,
-                 repeat: bool = False, keep_f64: bool = False, build: str = "fold"):
+                 repeat: bool = False, keep_f64: bool = False, build: str = "fold", texel: Optional[str] = None):
+        if texel not in (None, "bf16"):
+            raise ValueError("texel is None or 'bf16'")
         v = np.ascontiguousarray(nodes)
-        if v.dtype not in _DT:
+        if texel == "bf16":
+            v = to_bf16(v)
+        elif v.dtype not in _DT:
             v = v.astype(np.float64)
         if v.ndim != 2 or v.shape[0] != v.shape[1]:
             raise ValueError("the node grid must be square")
@@ -258,8 +279,9 @@ class Asset:
         self.ctx = ctx
         h = C.c_void_p()
         flags = (KEEP_F64 if keep_f64 else 0) | (BUILD_DIRECT if build == "direct" else 0)
-        ctx.check(lib().dmap_asset_create(ctx.h, v.ctypes.data, _DT[v.dtype], v.shape[0], scale, offset, int(repeat),
-                                          flags, C.byref(h)), "dmap_asset_create")
+        dt = BF16 if texel == "bf16" else _DT[v.dtype]
+        ctx.check(lib().dmap_asset_create(ctx.h, v.ctypes.data, dt, v.shape[0], scale, offset, int(repeat), flags,
+                                          C.byref(h)), "dmap_asset_create")
         self.h = h
         self.nodes = v.shape[0]
         self.n_leaf = v.shape[0] - 1
@@ -342,9 +364,10 @@ class Scene:
         return self
 
     @classmethod
-    def from_synthetic(cls, ctx: Context, scene, keep_f64: bool = False, build: str = "fold"):
-        """A dmap_b200.scenes.Scene on the device."""
-        assets = [Asset(ctx, a.nodes, a.scale, a.offset, a.repeat, keep_f64, build) for a in scene.assets]
+    def from_synthetic(cls, ctx: Context, scene, keep_f64: bool = False, build: str = "fold",
+                       texel: Optional[str] = None):
+        """A dmap_b200.scenes.Scene on the device (texel as Asset's)."""
+        assets = [Asset(ctx, a.nodes, a.scale, a.offset, a.repeat, keep_f64, build, texel) for a in scene.assets]
         return cls(ctx, assets, scene.tris, scene.tri_asset)
 
     def triangle_info(self, tri: int) -> np.ndarray:

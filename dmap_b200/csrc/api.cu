@@ -100,8 +100,8 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
     int n = nodes - 1;
     if (nodes < 2 || (n & (n - 1)) != 0 || n > (1 << 16))
         return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: the node grid must be (2^L + 1)^2 with 2^L <= 65536");
-    if (dtype != DMAP_F32 && dtype != DMAP_F16 && dtype != DMAP_F64)
-        return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: dtype must be F32, F16 or F64");
+    if (dtype != DMAP_F32 && dtype != DMAP_F16 && dtype != DMAP_BF16 && dtype != DMAP_F64)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: dtype must be F32, F16, BF16 or F64");
     if (!std::isfinite(scale) || !std::isfinite(offset))
         return fail(ctx, DMAP_ERR_INVALID, "dmap_asset_create: scale and offset must be finite");
     DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -111,7 +111,7 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
     size_t per16 = 16 / es;
     int pitch = (int)(((size_t)nodes + per16 - 1) / per16 * per16);
     AssetDev &d = a->dev;
-    d.dtype = dtype == DMAP_F32 ? 0 : dtype == DMAP_F16 ? 1 : 2;
+    d.dtype = dtype == DMAP_F32 ? 0 : dtype == DMAP_F16 ? 1 : dtype == DMAP_BF16 ? 3 : 2;
     d.W = nodes;
     d.pitch = pitch;
     d.n_leaf = n;
@@ -158,9 +158,10 @@ dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_d
     cuuint64_t strides[1] = {(cuuint64_t)pitch * es};
     cuuint32_t box[2] = {box_w, (cuuint32_t)(T + 1)};
     cuuint32_t estr[2] = {1, 1};
-    CUtensorMapDataType tdt = dtype == DMAP_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                              : dtype == DMAP_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUtensorMapDataType tdt = dtype == DMAP_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                              : dtype == DMAP_F16  ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                              : dtype == DMAP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     CUresult cr = enc(&tmap, tdt, 2, a->nodes, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

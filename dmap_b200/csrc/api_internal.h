@@ -101,7 +101,7 @@ inline dmap_status cuda_fail(dmap_context *ctx, cudaError_t e, const char *what)
             return cuda_fail(ctx, e_, #call);                                                                         \
     } while (0)
 
-inline size_t dtype_size(dmap_dtype t) { return t == DMAP_F64 ? 8 : t == DMAP_F16 ? 2 : 4; }
+inline size_t dtype_size(dmap_dtype t) { return t == DMAP_F64 ? 8 : (t == DMAP_F16 || t == DMAP_BF16) ? 2 : 4; }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,

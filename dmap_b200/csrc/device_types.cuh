@@ -21,7 +21,7 @@ constexpr int kMaxLevels = 24;
 struct AssetDev
 {
     const void *nodes;   // node grid
-    int dtype;           // 0 f32, 1 f16, 2 f64
+    int dtype;           // 0 f32, 1 f16, 2 f64, 3 bf16
     int W;               // nodes per side (2^L + 1)
     int pitch;           // elements per row
     int n_leaf;          // 2^L

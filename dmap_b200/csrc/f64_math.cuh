@@ -9,6 +9,7 @@
 // the same order; std::min(a, b) = b < a ? b : a; std::max(a, b) = a < b ? b : a.
 #pragma once
 #include "device_types.cuh"
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 namespace d64
@@ -187,6 +188,8 @@ __device__ __forceinline__ double grid_value(const AssetDev &a, int j, int i)
         return (double)__ldg(static_cast<const float *>(a.nodes) + k);
     if (a.dtype == 1)
         return (double)__half2float(static_cast<const __half *>(a.nodes)[k]);
+    if (a.dtype == 3)
+        return (double)__bfloat162float(static_cast<const __nv_bfloat16 *>(a.nodes)[k]);
     return __ldg(static_cast<const double *>(a.nodes) + k);
 }
 

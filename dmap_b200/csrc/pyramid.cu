@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 namespace
@@ -175,6 +176,8 @@ __device__ __forceinline__ double to_d<float>(float x) { return (double)x; }
 template <>
 __device__ __forceinline__ double to_d<__half>(__half x) { return (double)__half2float(x); }
 template <>
+__device__ __forceinline__ double to_d<__nv_bfloat16>(__nv_bfloat16 x) { return (double)__bfloat162float(x); }
+template <>
 __device__ __forceinline__ double to_d<double>(double x) { return x; }
 
 __device__ __forceinline__ bool mbar_wait(unsigned bar_addr, unsigned phase)
@@ -286,6 +289,7 @@ __device__ __forceinline__ double direct_value(const AssetDev &a, int j, int i) 
     size_t k = (size_t)j * a.pitch + i;
     double v = a.dtype == 0   ? (double)static_cast<const float *>(a.nodes)[k]
                : a.dtype == 1 ? (double)__half2float(static_cast<const __half *>(a.nodes)[k])
+               : a.dtype == 3 ? (double)__bfloat162float(static_cast<const __nv_bfloat16 *>(a.nodes)[k])
                               : static_cast<const double *>(a.nodes)[k];
     return v * a.scale;
 }
@@ -508,6 +512,8 @@ cudaError_t launch_pyramid(const void *tmap, const dmapdev::AssetDev &a, int til
         e = launch_leaf<float>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
     else if (a.dtype == 1)
         e = launch_leaf<__half>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
+    else if (a.dtype == 3)
+        e = launch_leaf<__nv_bfloat16>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
     else
         e = launch_leaf<double>(tmap, a, tile, pyr64, pyr32, status, all64, stream);
     if (e != cudaSuccess)
@@ -638,9 +644,9 @@ extern "C" dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dt
         return DMAP_ERR_INVALID;
     if (n > kNoallocMaxLeaf)
         return DMAP_ERR_INVALID; // beyond the fixed scratch: use dmap_asset_create
-    if (dtype != DMAP_F32 && dtype != DMAP_F16 && dtype != DMAP_F64)
+    if (dtype != DMAP_F32 && dtype != DMAP_F16 && dtype != DMAP_BF16 && dtype != DMAP_F64)
         return DMAP_ERR_INVALID;
-    size_t es = dtype == DMAP_F64 ? 8 : dtype == DMAP_F16 ? 2 : 4;
+    size_t es = dtype == DMAP_F64 ? 8 : (dtype == DMAP_F16 || dtype == DMAP_BF16) ? 2 : 4;
     if (pitch < nodes || ((size_t)pitch * es) % 16 != 0 || ((uintptr_t)nodes_dev & 15) != 0 ||
         ((uintptr_t)pyr32_dev & 15) != 0 || !std::isfinite(scale) || !std::isfinite(offset))
         return DMAP_ERR_INVALID;
@@ -655,7 +661,7 @@ extern "C" dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dt
 
     AssetDev a{};
     a.nodes = nodes_dev;
-    a.dtype = dtype == DMAP_F32 ? 0 : dtype == DMAP_F16 ? 1 : 2;
+    a.dtype = dtype == DMAP_F32 ? 0 : dtype == DMAP_F16 ? 1 : dtype == DMAP_BF16 ? 3 : 2;
     a.W = nodes;
     a.pitch = pitch;
     a.n_leaf = n;
@@ -688,9 +694,10 @@ extern "C" dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dt
     cuuint64_t strides[1] = {(cuuint64_t)pitch * es};
     cuuint32_t box[2] = {box_w, (cuuint32_t)(T + 1)};
     cuuint32_t estr[2] = {1, 1};
-    CUtensorMapDataType tdt = dtype == DMAP_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                              : dtype == DMAP_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUtensorMapDataType tdt = dtype == DMAP_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                              : dtype == DMAP_F16  ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                              : dtype == DMAP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     if (reinterpret_cast<NoallocEncodeFn>(fn)(&tmap, tdt, 2, const_cast<void *>(nodes_dev), dims, strides, box, estr,
                                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

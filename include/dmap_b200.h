@@ -35,7 +35,8 @@ typedef enum dmap_status {
     DMAP_ERR_CANCELLED = 9    /* a served request was cancelled */
 } dmap_status;
 
-typedef enum dmap_dtype { DMAP_F32 = 0, DMAP_F16 = 1, DMAP_F64 = 2 } dmap_dtype;
+/* Ray and hit records are F32 or F64; height texels may also be F16 or BF16. */
+typedef enum dmap_dtype { DMAP_F32 = 0, DMAP_F16 = 1, DMAP_F64 = 2, DMAP_BF16 = 3 } dmap_dtype;
 
 typedef struct dmap_context dmap_context;
 typedef struct dmap_asset dmap_asset;
@@ -68,7 +69,7 @@ int64_t dmap_kernel_launches(const dmap_context *ctx);
  * coordinates wrapping when `repeat`, clamping otherwise.
  * Replaces DisplacementAsset's grid + TaylorPyramid(const HeightGrid &, PyramidBuild::Fold)
  * (displacement_asset.cpp:16-35, taylor_pyramid.h:89-92, taylor_pyramid.cpp:324-366).
- * `values_host` is host memory of `dtype` (F32, F16 or F64).
+ * `values_host` is host memory of `dtype` (F32, F16, BF16 or F64).
  */
 dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_dtype dtype, int nodes, double scale,
                               double offset, int repeat, unsigned flags, dmap_asset **out);

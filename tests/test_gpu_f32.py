@@ -89,6 +89,19 @@ def test_f32_f16_texels_and_offset(ctx, oracle):
     _check(cpu, dev, rays)
 
 
+def test_f32_bf16_texels(ctx, oracle):
+    """BF16 texels: the device stores bfloat16, the oracle sees the same
+    values widened to double; every hit record equals the oracle's."""
+    sc = helpers.small_sphere(64, patches=(0, 1, 2, 17))
+    for a in sc.assets:
+        a.nodes = dm.from_bf16(dm.to_bf16(a.nodes))
+        a.scale, a.offset = 0.9, 0.01
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc, texel="bf16")
+    rays = np.concatenate([helpers.near_surface_rays(cpu, 2000), helpers.aimed_rays(cpu, 2000)[0]])
+    n, _ = _check(cpu, dev, rays)
+    assert n > 1000
+
+
 def test_f32_never_miss(ctx, oracle):
     sc = helpers.small_sphere(32)
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)

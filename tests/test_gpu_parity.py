@@ -52,6 +52,21 @@ def test_device_pyramid_equals_oracle(ctx, oracle, dtype, scale, offset, repeat)
             assert np.array_equal(got[ch], lv[ch]), (k, ch)
 
 
+@pytest.mark.parametrize("build", ["fold", "direct"])
+def test_device_pyramid_bf16_equals_oracle(ctx, oracle, build):
+    """BF16 texels: the device pyramid of the bfloat16 grid equals the
+    oracle's pyramid of the same values widened to double."""
+    rng = np.random.default_rng(5)
+    v = rng.random((129, 129)) * 2.0 - 1.0
+    a = dm.Asset(ctx, v, 0.3, 0.1, True, keep_f64=True, build=build, texel="bf16")
+    ref = oracle.pyramid(dm.from_bf16(dm.to_bf16(v)), 0.3, 0.1, build)
+    assert a.n_levels == len(ref)
+    for k, lv in enumerate(ref):
+        got = a.level(k, "f64")
+        for ch in CHANNELS:
+            assert np.array_equal(got[ch], lv[ch]), (k, ch)
+
+
 def _compare(cpu, dev, rays, bound="both", k=1, leaf="newton", order="nearest"):
     ho, so = cpu.intersect(rays, bound, k, leaf, stats=True, order=order)
     hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, leaf, precision="f64", order=order), np.float64,
