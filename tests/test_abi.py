@@ -31,3 +31,21 @@ def test_null_context_is_rejected_without_a_device():
     import numpy as np
     v = np.zeros((3, 3), np.float32)
     assert lib.dmap_asset_create(None, v.ctypes.data, 0, 3, 1.0, 0.0, 0, 0, ctypes.byref(h)) != 0
+
+
+def test_bf16_texel_rounding():
+    """to_bf16 rounds to nearest with ties to even, as torch's conversion
+    does, and from_bf16 gives the patterns' values exactly."""
+    import numpy as np
+    import torch
+    import dmap_b200 as dm
+    rng = np.random.default_rng(9)
+    x = np.concatenate([(rng.random(20000) * 2 - 1) * 10.0 ** rng.integers(-6, 6, 20000),
+                        np.float32(1.0) + np.arange(-64, 65, dtype=np.float32) * np.float32(2.0 ** -8),
+                        [0.0, -0.0, 1e-40, -1e-40, 3.0e38]]).astype(np.float32)
+    bits = dm.to_bf16(x)
+    ref = torch.from_numpy(x).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    assert np.array_equal(bits, ref)
+    v = dm.from_bf16(bits)
+    assert np.array_equal(v, torch.from_numpy(x).to(torch.bfloat16).to(torch.float64).numpy())
+    assert np.array_equal(dm.to_bf16(v), bits)
