@@ -105,3 +105,17 @@ def test_filtered_nearest_order_same_hits(oracle, name):
     assert np.array_equal(hi[hit, 10], hn[hit, 10])
     tol = np.array([so.triangle_info(t)[2] for t in range(so.n_tri)])
     assert (np.abs(hi[hit, 0] - hn[hit, 0]) <= 4 * tol[hi[hit, 10].astype(int)]).all()
+
+
+@pytest.mark.parametrize("lib", ["oracle", "reference"])
+def test_filter_limits(request, lib):
+    """A mask that is transparent everywhere leaves no hit; one that covers
+    no triangle leaves the unfiltered query."""
+    cpu_lib = request.getfixturevalue(lib)
+    sc, cpu, rays = scene_and_rays("charts", cpu_lib)
+    h0, _ = cpu.intersect(rays, order="index")
+    assert (h0[:, 10] >= 0).sum() > 100
+    cpu.set_opacity(np.zeros((4, 4), np.uint8))
+    assert not (cpu.intersect(rays, order="index")[0][:, 10] >= 0).any()
+    cpu.set_opacity(np.zeros((4, 4), np.uint8), tri_flags=np.zeros(cpu.n_tri, np.uint8))
+    assert np.array_equal(cpu.intersect(rays, order="index")[0], h0)
