@@ -153,80 +153,112 @@ def work_per_ray(stats):
                                                                       "sub_squares", "newton_iters"])}
 
 
-def cpu_sample(sc, rays, hits_t, budget_s: float, use_ref: bool):
-    """Times the CPU reference on a bounded sample: a block of primary rays
-    around the image centre and their bounce rays, over only the patches
-    whose boxes those rays reach (the flat loop's result is unchanged by
-    dropping triangles a ray's box test rejects)."""
+CPU_STRIDE = 64   # the CPU legs answer every 64th ray of the step's ray list
+
+
+def cpu_scene(sc, use_ref: bool):
+    """The scene on the CPU checker: the reference's own sources compiled
+    here (oracle/_ref) when present, else the C port; every patch."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import py_oracle
     lib = py_oracle.Reference() if use_ref and py_oracle.Reference.available() else py_oracle.Oracle()
     kind = "reference" if isinstance(lib, py_oracle.Reference) else "port"
-    W, H = (1920, 1080) if len(rays) == 1920 * 1080 else (480, 270) if len(rays) == 480 * 270 else (None, None)
-    if W:
-        jj, ii = np.mgrid[H // 2 - 32:H // 2 + 32, W // 2 - 32:W // 2 + 32]
-        idx = (jj * W + ii).ravel()
-    else:
-        idx = np.arange(min(len(rays), 4096))
-    sample = rays[idx]
-    ok = np.isfinite(hits_t[idx])
-    # object set: patches whose triangle boxes any sample ray meets
-    tris = sc.tris
-    keep_assets = sorted(set(sc.tri_asset.tolist())) if len(sc.assets) <= 4 else None
-    sub = sc
-    if keep_assets is None:
-        from dmap_b200 import Scene  # noqa
-        lo = np.minimum(np.minimum(tris[:, 0:3], tris[:, 3:6]), tris[:, 6:9]) - 0.2
-        hi = np.maximum(np.maximum(tris[:, 0:3], tris[:, 3:6]), tris[:, 6:9]) + 0.2
-        o, d = sample[:, 0:3].astype(np.float64), sample[:, 3:6].astype(np.float64)
-        with np.errstate(divide="ignore", invalid="ignore"):
-            inv = 1.0 / d
-            t0 = (lo[None] - o[:, None]) * inv[:, None]
-            t1 = (hi[None] - o[:, None]) * inv[:, None]
-        tn = np.nanmax(np.minimum(t0, t1), axis=2)
-        tf = np.nanmin(np.maximum(t0, t1), axis=2)
-        touched = np.any((tn <= tf) & (tf >= 0), axis=0)
-        keep_assets = sorted(set(sc.tri_asset[touched].tolist()))
-        sub = scenes.Scene([sc.assets[a] for a in keep_assets],
-                           np.concatenate([sc.tris[sc.tri_asset == a] for a in keep_assets]),
-                           np.concatenate([np.full((sc.tri_asset == a).sum(), k, np.int32)
-                                           for k, a in enumerate(keep_assets)]))
-    cpu = py_oracle.CpuScene(lib, sub)
-    threads = os.cpu_count() or 1
+    return py_oracle.CpuScene(lib, sc), kind
+
+
+def stride_sample(rays_all, stride: int = CPU_STRIDE):
+    """Every stride-th ray of the step's whole ray list (primaries then
+    bounces, in order), so the sample keeps the workload's mix of misses,
+    primary hits and bounce rays over all patches."""
+    return np.ascontiguousarray(rays_all[::stride])
+
+
+def sample_desc(n_sample, n_all, n_patches):
+    return (f"{n_sample} rays: every {CPU_STRIDE}th of the step's {n_all} (primaries and bounces in proportion), "
+            f"all {n_patches} patches, flat loop")
+
+
+def time_cpu(cpu, sample, budget_s: float, threads: int):
+    """Rays/s of the CPU flat loop on the sample, repeated to fill about
+    budget_s seconds of CPU work."""
     t = time.perf_counter()
-    h, _ = cpu.intersect(sample, threads=threads, order="index")
+    cpu.intersect(sample, threads=threads, order="index")
     dt = time.perf_counter() - t
-    # the bounce rays of the sample's hits
-    hit = np.isfinite(h[:, 0])
-    b = scenes.bounce_rays(sample[hit], h[hit, 0], h[hit, 5:8])
-    allr = np.concatenate([sample, b])
-    reps = max(1, int(budget_s / max(dt * len(allr) / len(sample), 1e-3)))
-    reps = min(reps, 64)
-    return cpu, allr, kind, threads, len(keep_assets), reps
+    reps = int(min(64, max(1, budget_s / max(dt, 1e-3))))
+    t = time.perf_counter()
+    for _ in range(reps):
+        cpu.intersect(sample, threads=threads, order="index")
+    return len(sample) * reps / (time.perf_counter() - t) / 1e6
 
 
 def run_cpu(args, rank, world):
-    sc, rays = build_scene(args.config, args.small)
-    # primary hits for the bounce rays: the CPU sample takes its own from the oracle
-    cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, rays, np.zeros(len(rays)), 10.0, True)
+    """The reference arm: the reference's own C++ query (oracle/_ref, flat
+    loop) on every host core. Its rays are the GPU arm's: the primaries, and
+    one bounce per primary hit from the CPU's own FP64 hits (bit-identical
+    to the device FP64 path's), then every CPU_STRIDE-th ray of that list
+    per step."""
+    sc, prim = build_scene(args.config, args.small)
+    cpu, kind = cpu_scene(sc, True)
+    threads = os.cpu_count() or 1
+    h0, _ = cpu.intersect(prim, threads=threads, order="index")
+    hit = h0[:, 10] >= 0
+    bounce = scenes.bounce_rays(prim[hit], h0[hit, 0], h0[hit, 5:8])
+    rays_all = np.concatenate([prim, bounce, extra_rays(args.config, sc, args.small)]).astype(np.float32)
+    sample = stride_sample(rays_all)
     times = []
     for s in range(args.warmup + args.steps):
         t = time.perf_counter()
-        cpu.intersect(allr, threads=threads, order="index")
+        cpu.intersect(sample, threads=threads, order="index")
         dt = time.perf_counter() - t
         if s >= args.warmup:
             times.append(dt)
     ms = 1e3 * float(np.mean(times))
-    v = len(allr) / (ms * 1e-3) / 1e6
+    v = len(sample) / (ms * 1e-3) / 1e6
+    desc = sample_desc(len(sample), len(rays_all), len(sc.assets))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(args), "sample_rays": len(allr), "sample_objects": n_obj},
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": kind,
-                             "sample": f"{len(allr)} rays (64x64 primary block at the image centre + bounces) "
-                                       f"over the {n_obj} patches they reach"},
+            "config": {"workload": workload_name(args), "rays_per_step": len(rays_all), "sample_rays": len(sample),
+                       "sample_objects": len(sc.assets), "order": "index (the reference's flat loop)"},
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": kind, "sample": desc},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def parity_fields(got, ref, extent):
+    """The timed step's FP32 hits against the FP64 device path's on the same
+    rays and triangle order (the FP64 path equals the CPU oracle bit for
+    bit): hit/miss set, false misses, and the t / uv / normal error."""
+    g_hit, r_hit = got["tri"] >= 0, ref["tri"] >= 0
+    both = g_hit & r_hit
+    out = {"rays": int(len(ref)), "hits": int(r_hit.sum()),
+           "mismatched_hit_set": int((g_hit != r_hit).sum()),
+           "false_misses": int((r_hit & ~g_hit).sum()),
+           "extra_hits": int((g_hit & ~r_hit).sum()),
+           "triangle_mismatch": int((both & (got["tri"] != ref["tri"])).sum())}
+    if both.any():
+        t_g = got["t"][both].astype(np.float64)
+        t_r = ref["t"][both]
+        dt = np.abs(t_g - t_r)
+        out["max_abs_dt"] = float(dt.max())
+        out["max_rel_dt"] = float(dt.max() / extent)
+        out["t_equal_to_rounded_fp64"] = float(np.mean(t_g == t_r.astype(np.float32)))
+        out["max_duv"] = float(np.abs(got["st"][both].astype(np.float64) - ref["st"][both]).max())
+        out["max_dng"] = float(np.abs(got["ng"][both].astype(np.float64) - ref["ng"][both]).max())
+    out["extent"] = extent
+    out["bar"] = "hit set identical, zero false misses, max |dt| <= 1e-5 x extent"
+    out["pass"] = bool(out["mismatched_hit_set"] == 0 and out.get("max_rel_dt", 0.0) <= 1e-5)
+    return out
+
+
+def scene_extent(dev, n_tri):
+    """Diagonal of the union of the triangles' object boxes."""
+    lo, hi = np.full(3, np.inf), np.full(3, -np.inf)
+    for k in range(n_tri):
+        info = dev.triangle_info(k)
+        lo = np.minimum(lo, info[3:6])
+        hi = np.maximum(hi, info[6:9])
+    return float(np.linalg.norm(hi - lo))
 
 
 def workload_name(args):
@@ -318,7 +350,7 @@ def main():
     my = np.ascontiguousarray(rays_all[lo:hi])
     n = len(my)
     # algorithmic work of the query on these rays (FP64 path counters, same triangle order)
-    _, st = dev.intersect(my, ref_opt, np.float64, stats=True)
+    h_ref, st = dev.intersect(my, ref_opt, np.float64, stats=True)
     flops_ray, bytes_ray, counts = work_per_ray(st)
     # and of the reference's flat loop (index order), for comparison
     counts_flat = work_per_ray(dev.intersect(my, flat_opt, np.float64, stats=True)[1])[2]
@@ -422,16 +454,19 @@ def main():
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
+    # parity of the last timed step's hits (outside the timed region)
+    got = np.frombuffer(hits_d.cpu().numpy().tobytes(), dm.HIT32)
+    line["parity"] = parity_fields(got, h_ref, scene_extent(dev, len(sc.tris)))
+    line["parity"]["against"] = "FP64 device path, same rays and triangle order (equal to the CPU oracle)"
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu, allr, kind, threads, n_obj, reps = cpu_sample(sc, prim, np.where(hit, 1.0, np.inf), 10.0, True)
-            t = time.perf_counter()
-            for _ in range(reps):
-                cpu.intersect(allr, threads=threads, order="index")
-            dt = (time.perf_counter() - t) / reps
-            line["cpu_baseline"] = {"value": len(allr) / dt / 1e6, "unit": "Mrays/s", "cores": threads,
-                                    "kind": kind, "sample": f"{len(allr)} rays (64x64 primary block at the image "
-                                                            f"centre + bounces) over the {n_obj} patches they reach"}
+            cpu, kind = cpu_scene(sc, True)
+            sample = stride_sample(rays_all)
+            threads = os.cpu_count() or 1
+            v = time_cpu(cpu, sample, 10.0, threads)
+            line["cpu_baseline"] = {"value": v, "unit": "Mrays/s", "cores": threads, "kind": kind,
+                                    "sample": sample_desc(len(sample), n_all, len(sc.assets))}
+            del cpu
         except Exception as e:  # the baseline is reported, not required
             line["cpu_baseline"] = {"error": str(e)[:200]}
     if rank == 0:

@@ -11,7 +11,7 @@ of include/dmap_b200.h (libdmap_b200.so, built in place by
   queries (ObjectIntersector::intersect, embree intersect_callback) and
   occlusion queries (occluded_callback) for a batch of rays.
 - ``TraversalOptions``: the reference's bound / slab_max_level / leaf
-  (traversal_options.h:600-608) plus precision, mode and the schedule.
+  (traversal_options.h:30-38) plus precision, mode and the schedule.
 - ``Scene.render``: the batched path tracer (emitter-sampled shadow rays
   through the occlusion query); ``Server``: continuous batching of many
   callers' requests over resident scenes; ``Scene.autotune``: the schedule
@@ -63,7 +63,7 @@ class DmapError(RuntimeError):
 class _Options(C.Structure):
     _fields_ = [("bound", C.c_int), ("slab_max_level", C.c_int), ("leaf", C.c_int), ("precision", C.c_int),
                 ("mode", C.c_int), ("polish_cond", C.c_double), ("schedule", C.c_int), ("rounds", C.c_int),
-                ("blocks_per_sm", C.c_int), ("order", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("order", C.c_int), ("node_visit_cap", C.c_int)]
 
 
 class _Camera(C.Structure):
@@ -139,6 +139,7 @@ def lib() -> C.CDLL:
             "dmap_asset_build_ms": (dbl, [vp]),
             "dmap_asset_pyramid_level": (i32, [vp, i32, i32, vp]),
             "dmap_scene_create": (i32, [vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
+            "dmap_scene_create_charts": (i32, [vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
             "dmap_scene_create_instanced": (i32, [vp, vp, i32, vp, vp, vp, i32, vp, vp, i32, C.POINTER(vp)]),
             "dmap_scene_destroy": (None, [vp]),
             "dmap_scene_triangle_count": (i32, [vp]),
@@ -170,6 +171,7 @@ def lib() -> C.CDLL:
             "dmap_server_poll": (i32, [vp, C.c_uint64]),
             "dmap_server_wait": (i32, [vp, C.c_uint64, dbl]),
             "dmap_server_cancel": (i32, [vp, C.c_uint64]),
+            "dmap_server_pause": (i32, [vp, C.c_int]),
             "dmap_server_latency": (i32, [vp, C.c_uint64, C.POINTER(dbl)]),
             "dmap_server_drain": (i32, [vp, dbl]),
             "dmap_server_get_stats": (i32, [vp, C.POINTER(_ServerStats)]),
@@ -201,11 +203,12 @@ class TraversalOptions:
     rounds: int = 6
     blocks_per_sm: int = 5
     order: str = "nearest"
+    node_visit_cap: int = 0
 
     def c(self) -> _Options:
         return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],
                         MODE[self.mode], self.polish_cond, SCHEDULE[self.schedule], self.rounds,
-                        self.blocks_per_sm, ORDER[self.order])
+                        self.blocks_per_sm, ORDER[self.order], self.node_visit_cap)
 
 
 class Context:
@@ -573,6 +576,10 @@ class Server:
 
     def cancel(self, rid: int) -> int:
         return lib().dmap_server_cancel(self.h, rid)
+
+    def pause(self, paused: bool = True):
+        """Holds (or resumes) admission: submitted requests stay queued."""
+        self.ctx.check(lib().dmap_server_pause(self.h, int(paused)), "dmap_server_pause")
 
     def latency_ms(self, rid: int) -> float:
         ms = C.c_double()

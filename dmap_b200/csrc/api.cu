@@ -87,6 +87,7 @@ void dmap_options_default(dmap_options *opt)
     opt->rounds = 6;
     opt->blocks_per_sm = 5;
     opt->order = DMAP_ORDER_NEAREST;
+    opt->node_visit_cap = 0;
 }
 
 // ---- assets ---------------------------------------------------------------
@@ -266,8 +267,8 @@ dmap_status dmap_asset_pyramid_level(const dmap_asset *a, int level, int precisi
 
 // ---- scenes ----------------------------------------------------------------
 
-dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset,
-                              const double *tris, int n_tri, dmap_scene **out)
+static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset,
+                                const double *tris, int stride, int n_tri, dmap_scene **out)
 {
     if (!ctx || !assets || n_assets <= 0 || !tri_asset || !tris || n_tri <= 0 || !out)
         return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: bad argument");
@@ -278,8 +279,8 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
     for (int k = 0; k < n_tri; ++k) {
         if (tri_asset[k] < 0 || tri_asset[k] >= n_assets)
             return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: triangle asset index out of range");
-        for (int q = 0; q < 24; ++q)
-            if (!std::isfinite(tris[24 * (size_t)k + q]))
+        for (int q = 0; q < stride; ++q)
+            if (!std::isfinite(tris[stride * (size_t)k + q]))
                 return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: non-finite triangle data");
     }
     DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -312,15 +313,15 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
     if ((e = cudaMalloc((void **)&s->assets_dev, sizeof(AssetDev) * n_assets)) != cudaSuccess ||
         (e = cudaMalloc((void **)&s->tris_dev, sizeof(TriDev) * n_tri)) != cudaSuccess ||
         (e = cudaMalloc((void **)&s->tris32_dev, sizeof(TriDev32) * n_tri)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&tris_dev, sizeof(double) * 24 * n_tri)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&tris_dev, sizeof(double) * stride * n_tri)) != cudaSuccess ||
         (e = cudaMalloc((void **)&ta_dev, sizeof(int) * n_tri)) != cudaSuccess)
         return cleanup(cuda_fail(ctx, e, "dmap_scene_create: cudaMalloc"));
     if ((e = cudaMemcpy(s->assets_dev, ad.data(), sizeof(AssetDev) * n_assets, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(tris_dev, tris, sizeof(double) * 24 * n_tri, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(tris_dev, tris, sizeof(double) * stride * n_tri, cudaMemcpyHostToDevice)) ||
         (e = cudaMemcpy(ta_dev, tri_asset, sizeof(int) * n_tri, cudaMemcpyHostToDevice)))
         return cleanup(cuda_fail(ctx, e, "dmap_scene_create: upload"));
-    if ((e = dmapk::launch_setup(tris_dev, ta_dev, s->assets_dev, n_tri, s->tris_dev, s->tris32_dev, ctx->status_dev,
-                                 ctx->stream)) != cudaSuccess)
+    if ((e = dmapk::launch_setup(tris_dev, stride, ta_dev, s->assets_dev, n_tri, s->tris_dev, s->tris32_dev,
+                                 ctx->status_dev, ctx->stream)) != cudaSuccess)
         return cleanup(cuda_fail(ctx, e, "dmap_scene_create: setup launch"));
     ctx->launches += 1;
     dmap_status st = sync_and_check(ctx, "dmap_scene_create");
@@ -441,6 +442,18 @@ dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int 
     return DMAP_OK;
 }
 
+dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset,
+                              const double *tris, int n_tri, dmap_scene **out)
+{
+    return scene_create(ctx, assets, n_assets, tri_asset, tris, dmapk::kVertexRecord, n_tri, out);
+}
+
+dmap_status dmap_scene_create_charts(dmap_context *ctx, dmap_asset *const *assets, int n_assets,
+                                     const int *tri_asset, const double *charts, int n_tri, dmap_scene **out)
+{
+    return scene_create(ctx, assets, n_assets, tri_asset, charts, dmapk::kChartRecord, n_tri, out);
+}
+
 dmap_status dmap_scene_create_instanced(dmap_context *ctx, dmap_asset *const *assets, int n_assets,
                                         const int *tri_asset, const double *tris, const int *object_first,
                                         int n_objects, const int *instance_object, const double *to_world,
@@ -526,6 +539,11 @@ dmap_status dmap_scene_set_opacity(dmap_scene *s, const uint8_t *mask_host, int 
     if (mask_host && !(m.uv_scale[0] != 0.0 && m.uv_scale[1] != 0.0 && std::isfinite(m.uv_scale[0]) &&
                        std::isfinite(m.uv_scale[1]) && std::isfinite(m.uv_offset[0]) && std::isfinite(m.uv_offset[1])))
         return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_set_opacity: uv_scale must be finite and non-zero");
+    // a server's queued or running requests on this scene were admitted
+    // under the current filter, and its worker thread may be launching them
+    if (s->server_pending.load() > 0)
+        return fail(ctx, DMAP_ERR_NOT_READY,
+                    "dmap_scene_set_opacity: a server still holds requests on this scene (drain it first)");
     DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
     // queries in flight, on any stream, may read the old mask
     DMAP_CUDA(ctx, cudaDeviceSynchronize());
@@ -603,7 +621,10 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
         return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad schedule options");
     if (o.order < 0 || o.order > 1)
         return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: bad order");
+    if (o.node_visit_cap < 0)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: node_visit_cap must be >= 0");
     q.order = o.order;
+    q.guard_cap = o.node_visit_cap > 0 ? o.node_visit_cap : (1 << 26);
     q.schedule = o.schedule;
     q.rounds = o.rounds;
     q.blocks_per_sm = o.blocks_per_sm;

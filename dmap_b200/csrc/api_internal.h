@@ -74,6 +74,9 @@ struct dmap_scene
     unsigned char *op_tri_dev = nullptr;
     int op_w = 0, op_h = 0;
     dmap_uv_map op_map = {{1.0, 1.0}, {0.0, 0.0}, 0};
+    // server requests on this scene not yet done (queued or running): the
+    // filter may not change under them
+    std::atomic<int> server_pending{0};
 };
 
 namespace dmapi

@@ -11,6 +11,7 @@
 //               rounding, h_min down, h_max up
 //   triangles   one TriDev (FP64) and one TriDev32 (FP32) record each
 #pragma once
+#include <cmath>
 #include <cstdint>
 
 namespace dmapdev
@@ -83,6 +84,33 @@ struct TriDev32
 constexpr unsigned kStatusCapped = 1u;
 constexpr unsigned kStatusBadInput = 2u;
 
+// A ray the query cannot answer: a non-finite origin or direction
+// component, a zero direction, or a NaN t_min / t_max. Such a ray is
+// answered as a miss (the reference has no defined result for it).
+__host__ __device__ __forceinline__ bool ray_unanswerable(const double *o, const double *d, double t_min,
+                                                          double t_max)
+{
+    bool bad = t_min != t_min || t_max != t_max || (d[0] == 0.0 && d[1] == 0.0 && d[2] == 0.0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        bad = bad || !(fabs(o[a]) <= 1.7976931348623157e308) || !(fabs(d[a]) <= 1.7976931348623157e308);
+    return bad;
+}
+
+// An unanswerable ray is replaced by one that every box test rejects
+// (t_min > t_max), so every kernel answers it as a miss without a branch of
+// its own.
+__host__ __device__ __forceinline__ void sanitize_ray(double *o, double *d, double &t_min, double &t_max)
+{
+    if (ray_unanswerable(o, d, t_min, t_max)) {
+        o[0] = o[1] = o[2] = 0.0;
+        d[0] = 1.0;
+        d[1] = d[2] = 0.0;
+        t_min = 1.0;
+        t_max = 0.0;
+    }
+}
+
 // Hit records, laid out as dmap_hit32 / dmap_hit64 of include/dmap_b200.h.
 struct Hit32
 {
@@ -101,6 +129,9 @@ struct Hit64
 // same names when it is included first).
 #ifndef DMAP_HIT_FP64_LEAF
 #define DMAP_HIT_FP64_LEAF 1 // the root came from the FP64 certified Newton leaf
+#endif
+#ifndef DMAP_HIT_CAPPED
+#define DMAP_HIT_CAPPED 2 // a walk cap of the query ran out for this ray
 #endif
 
 // Per-ray counter slots (TraversalStats), as DMAP_ST_* of include/dmap_b200.h.

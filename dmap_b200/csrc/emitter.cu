@@ -28,7 +28,7 @@ namespace
 {
 using namespace d64;
 
-// FootprintChild (descent_sampler.h:67-73)
+// FootprintChild (descent_sampler.h:71-78)
 struct FpChild
 {
     int overlap; // OUTSIDE / INSIDE / STRADDLE
@@ -79,7 +79,7 @@ struct HostTile
     int n_leaf = 0, n_levels = 0;
     std::vector<std::vector<double>> mean;
 
-    double mean_at(int level, int64_t i, int64_t j) const // emission_tile.cpp:91-110 (repeat)
+    double mean_at(int level, int64_t i, int64_t j) const // emission_tile.cpp:99-118 (repeat)
     {
         if (level >= n_levels)
             return mean.back()[0];
@@ -141,7 +141,7 @@ int host_classify(const TriDev &T, double cx, double cy, double s) // uv_clip.cp
     return all_inside ? INSIDE : STRADDLE;
 }
 
-double host_clipped_area(const TriDev &T, double cx, double cy, double s) // uv_clip.cpp:51-90
+double host_clipped_area(const TriDev &T, double cx, double cy, double s) // uv_clip.cpp:46-83
 {
     double px[8], py[8], qx[8], qy[8];
     int n = 4;
@@ -381,7 +381,7 @@ __device__ __forceinline__ Receiver load_receiver(const double *r, int64_t k)
     return R;
 }
 
-__device__ inline v2 sample_polygon(const ClipPoly &poly, double xi_tri, double xi1, double xi2) // uv_clip.cpp:92-115
+__device__ inline v2 sample_polygon(const ClipPoly &poly, double xi_tri, double xi1, double xi2) // uv_clip.cpp:85-108
 {
     double areas[8];
     double total = 0.0;
@@ -517,7 +517,7 @@ __global__ void pdf_kernel(Emit E, const int32_t *__restrict__ tri_of, const dou
             const TriEmit &F = E.temit[tri];
             const Receiver rcv = load_receiver(recv, k);
             const double u = uv[2 * k], v = uv[2 * k + 1];
-            // pdf_uv / leaf_prob (descent_sampler.cpp:292-354)
+            // pdf_uv / leaf_prob (descent_sampler.cpp:290-356)
             const int n_leaf = g.n_leaf;
             const int64_t i = (int64_t)floor(u / (1.0 / n_leaf)), j = (int64_t)floor(v / (1.0 / n_leaf));
             const int L = F.root_level;

@@ -29,7 +29,7 @@ __device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) 
 
 struct Node32 { float h0, gu, gv, r, mn, mx; };
 
-// TaylorPyramid::node (taylor_pyramid.cpp:368-383) on the FP32 pyramid:
+// TaylorPyramid::node (taylor_pyramid.cpp:259-274) on the FP32 pyramid:
 // wrapped indices (the level's width is a power of two), above the root the
 // root's height range as a min-max node.
 __device__ __forceinline__ Node32 fetch_node(const AssetDev &a, int level, int i, int j)
@@ -188,7 +188,7 @@ __device__ __forceinline__ void box_axis(float a0, float au, float av, float cx,
     float half = ru_add(ru_add(fabsf(a), fabsf(b)), k);
     m_lo = __fsub_rd(c, half);
     m_hi = __fadd_ru(c, half);
-    // h m (affine_form.cpp:146-156 with h = mid +- hh), then + p
+    // h m (affine_form.cpp:35-47 with h = mid +- hh), then + p
     float sc = mid * c, sa = mid * a, sb = mid * b;
     float sk = ru_fma(G, mag3(sc, sa, sb), ru_fma(hh, ru_add(mag3(c, a, b), k), ru_mul(fabsf(mid), k)));
     float tc = sc + pc, ta = sa + pa, tb = sb + pb;
@@ -290,6 +290,7 @@ __device__ __forceinline__ void load_ray(const R *rays, int64_t k, double *o, do
     }
     t_min = (double)r[6];
     t_max = (double)r[7];
+    dmapdev::sanitize_ray(o, d, t_min, t_max);
 }
 
 template <typename H, typename Fp>

@@ -1,5 +1,5 @@
 // The certified Newton leaf in double with the reference's operation order
-// (displaced_intersector.cpp:222-426: plane_basis, newton_from,
+// (displaced_intersector.cpp:22-27,239-440: plane_basis, newton_from,
 // sub_square_bound, search_leaf, intersect_newton, the two-triangle leaf).
 // Included by translation units compiled with -fmad=false.
 #pragma once
@@ -11,7 +11,7 @@ namespace d64
 
 struct hit64 { double t; v2 st, bary; v3 ng; int64_t i, j; };
 
-__device__ inline void plane_basis(v3 n, v3 &d1, v3 &d2) // :222-227
+__device__ inline void plane_basis(v3 n, v3 &d1, v3 &d2) // :22-27
 {
     v3 a = fabs(n.x) < 0.9 ? V3(1.0, 0.0, 0.0) : V3(0.0, 1.0, 0.0);
     d1 = normalized3(cross3(a, n));
@@ -81,7 +81,7 @@ __device__ inline bool newton_from(const TriDev &T, const AssetDev &g, v3 o, v3 
 
 struct leafbound { v2 lo; double w, h00, h10, h01, h11; af3 N_hat; v3 o, dn, d1, d2; double d_len; };
 
-__device__ __forceinline__ af restricted(af f, double a, double b, double rho) // :272-276
+__device__ __forceinline__ af restricted(af f, double a, double b, double rho) // :72-76
 {
     double alpha = 2.0 * a - 1.0, beta = 2.0 * b - 1.0, r = 2.0 * rho;
     return {(f.c + f.a * alpha) + f.b * beta, f.a * r, f.b * r, f.k};
@@ -188,7 +188,7 @@ __device__ inline bool intersect_newton(const TriDev &T, const AssetDev &g, v3 o
 }
 
 __device__ inline bool ray_triangle(v3 o, v3 d, double t_min, double t_max, v3 A, v3 B, v3 C, double &t, double &b1,
-                             double &b2) // :230-249
+                             double &b2) // :30-49
 {
     v3 e1 = sub3(B, A), e2 = sub3(C, A);
     v3 p = cross3(d, e2);

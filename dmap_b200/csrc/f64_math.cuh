@@ -67,9 +67,9 @@ __device__ __forceinline__ ivl interval(af f) // affine_form.h:50-54
     double e = (fabs(f.a) + fabs(f.b)) + f.k;
     return {f.c - e, f.c + e};
 }
-__device__ __forceinline__ af add(af x, af y) { return {x.c + y.c, x.a + y.a, x.b + y.b, x.k + y.k}; } // :126-133
-__device__ __forceinline__ af scale(double s, af x) { return {x.c * s, x.a * s, x.b * s, x.k * fabs(s)}; } // :158-165
-__device__ __forceinline__ af mul(af x, af r) // :146-156
+__device__ __forceinline__ af add(af x, af y) { return {x.c + y.c, x.a + y.a, x.b + y.b, x.k + y.k}; } // affine_form.cpp:17-24
+__device__ __forceinline__ af scale(double s, af x) { return {x.c * s, x.a * s, x.b * s, x.k * fabs(s)}; } // affine_form.cpp:49-56
+__device__ __forceinline__ af mul(af x, af r) // affine_form.cpp:35-47
 {
     double u = (fabs(x.a) + fabs(x.b)) + x.k;
     double v = (fabs(r.a) + fabs(r.b)) + r.k;
@@ -82,7 +82,7 @@ __device__ __forceinline__ af mul(af x, af r) // :146-156
     return o;
 }
 __device__ __forceinline__ double grs(double x) { return 1.0 / sqrt(x); }
-__device__ __forceinline__ af rsqrt_form(af f) // :173-185, Min-Range
+__device__ __forceinline__ af rsqrt_form(af f) // affine_form.cpp:64-76, Min-Range
 {
     ivl range = interval(f);
     double lo = range.lo, hi = range.hi;
@@ -95,7 +95,7 @@ __device__ __forceinline__ af3 AF3(v3 c, v3 a, v3 b)
 {
     return {{c.x, a.x, b.x, 0.0}, {c.y, a.y, b.y, 0.0}, {c.z, a.z, b.z, 0.0}};
 }
-__device__ __forceinline__ af sq_length(const af3 &v) // :187-194
+__device__ __forceinline__ af sq_length(const af3 &v) // affine_form.cpp:78-85
 {
     v3 xc = {v.x.c, v.y.c, v.z.c}, xu = {v.x.a, v.y.a, v.z.a}, xv = {v.x.b, v.y.b, v.z.b};
     v3 xk = {v.x.k, v.y.k, v.z.k};
@@ -103,7 +103,7 @@ __device__ __forceinline__ af sq_length(const af3 &v) // :187-194
     double offset = 0.5 * dot3(dev, dev);
     return {dot3(xc, xc) + offset, 2.0 * dot3(xc, xu), 2.0 * dot3(xc, xv), 2.0 * fabs(dot3(xc, xk)) + offset};
 }
-__device__ __forceinline__ void normalize(af3 &v) // :196-204
+__device__ __forceinline__ void normalize(af3 &v) // affine_form.cpp:87-95
 {
     af l = sq_length(v);
     if (interval(l).lo <= 0.0) {
@@ -116,11 +116,11 @@ __device__ __forceinline__ void normalize(af3 &v) // :196-204
     v.z = mul(r, v.z);
 }
 __device__ __forceinline__ af3 add(const af3 &a, const af3 &b) { return {add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)}; }
-__device__ __forceinline__ af dot(v3 a, const af3 &b) // :210
+__device__ __forceinline__ af dot(v3 a, const af3 &b) // affine_form.cpp:101
 {
     return add(add(scale(a.x, b.x), scale(a.y, b.y)), scale(a.z, b.z));
 }
-__device__ __forceinline__ af3 matmul(const double (*A)[3], const af3 &v) // :212-215
+__device__ __forceinline__ af3 matmul(const double (*A)[3], const af3 &v) // affine_form.cpp:103-106
 {
     return {dot(V3(A[0][0], A[0][1], A[0][2]), v), dot(V3(A[1][0], A[1][1], A[1][2]), v),
             dot(V3(A[2][0], A[2][1], A[2][2]), v)};
@@ -135,11 +135,11 @@ __device__ __forceinline__ double cell_width(const AssetDev &a, int level) // ta
     return ldexp(1.0, level) / a.n_leaf;
 }
 
-__device__ __forceinline__ node pyramid_node(const AssetDev &a, int level, int64_t i, int64_t j) // taylor_pyramid.cpp:368-383
+__device__ __forceinline__ node pyramid_node(const AssetDev &a, int level, int64_t i, int64_t j) // taylor_pyramid.cpp:259-274
 {
     node n;
     // pyr64 holds the levels before the offset; the reference adds it once
-    // after the build (taylor_pyramid.cpp:351-359), here on read.
+    // after the build (taylor_pyramid.cpp:239-250), here on read.
     if (level >= a.n_levels) {
         const double *root = a.pyr64 + 8 * a.level_off[a.n_levels - 1];
         double lo = root[6], hi = root[7];
@@ -195,7 +195,7 @@ __device__ __forceinline__ double grid_value(const AssetDev &a, int j, int i)
 
 __device__ __forceinline__ void grid_cell(const AssetDev &g, double x, double y, int &i, int &j, double &s, double &t)
 {
-    // displaced_surface.cpp:364-379
+    // displaced_surface.cpp:12-27
     if (g.repeat) {
         x -= floor(x);
         y -= floor(y);
@@ -212,7 +212,7 @@ __device__ __forceinline__ void grid_cell(const AssetDev &g, double x, double y,
     t = fy - j;
 }
 
-__device__ __forceinline__ double grid_h(const AssetDev &g, double x, double y) // displaced_surface.cpp:381-389
+__device__ __forceinline__ double grid_h(const AssetDev &g, double x, double y) // displaced_surface.cpp:29-37
 {
     int i, j;
     double s, t;
@@ -225,7 +225,7 @@ __device__ __forceinline__ double grid_h(const AssetDev &g, double x, double y) 
 
 __device__ __forceinline__ void grid_h_grad(const AssetDev &g, double x, double y, double &h, v2 &gr)
 {
-    // displaced_surface.cpp:381-399, h and grad from one cell lookup
+    // displaced_surface.cpp:29-47, h and grad from one cell lookup
     int i, j;
     double s, t;
     grid_cell(g, x, y, i, j, s, t);
@@ -238,7 +238,7 @@ __device__ __forceinline__ void grid_h_grad(const AssetDev &g, double x, double 
     gr = {g.scale * (dh_ds * (g.W - 1)), g.scale * (dh_dt * (g.W - 1))};
 }
 
-// ---- base triangle (displaced_surface.h:300-304, .cpp:451-460) -----------
+// ---- base triangle (displaced_surface.h:83-87, .cpp:99-108) -----------
 __device__ __forceinline__ v3 tri_P(const TriDev &T, double s, double t)
 {
     return add3(add3(L3(T.q0), mul3(s, L3(T.e1))), mul3(t, L3(T.e2)));
@@ -300,7 +300,7 @@ struct ClipPoly
     v2 p[8];
 };
 
-// clip_square (uv_clip.cpp:61-90): Sutherland-Hodgman of the square (c, s)
+// clip_square (uv_clip.cpp:56-83): Sutherland-Hodgman of the square (c, s)
 // against the domain's three inward half-planes (at most 7 vertices).
 __device__ inline ClipPoly clip_square(const TriDev &T, v2 c, double s)
 {
@@ -337,7 +337,7 @@ __device__ __forceinline__ double interval_tolerance(double t_scale) { return 1e
 
 struct box3 { v3 lo, hi; };
 
-__device__ __forceinline__ bool box_clip(const box3 &B, v3 o, v3 d, double &t0, double &t1) // :25-44
+__device__ __forceinline__ bool box_clip(const box3 &B, v3 o, v3 d, double &t0, double &t1) // node_bounds.cpp:25-44
 {
     for (int a = 0; a < 3; ++a) {
         double da = comp(d, a), oa = comp(o, a);

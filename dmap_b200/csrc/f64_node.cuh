@@ -1,7 +1,7 @@
 // The node test in double with the reference's operation order
 // (node_bounds.cpp:83-211: node_bound, box_interval, slab_interval,
 // node_interval) and the level-0 pyramid node computed straight from the
-// node grid (leaf_level, taylor_pyramid.cpp:154-176), for translation units
+// node grid (leaf_level, taylor_pyramid.cpp:45-67), for translation units
 // compiled with -fmad=false: the FP64 walk, and the FP32 path's check of a
 // leaf cell before its leaf runs.
 #pragma once
@@ -82,7 +82,7 @@ __device__ __forceinline__ ivl IV(double lo, double hi) { return {lo, hi}; }
 __device__ __forceinline__ ivl iv_add(ivl a, ivl b) { return {a.lo + b.lo, a.hi + b.hi}; }
 __device__ __forceinline__ ivl iv_scale(double s, ivl a) { return s >= 0.0 ? IV(s * a.lo, s * a.hi) : IV(s * a.hi, s * a.lo); }
 
-// The ray in the triangle's tangent frame (displaced_intersector.cpp:184-186).
+// The ray in the triangle's tangent frame (displaced_intersector.cpp:178).
 struct tray { v3 o, d; double t_min, t_max; };
 
 __device__ __forceinline__ tray tangent_ray64(const TriDev &T, v3 o, v3 d, double t_min, double t_max)

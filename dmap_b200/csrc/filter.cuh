@@ -2,7 +2,7 @@
 // intersect and occluded callbacks run it (displaced_geometry.cpp:53-106):
 // the triangle's nearest crossing past t_lo goes to the filter; a crossing it
 // rejects raises t_lo to the crossing's t and the triangle is walked again,
-// at most max_filter_passes times (displaced_geometry.h:62). The filter is
+// at most max_filter_passes times (displaced_geometry.h:64). The filter is
 // ks's opacity map reduced to a binary texel mask over the object's texture
 // coordinates. Included by translation units compiled with -fmad=false, so
 // the texture coordinate is the reference's to the bit.
@@ -22,7 +22,7 @@ __device__ inline bool crossing_opaque(const dmapk::QueryOpts &q, const TriDev &
     if (!q.op_mask || (q.op_tri && !q.op_tri[tri]))
         return true;
     // potential_hit hands the filter float barycentrics (displaced_geometry.cpp:21-34);
-    // compute_hit_texcoord (:189-193): BaseTriangle::param (displaced_surface.h:88)
+    // compute_hit_texcoord (:189-193): BaseTriangle::param (displaced_surface.h:87)
     // and DisplacedObject::object_uv (scene_spec.cpp:382-388), rounded to float
     const double u = (double)(float)bu, v = (double)(float)bv;
     const double s = (T.t0[0] + u * (T.t1[0] - T.t0[0])) + v * (T.t2[0] - T.t0[0]);

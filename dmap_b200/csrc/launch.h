@@ -19,6 +19,7 @@ struct QueryOpts
     int rounds;               // wavefront: walk/leaf rounds before the inline-leaf drain
     int blocks_per_sm;        // wavefront walk: resident 128-thread CTAs per SM
     int order = 1;            // DMAP_ORDER_*: 0 index order, 1 nearest box entry first
+    int guard_cap = 1 << 26;  // FP32 walk: cells one triangle walk may visit before it gives up
     // When set, the number of rays is read here on the device when the query
     // runs (at most the n the launch is given, which sizes grids and scratch):
     // stages of a device-driven pipeline pass counts they produced themselves.
@@ -80,10 +81,13 @@ int direct_launches(int n_leaf);
 cudaError_t launch_pyramid_direct(const dmapdev::AssetDev &a, double *pyr64, float *pyr32, void *hull_scratch,
                                   cudaStream_t stream, bool all64);
 
-// Per-triangle setup (setup.cu).
-cudaError_t launch_setup(const double *tris_dev, const int *tri_asset_dev, const dmapdev::AssetDev *assets_dev,
-                         int n_tri, dmapdev::TriDev *out, dmapdev::TriDev32 *out32, unsigned *status,
-                         cudaStream_t stream);
+// Per-triangle setup (setup.cu) over records of `stride` doubles: vertex
+// records (kVertexRecord) or BaseTriangle chart records (kChartRecord).
+constexpr int kVertexRecord = 24;
+constexpr int kChartRecord = 37;
+cudaError_t launch_setup(const double *tris_dev, int stride, const int *tri_asset_dev,
+                         const dmapdev::AssetDev *assets_dev, int n_tri, dmapdev::TriDev *out,
+                         dmapdev::TriDev32 *out32, unsigned *status, cudaStream_t stream);
 
 // The FP64 walk, one thread per ray over every triangle (walk64.cu).
 cudaError_t launch_walk64(const dmapdev::TriDev *tris, int n_tri, const dmapdev::AssetDev *assets, const void *rays,

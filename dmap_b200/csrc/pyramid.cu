@@ -1,4 +1,4 @@
-// K1: the Taylor bound pyramid on the device (taylor_pyramid.cpp:154-247,
+// K1: the Taylor bound pyramid on the device (taylor_pyramid.cpp:45-138,
 // leaf_level and fold, the reference's default Fold build).
 //
 // One CTA per tile of T x T leaf cells (T = min(16, 2^L)), one thread per
@@ -24,6 +24,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <mutex>
 
 namespace
 {
@@ -55,7 +56,7 @@ __device__ __forceinline__ double shfl(double v, int lane_mask)
 }
 
 // Fold four children held by lanes {L, L^1, L^2, L^3} of one warp into
-// their parent (taylor_pyramid.cpp:186-247). `b` is the lane's child u bit,
+// their parent (taylor_pyramid.cpp:77-138). `b` is the lane's child u bit,
 // `a` its v bit; s is the parent half-extent. Every lane returns the parent.
 __device__ __forceinline__ Node8 fold4(const Node8 &c, int a, int b, double s)
 {
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(256) pyramid_leaf_kernel(const __grid_constant
     int t = threadIdx.x;
     bool active = t < T * T; // a 1-, 2- or 4-cell tile still runs one full warp
     int x = active ? (int)compact1by1((unsigned)t) : 0, y = active ? (int)compact1by1((unsigned)t >> 1) : 0;
-    // leaf_level (taylor_pyramid.cpp:154-176) on V = values * scale
+    // leaf_level (taylor_pyramid.cpp:45-67) on V = values * scale
     double v00 = to_d(tile[y * box_w + x]) * a.scale, v10 = to_d(tile[y * box_w + x + 1]) * a.scale;
     double v01 = to_d(tile[(y + 1) * box_w + x]) * a.scale, v11 = to_d(tile[(y + 1) * box_w + x + 1]) * a.scale;
     double w = 1.0 / a.n_leaf;
@@ -613,23 +614,64 @@ typedef CUresult (*NoallocEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32
                                     CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
                                     CUtensorMapFloatOOBfill);
 
-// The device address of the scratch array on the current device, looked up
-// once per device with that device current (the host-side symbol is only a
-// stand-in and must never reach a kernel).
+typedef CUresult (*NoallocCtxCurrentFn)(CUcontext *);
+typedef CUresult (*NoallocCtxIdFn)(CUcontext, unsigned long long *);
+
+// The unique id of the calling thread's current context (cuCtxGetId ids are
+// never reused within a process), or false when none is current yet.
+bool noalloc_context_id(unsigned long long &id)
+{
+    static NoallocCtxCurrentFn get_current = nullptr;
+    static NoallocCtxIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<NoallocCtxCurrentFn>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<NoallocCtxIdFn>(fn);
+    });
+    CUcontext ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx)
+        return false;
+    return get_id(ctx, &id) == CUDA_SUCCESS;
+}
+
+// The device address of the scratch array in the calling thread's current
+// context (the host-side symbol is only a stand-in and must never reach a
+// kernel). The address is looked up with cudaGetSymbolAddress the first time
+// a device is used and again whenever that device's context is new (after a
+// cudaDeviceReset, or a primary context released and retained again), so a
+// cached address never outlives its context; a mutex orders the look-ups of
+// concurrent first calls.
 double *noalloc_scratch(int device, cudaError_t &err)
 {
-    static double *addr[64] = {};
+    struct Slot
+    {
+        unsigned long long ctx_id;
+        double *addr;
+    };
+    static std::mutex mu;
+    static Slot slots[64] = {};
     err = cudaSuccess;
     if (device < 0 || device >= 64)
         return nullptr;
-    if (!addr[device]) {
-        double *p = nullptr;
-        err = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
-        if (err != cudaSuccess)
-            return nullptr;
-        addr[device] = p;
-    }
-    return addr[device];
+    std::lock_guard<std::mutex> lock(mu);
+    unsigned long long id = 0;
+    if (noalloc_context_id(id) && slots[device].addr && slots[device].ctx_id == id)
+        return slots[device].addr;
+    double *p = nullptr;
+    err = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+    if (err != cudaSuccess)
+        return nullptr;
+    // the look-up made the device's primary context current if none was
+    if (noalloc_context_id(id))
+        slots[device] = Slot{id, p};
+    return p;
 }
 } // namespace
 

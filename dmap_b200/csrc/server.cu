@@ -101,6 +101,7 @@ struct dmap_server
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
     uint64_t next_id = 1;
     bool stop = false;
+    bool paused = false; // dmap_server_pause: queued requests wait, running ones finish
     std::thread worker;
 
     size_t held = 0, peak = 0, slot_bytes = 0;
@@ -128,6 +129,7 @@ struct dmap_server
         r->status = st;
         r->state = State::Done;
         r->t_done = Clock::now();
+        --r->scene->server_pending;
         if (st == DMAP_OK) {
             ++completed;
             lat_ms.push_back(ms_between(r->t_submit, r->t_done));
@@ -323,7 +325,8 @@ struct dmap_server
                     retire(sl);
                     progressed = true;
                 }
-            admit();
+            if (!paused)
+                admit();
             for (Slot &sl : slots)
                 if (!sl.busy && fill(sl))
                     progressed = true;
@@ -335,7 +338,7 @@ struct dmap_server
             if (busy)
                 cv_work.wait_for(lk, std::chrono::microseconds(100));
             else
-                cv_work.wait(lk, [&] { return stop || !queued.empty(); });
+                cv_work.wait(lk, [&] { return stop || (!paused && !queued.empty()); });
         }
     }
 
@@ -355,6 +358,7 @@ struct dmap_server
         }
         ++submitted;
         *id = r->id;
+        ++r->scene->server_pending;
         queued.push_back(r.get());
         all[r->id] = std::move(r);
         cv_work.notify_one();
@@ -427,6 +431,7 @@ void dmap_server_destroy(dmap_server *S)
         for (Request *r : S->queued) {
             r->state = State::Done;
             r->status = DMAP_ERR_CANCELLED;
+            --r->scene->server_pending;
             ++S->cancelled;
         }
         S->queued.clear();
@@ -539,6 +544,16 @@ dmap_status dmap_server_wait(dmap_server *S, uint64_t id, double timeout_s)
     return r->status;
 }
 
+dmap_status dmap_server_pause(dmap_server *S, int paused)
+{
+    if (!S)
+        return DMAP_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->paused = paused != 0;
+    S->cv_work.notify_all();
+    return DMAP_OK;
+}
+
 dmap_status dmap_server_cancel(dmap_server *S, uint64_t id)
 {
     if (!S)
@@ -552,6 +567,7 @@ dmap_status dmap_server_cancel(dmap_server *S, uint64_t id)
     S->queued.erase(std::find(S->queued.begin(), S->queued.end(), r));
     r->state = State::Done;
     r->status = DMAP_ERR_CANCELLED;
+    --r->scene->server_pending;
     ++S->cancelled;
     S->cv_done.notify_all();
     return DMAP_ERR_CANCELLED;

@@ -1,10 +1,10 @@
 // Per-triangle setup (one thread per base triangle), in double with the
 // reference's operation order (compiled with -fmad=false):
-//   BaseTriangle general-chart constructor   displaced_surface.cpp:406-443
+//   BaseTriangle general-chart constructor   displaced_surface.cpp:54-91
 //   tangent_frame                             node_bounds.cpp:13-23
 //   UvTriangle                                uv_clip.cpp:10-25
 //   footprint_roots                           descent_sampler.cpp:66-83
-//   DisplacedIntersector roots, tolerance     displaced_intersector.cpp:335-351
+//   DisplacedIntersector roots, tolerance     displaced_intersector.cpp:135-151
 //   triangle_height_range (explicit stack)    node_bounds.cpp:218-249
 //   triangle_aabb                             node_bounds.cpp:251-269
 // and the FP32 record derived from it, rounded outward where it bounds.
@@ -53,32 +53,53 @@ __device__ void node_hrange(const AssetDev &a, int level, int64_t i, int64_t j, 
     hi = (double)p[7];
 }
 
-__device__ bool init_triangle(TriDev &T, const double *r)
+// The base triangle's chart. A vertex record (24 doubles: p0 p1 p2 m0 m1 m2
+// t0 t1 t2) runs the general-chart constructor; a chart record (37 doubles:
+// p0 p1 p2, q0 e1 e2, t0 t1 t2, m0 Mu Mv, J row-major) carries a
+// BaseTriangle the caller already built, whose fields are taken as they are.
+__device__ bool init_triangle(TriDev &T, const double *r, bool chart)
 {
-    v3 p0 = L3(r), p1 = L3(r + 3), p2 = L3(r + 6), m0 = L3(r + 9), m1 = L3(r + 12), m2 = L3(r + 15);
+    v3 p0 = L3(r), p1 = L3(r + 3), p2 = L3(r + 6);
     v2 t0 = L2(r + 18), t1 = L2(r + 20), t2 = L2(r + 22);
     T.t0[0] = t0.x, T.t0[1] = t0.y, T.t1[0] = t1.x, T.t1[1] = t1.y, T.t2[0] = t2.x, T.t2[1] = t2.y;
-    v3 eb1 = sub3(p1, p0), eb2 = sub3(p2, p0), Mb1 = sub3(m1, m0), Mb2 = sub3(m2, m0);
+    v3 eb1 = sub3(p1, p0), eb2 = sub3(p2, p0);
     v3 wn = cross3(eb1, eb2); // winding_normal (displaced_surface.cpp:158)
     T.wn[0] = wn.x, T.wn[1] = wn.y, T.wn[2] = wn.z;
     double T00 = t1.x - t0.x, T10 = t1.y - t0.y, T01 = t2.x - t0.x, T11 = t2.y - t0.y;
     double det = T00 * T11 - T10 * T01;
     if (!(fabs(det) > 1e-30))
         return false;
-    double invdet = 1.0 / det;
-    T.J[0][0] = T11 * invdet;
-    T.J[1][0] = -T10 * invdet;
-    T.J[0][1] = -T01 * invdet;
-    T.J[1][1] = T00 * invdet;
-    v2 c = {(-T.J[0][0]) * t0.x + (-T.J[0][1]) * t0.y, (-T.J[1][0]) * t0.x + (-T.J[1][1]) * t0.y};
-    for (int a = 0; a < 3; ++a) {
-        double E0 = comp(eb1, a), E1 = comp(eb2, a), D0 = comp(Mb1, a), D1 = comp(Mb2, a);
-        T.q0[a] = comp(p0, a) + (E0 * c.x + E1 * c.y);
-        T.e1[a] = E0 * T.J[0][0] + E1 * T.J[1][0];
-        T.e2[a] = E0 * T.J[0][1] + E1 * T.J[1][1];
-        T.m0[a] = comp(m0, a) + (D0 * c.x + D1 * c.y);
-        T.Mu[a] = D0 * T.J[0][0] + D1 * T.J[1][0];
-        T.Mv[a] = D0 * T.J[0][1] + D1 * T.J[1][1];
+    if (chart) {
+        for (int a = 0; a < 3; ++a) {
+            T.q0[a] = r[9 + a];
+            T.e1[a] = r[12 + a];
+            T.e2[a] = r[15 + a];
+            T.m0[a] = r[24 + a];
+            T.Mu[a] = r[27 + a];
+            T.Mv[a] = r[30 + a];
+        }
+        T.J[0][0] = r[33];
+        T.J[0][1] = r[34];
+        T.J[1][0] = r[35];
+        T.J[1][1] = r[36];
+    } else {
+        v3 m0 = L3(r + 9), m1 = L3(r + 12), m2 = L3(r + 15);
+        v3 Mb1 = sub3(m1, m0), Mb2 = sub3(m2, m0);
+        double invdet = 1.0 / det;
+        T.J[0][0] = T11 * invdet;
+        T.J[1][0] = -T10 * invdet;
+        T.J[0][1] = -T01 * invdet;
+        T.J[1][1] = T00 * invdet;
+        v2 c = {(-T.J[0][0]) * t0.x + (-T.J[0][1]) * t0.y, (-T.J[1][0]) * t0.x + (-T.J[1][1]) * t0.y};
+        for (int a = 0; a < 3; ++a) {
+            double E0 = comp(eb1, a), E1 = comp(eb2, a), D0 = comp(Mb1, a), D1 = comp(Mb2, a);
+            T.q0[a] = comp(p0, a) + (E0 * c.x + E1 * c.y);
+            T.e1[a] = E0 * T.J[0][0] + E1 * T.J[1][0];
+            T.e2[a] = E0 * T.J[0][1] + E1 * T.J[1][1];
+            T.m0[a] = comp(m0, a) + (D0 * c.x + D1 * c.y);
+            T.Mu[a] = D0 * T.J[0][0] + D1 * T.J[1][0];
+            T.Mv[a] = D0 * T.J[0][1] + D1 * T.J[1][1];
+        }
     }
     // tangent frame: [e1 e2 ng]^-1 by cofactors
     v3 ng = normalized3(cross3(L3(T.e1), L3(T.e2)));
@@ -254,7 +275,7 @@ __device__ void derive32(const TriDev &T, TriDev32 &S)
     S.q22 = (float)dot3(Mv, Mv);
 }
 
-__global__ void setup_kernel(const double *__restrict__ tris, const int *__restrict__ tri_asset,
+__global__ void setup_kernel(const double *__restrict__ tris, int stride, const int *__restrict__ tri_asset,
                              const AssetDev *__restrict__ assets, int n_tri, TriDev *out, TriDev32 *out32,
                              unsigned *status)
 {
@@ -264,7 +285,7 @@ __global__ void setup_kernel(const double *__restrict__ tris, const int *__restr
     TriDev T;
     T.asset = tri_asset[k];
     T.status = 0;
-    if (!init_triangle(T, tris + 24 * (size_t)k)) {
+    if (!init_triangle(T, tris + stride * (size_t)k, stride == dmapk::kChartRecord)) {
         T.status = 1;
         atomicOr(status, dmapdev::kStatusBadInput);
         out[k] = T;
@@ -281,13 +302,14 @@ __global__ void setup_kernel(const double *__restrict__ tris, const int *__restr
 
 namespace dmapk
 {
-cudaError_t launch_setup(const double *tris_dev, const int *tri_asset_dev, const dmapdev::AssetDev *assets_dev,
-                         int n_tri, dmapdev::TriDev *out, dmapdev::TriDev32 *out32, unsigned *status,
-                         cudaStream_t stream)
+cudaError_t launch_setup(const double *tris_dev, int stride, const int *tri_asset_dev,
+                         const dmapdev::AssetDev *assets_dev, int n_tri, dmapdev::TriDev *out,
+                         dmapdev::TriDev32 *out32, unsigned *status, cudaStream_t stream)
 {
     int threads = 64;
     int blocks = (n_tri + threads - 1) / threads;
-    setup_kernel<<<blocks, threads, 0, stream>>>(tris_dev, tri_asset_dev, assets_dev, n_tri, out, out32, status);
+    setup_kernel<<<blocks, threads, 0, stream>>>(tris_dev, stride, tri_asset_dev, assets_dev, n_tri, out, out32,
+                                                 status);
     return cudaGetLastError();
 }
 } // namespace dmapk

@@ -176,7 +176,7 @@ __device__ __forceinline__ float far_bound(float t1) { return ru_add(ru_mul(t1, 
 // DisplacedIntersector::intersect with the FP32 node test.
 __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const AssetDev &g, const double *o,
                                 const double *d, double t_min, double &t_max, const dmapk::QueryOpts &opt,
-                                d64::hit64 &hit, int64_t *st, float t_far, unsigned *status)
+                                d64::hit64 &hit, int64_t *st, float t_far, unsigned *status, bool &capped)
 {
     Ray32 r;
     tangent_ray(T, o, d, t_far, r);
@@ -190,8 +190,9 @@ __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const Asse
         cell_next(end, si, sj, T.root_level);
         int guard = 0;
         while (!(cur.level == end.level && cur.i == end.i && cur.j == end.j)) {
-            if (++guard > (1 << 26)) { // a finite tree: the cap only guards corrupt records
+            if (++guard > opt.guard_cap) { // a finite tree: the cap guards corrupt records
                 atomicOr(status, dmapdev::kStatusCapped);
+                capped = true;
                 break;
             }
             float w = pow2f(cur.level - log2n);
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
     int64_t *sp = stats ? st : nullptr;
     d64::hit64 best;
     int best_tri = -1;
-    bool found = false;
+    bool found = false, capped = false;
     // the next triangle: index order, or (nearest) the smallest (key, index)
     // past the cursor among the candidates the ray still reaches
     double inv[3], ckey = -INFINITY;
@@ -300,7 +301,8 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
         double t_lo = t_min;
         for (int pass = 0; pass < (opt.op_mask ? dmapdev::kFilterPasses : 1); ++pass) {
             double tm = t_max;
-            if (!triangle_walk32(T, tris64[t], assets[T.asset], o, d, t_lo, tm, opt, h, sp, far_bound(t1), status))
+            if (!triangle_walk32(T, tris64[t], assets[T.asset], o, d, t_lo, tm, opt, h, sp, far_bound(t1), status,
+                                 capped))
                 break;
             if (dmapdev::crossing_opaque(opt, tris64[t], t, h.bary.x, h.bary.y)) {
                 got = true;
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
                 break;
         }
     }
-    store_hit<H, Fp>(hits, k, found, best, best_tri, found ? DMAP_HIT_FP64_LEAF : 0);
+    store_hit<H, Fp>(hits, k, found, best, best_tri, (found ? DMAP_HIT_FP64_LEAF : 0) | (capped ? DMAP_HIT_CAPPED : 0));
     if (stats)
         for (int q = 0; q < DMAP_ST_N; ++q)
             stats[DMAP_ST_N * k + q] = st[q];
@@ -358,6 +360,7 @@ struct LeafJob
 // RayState.flags
 constexpr int kFoundInTri = 1; // a hit was taken in the triangle in progress
 constexpr int kResumeHere = 2; // parked before visiting cell `cur` (or at the walk's end): resume without cell_next
+constexpr int kCapped = 4;     // a triangle walk of this ray ran out of its cell-visit cap (DMAP_HIT_CAPPED)
 
 // Counter slots of one round: the walk's fetch counter, the leaf queue's
 // length, the leaf kernel's fetch counter, the resume queue's length.
@@ -829,7 +832,9 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
             if (!hit_box) {
                 if (best_tri < 0) {
                     d64::hit64 none;
-                    store_hit<H, Fp>(hits, ray, false, none, -1, 0);
+                    store_hit<H, Fp>(hits, ray, false, none, -1, (flags & kCapped) ? DMAP_HIT_CAPPED : 0);
+                } else if (flags & kCapped) {
+                    hits[ray].flags |= DMAP_HIT_CAPPED; // the stored hit is final: this lane owns the ray
                 }
                 flush_stats();
                 phase = NEED;
@@ -878,8 +883,9 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     phase = TOP;
                     break;
                 }
-                if (++guard > (1 << 26)) { // a finite tree: the cap only guards corrupt records
+                if (++guard > opt.guard_cap) { // a finite tree: the cap guards corrupt records
                     atomicOr(status, dmapdev::kStatusCapped);
+                    flags |= kCapped;
                     ++tri;
                     phase = TOP;
                     break;
@@ -924,7 +930,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                         best_tri = tri;
                         flags |= kFoundInTri;
                         nah = lah = 0;
-                        store_hit<H, Fp>(hits, ray, true, lh, tri, DMAP_HIT_FP64_LEAF);
+                        store_hit<H, Fp>(hits, ray, true, lh, tri,
+                                         DMAP_HIT_FP64_LEAF | ((flags & kCapped) ? DMAP_HIT_CAPPED : 0));
                         if (opt.mode == 1) {
                             flush_stats();
                             phase = NEED;
@@ -1158,7 +1165,8 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
                 s.best_tri = tri;
                 s.flags |= kFoundInTri;
                 s.nah = s.lah = 0;
-                store_hit<H, Fp>(hits, ray, true, h, tri, DMAP_HIT_FP64_LEAF);
+                store_hit<H, Fp>(hits, ray, true, h, tri,
+                                 DMAP_HIT_FP64_LEAF | ((s.flags & kCapped) ? DMAP_HIT_CAPPED : 0));
                 if (opt.mode == 1) { // occlusion: any hit answers the query
                     answered = true;
                     sp = 0;

@@ -1,6 +1,6 @@
 // The FP64 query path: one thread per ray, every triangle of the scene in
 // order behind its AABB (ObjectIntersector::intersect_flat,
-// displaced_intersector.cpp:778-799), each walked with TFDM's stackless
+// displaced_intersector.cpp:578-599), each walked with TFDM's stackless
 // quadtree walk and the certified Newton leaf
 // (displaced_intersector.cpp:175-388, node_bounds.cpp:83-211), in double
 // with the reference's operation order (compiled with -fmad=false). This is
@@ -130,10 +130,12 @@ template <typename R>
 __device__ __forceinline__ void load_ray(const R *rays, int64_t k, v3 &o, v3 &d, double &t_min, double &t_max)
 {
     const R *r = rays + 8 * k;
-    o = {(double)r[0], (double)r[1], (double)r[2]};
-    d = {(double)r[3], (double)r[4], (double)r[5]};
+    double oo[3] = {(double)r[0], (double)r[1], (double)r[2]}, dd[3] = {(double)r[3], (double)r[4], (double)r[5]};
     t_min = (double)r[6];
     t_max = (double)r[7];
+    dmapdev::sanitize_ray(oo, dd, t_min, t_max);
+    o = {oo[0], oo[1], oo[2]};
+    d = {dd[0], dd[1], dd[2]};
 }
 
 template <typename H, typename F>

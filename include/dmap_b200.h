@@ -27,7 +27,7 @@ typedef enum dmap_status {
     DMAP_ERR_INVALID = 1,     /* bad argument (the reference ASSERTs instead) */
     DMAP_ERR_CUDA = 2,        /* a CUDA call failed; dmap_last_error() has the text */
     DMAP_ERR_OOM = 3,         /* device allocation failed */
-    DMAP_ERR_DEGENERATE = 4,  /* a base triangle is degenerate in texture space (displaced_surface.cpp:419) */
+    DMAP_ERR_DEGENERATE = 4,  /* a base triangle is degenerate in texture space (displaced_surface.cpp:67) */
     DMAP_ERR_BUDGET = 5,      /* the request does not fit the server's memory budget */
     DMAP_ERR_LIMIT = 6,       /* an iteration cap ran out on the device; results are flagged */
     DMAP_ERR_NOT_READY = 7,   /* a served request has not finished */
@@ -68,7 +68,7 @@ int64_t dmap_kernel_launches(const dmap_context *ctx);
  * Taylor bound pyramid on the device: h = scale * value + offset, texture
  * coordinates wrapping when `repeat`, clamping otherwise.
  * Replaces DisplacementAsset's grid + TaylorPyramid(const HeightGrid &, PyramidBuild::Fold)
- * (displacement_asset.cpp:16-35, taylor_pyramid.h:89-92, taylor_pyramid.cpp:324-366).
+ * (displacement_asset.cpp:16-35, taylor_pyramid.h:89-92, taylor_pyramid.cpp:215-257).
  * `values_host` is host memory of `dtype` (F32, F16, BF16 or F64).
  */
 dmap_status dmap_asset_create(dmap_context *ctx, const void *values_host, dmap_dtype dtype, int nodes, double scale,
@@ -105,10 +105,15 @@ dmap_status dmap_asset_pyramid_level(const dmap_asset *asset, int level, int pre
  * The FP64 working levels live in a fixed device array of the library (22.4
  * MB per GPU that loads it, held until exit), so maps are limited to
  * 2^L <= 512 texels per side; larger ones return DMAP_ERR_INVALID. The first
- * call on each device looks up that array's device address; make it before
- * any stream capture. Runs on `stream` (a cudaStream_t, NULL = the legacy
- * default stream) and returns when the pyramid is written. Calls share the
- * array: calls that overlap on the GPU race, so serialize them.
+ * call on each device (and the first after that device's context was
+ * recreated) looks up the array's device address. Under lazy module loading
+ * (CUDA's default) that look-up loads the library's device code and commits
+ * the array, so that first call can itself take device memory: make it at
+ * start-up, before any frame and before any stream capture (a call on a 3 x 3
+ * node grid is enough). Later calls allocate nothing. Runs on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream) and returns when the
+ * pyramid is written. Calls share the array, which keeps the last call's
+ * contents: calls that overlap on the GPU race, so serialize them.
  */
 dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dtype dtype, int nodes, int pitch, double scale,
                                        double offset, int repeat, float *pyr32_dev, void *stream);
@@ -121,12 +126,25 @@ dmap_status dmap_pyramid_build_noalloc(const void *nodes_dev, dmap_dtype dtype, 
  * AABB. tris_host: n_tri x 24 doubles (p0, p1, p2, m0, m1, m2 as xyz; t0,
  * t1, t2 as texture uv), tri_asset[k] indexes `assets`.
  * Replaces ObjectIntersector(const std::vector<BaseTriangle> &, const TaylorPyramid &,
- * const HeightGrid &) (displaced_intersector.h:183-184, displaced_intersector.cpp:666-679)
- * with the BaseTriangle general-chart constructor (displaced_surface.h:296-298).
+ * const HeightGrid &) (displaced_intersector.h:183-184, displaced_intersector.cpp:466-479)
+ * with the BaseTriangle general-chart constructor (displaced_surface.h:79-81).
  * A scene borrows its assets: destroy the scene first.
  */
 dmap_status dmap_scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset_host,
                               const double *tris_host, int n_tri, dmap_scene **out);
+/*
+ * The same scene from BaseTriangles the caller already built (the
+ * reference's own objects, displaced_surface.h:63-95): n_tri x 37 doubles
+ * per triangle, p0 p1 p2 (positions), q0 e1 e2 (the chart's P), t0 t1 t2
+ * (texture uv), m0 Mu Mv (the chart's M), J (2 x 2, row major), taken as
+ * they are instead of rebuilt from vertex normals, so a drop-in over
+ * ObjectIntersector(const std::vector<BaseTriangle> &, ...) sees exactly
+ * the triangles the reference walks. Replaces the same constructor as
+ * dmap_scene_create (displaced_intersector.cpp:466-479).
+ */
+dmap_status dmap_scene_create_charts(dmap_context *ctx, dmap_asset *const *assets, int n_assets,
+                                     const int *tri_asset_host, const double *charts_host, int n_tri,
+                                     dmap_scene **out);
 /*
  * Scene-level instancing: the reference's scene objects placed by their
  * to_world transforms as embree instances (displaced_scene.cpp:79-87,
@@ -153,13 +171,13 @@ int dmap_scene_triangle_count(const dmap_scene *scene);
  * Per-triangle setup results (11 doubles: root_level, n_roots,
  * residual_tolerance, aabb lo xyz, aabb hi xyz, h_min, h_max), the fields
  * DisplacedIntersector's constructor and triangle_aabb produce
- * (displaced_intersector.cpp:335-351, node_bounds.cpp:347-378).
+ * (displaced_intersector.cpp:135-151, node_bounds.cpp:238-269).
  */
 dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *out11);
 
 /* ---- queries ------------------------------------------------------------ */
 
-/* TraversalOptions (traversal_options.h:600-608) plus the device choices. */
+/* TraversalOptions (traversal_options.h:30-38) plus the device choices. */
 #define DMAP_BOUND_BOX 0
 #define DMAP_BOUND_SLAB 1
 #define DMAP_BOUND_BOTH 2
@@ -205,6 +223,10 @@ typedef struct dmap_options {
                            default 6; 0 = one walk with every leaf inline) */
     int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 5, at most 5 resident) */
     int order;          /* DMAP_ORDER_*, default NEAREST */
+    int node_visit_cap; /* FP32 path: cells one triangle's walk may visit before it gives up (0 = the default,
+                           2^26, far above any walk of a well-formed scene). A ray whose walk gives up keeps
+                           what it found, its hit record gets DMAP_HIT_CAPPED, and the call reports
+                           DMAP_ERR_LIMIT */
 } dmap_options;
 
 /* Fills the defaults above. */
@@ -284,7 +306,7 @@ dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, d
  * (displaced_geometry.cpp:53-106). The crossing a triangle's walk returns
  * goes to the filter; a crossing it rejects is skipped and the triangle is
  * walked again from t_min = that crossing's t, at most 64 times
- * (max_filter_passes, displaced_geometry.h:62); an occlusion query takes
+ * (max_filter_passes, displaced_geometry.h:64); an occlusion query takes
  * the nearest crossing of each triangle for the filter to judge. The
  * filter: the crossing's texture coordinate (compute_hit_texcoord,
  * displaced_geometry.cpp:189-193: the float barycentrics the filter sees,
@@ -297,7 +319,10 @@ dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, d
  * Queries on a filtered scene run the one-thread-per-ray schedules
  * (DMAP_PRECISION_F64, or DMAP_PRECISION_F32 with DMAP_SCHEDULE_SIMPLE);
  * the wavefront schedule, dmap_render and the server return
- * DMAP_ERR_UNSUPPORTED for it.
+ * DMAP_ERR_UNSUPPORTED for it. While a server holds requests on the scene
+ * (queued or running), the filter cannot change: this call returns
+ * DMAP_ERR_NOT_READY until they are done (dmap_server_drain); do not call it
+ * concurrently with a submit on the same scene.
  */
 dmap_status dmap_scene_set_opacity(dmap_scene *scene, const uint8_t *mask_host, int w, int h, const dmap_uv_map *map,
                                    const uint8_t *tri_flags_host);
@@ -326,7 +351,7 @@ dmap_status dmap_tessellate_uniform_host(dmap_scene *scene, int n, float *vertic
 
 /*
  * The texel-aligned tessellation (append_texel_tessellation,
- * displaced_tessellation.cpp:97-137) over the scene's triangles in order:
+ * displaced_tessellation.cpp:101-136) over the scene's triangles in order:
  * every leaf cell meeting a triangle's uv domain split into m x m sub-cells,
  * each inside sub-cell into two faces along the (1,0)-(0,1) diagonal and each
  * straddling one into the fan of its clipped polygon; faces keep the base
@@ -394,7 +419,7 @@ typedef struct dmap_emitter_point {
 dmap_status dmap_emitter_sample(dmap_emitter *emitter, const int32_t *tri_dev, const float *uniforms_dev,
                                 int uniforms_per_sample, const double *receivers_dev, int64_t n,
                                 dmap_emitter_point *out_dev, void *stream);
-/* DescentSampler::pdf_uv / pdf_area (descent_sampler.cpp:344-362) at n
+/* DescentSampler::pdf_uv / pdf_area (descent_sampler.cpp:346-364) at n
  * points (uv_dev: 2 doubles each) of triangles tri_dev; pdf_area_dev may be
  * NULL. The re-walk equals the sampled pdf at sampled points. */
 dmap_status dmap_emitter_pdf(dmap_emitter *emitter, const int32_t *tri_dev, const double *uv_dev,
@@ -543,6 +568,13 @@ dmap_status dmap_server_submit_render(dmap_server *srv, dmap_scene *scene, const
 dmap_status dmap_server_poll(dmap_server *srv, uint64_t id);
 /* Blocks until the request completes or timeout_s passes (< 0: no limit). */
 dmap_status dmap_server_wait(dmap_server *srv, uint64_t id, double timeout_s);
+/*
+ * Holds (paused != 0) or resumes admission: while held, submitted requests
+ * stay queued (cancellable) and admitted ones run to completion. A drain
+ * while held waits for queued requests until its timeout. No reference
+ * counterpart (serving).
+ */
+dmap_status dmap_server_pause(dmap_server *srv, int paused);
 /* Cancels a request that is still queued (DMAP_ERR_NOT_READY once it runs). */
 dmap_status dmap_server_cancel(dmap_server *srv, uint64_t id);
 /* Latency in ms of a completed request (submit to completion). */

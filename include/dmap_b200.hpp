@@ -8,7 +8,7 @@
 //                                 hit, triangle, stats) call, plus intersect_batch
 //   dmapgpu::TraversalOptions, DisplacedHit, TraversalStats
 //                               ~ the reference's structs of the same names
-//                                 (traversal_options.h:600-608,
+//                                 (traversal_options.h:30-38,
 //                                 displaced_intersector.h:89-114)
 //
 // Header-only; link libdmap_b200.so. Vectors are std::array<double, 3>, so

@@ -103,15 +103,15 @@ static inline ivl af_interval(af f) /* affine_form.h:50-54 */
     ivl r = {f.c - e, f.c + e};
     return r;
 }
-static inline af af_add(af x, af y) /* affine_form.cpp:126-133 */
+static inline af af_add(af x, af y) /* affine_form.cpp:17-24 */
 {
     return AF(x.c + y.c, x.a + y.a, x.b + y.b, x.k + y.k);
 }
-static inline af af_scale(double s, af x) /* affine_form.cpp:158-165 */
+static inline af af_scale(double s, af x) /* affine_form.cpp:49-56 */
 {
     return AF(x.c * s, x.a * s, x.b * s, x.k * fabs(s));
 }
-static inline af af_mul(af x, af r) /* affine_form.cpp:146-156 */
+static inline af af_mul(af x, af r) /* affine_form.cpp:35-47 */
 {
     double u = (fabs(x.a) + fabs(x.b)) + x.k;
     double v = (fabs(r.a) + fabs(r.b)) + r.k;
@@ -124,7 +124,7 @@ static inline af af_mul(af x, af r) /* affine_form.cpp:146-156 */
     return o;
 }
 static inline double g_rsqrt(double x) { return 1.0 / sqrt(x); }
-static af af_rsqrt(af f) /* affine_form.cpp:173-185, Min-Range */
+static af af_rsqrt(af f) /* affine_form.cpp:64-76, Min-Range */
 {
     ivl range = af_interval(f);
     double lo = range.lo, hi = range.hi;
@@ -139,7 +139,7 @@ static inline af3 AF3(v3 c, v3 a, v3 b)
     return r;
 }
 static inline af *af3_comp(af3 *v, int k) { return k == 0 ? &v->x : k == 1 ? &v->y : &v->z; }
-static af af3_sq_length(const af3 *v) /* affine_form.cpp:187-194 */
+static af af3_sq_length(const af3 *v) /* affine_form.cpp:78-85 */
 {
     v3 xc = V3(v->x.c, v->y.c, v->z.c), xu = V3(v->x.a, v->y.a, v->z.a);
     v3 xv = V3(v->x.b, v->y.b, v->z.b), xk = V3(v->x.k, v->y.k, v->z.k);
@@ -148,7 +148,7 @@ static af af3_sq_length(const af3 *v) /* affine_form.cpp:187-194 */
     double offset = 0.5 * dot3(dev, dev);
     return AF(dot3(xc, xc) + offset, 2.0 * dot3(xc, xu), 2.0 * dot3(xc, xv), 2.0 * fabs(dot3(xc, xk)) + offset);
 }
-static void af3_normalize(af3 *v) /* affine_form.cpp:196-204 */
+static void af3_normalize(af3 *v) /* affine_form.cpp:87-95 */
 {
     af l = af3_sq_length(v);
     if (af_interval(l).lo <= 0.0) {
@@ -160,16 +160,16 @@ static void af3_normalize(af3 *v) /* affine_form.cpp:196-204 */
     v->y = af_mul(r, v->y);
     v->z = af_mul(r, v->z);
 }
-static inline af3 af3_add(af3 a, af3 b) /* affine_form.cpp:206 */
+static inline af3 af3_add(af3 a, af3 b) /* affine_form.cpp:97 */
 {
     af3 r = {af_add(a.x, b.x), af_add(a.y, b.y), af_add(a.z, b.z)};
     return r;
 }
-static inline af af_dot(v3 a, af3 b) /* affine_form.cpp:210 */
+static inline af af_dot(v3 a, af3 b) /* affine_form.cpp:101 */
 {
     return af_add(af_add(af_scale(a.x, b.x), af_scale(a.y, b.y)), af_scale(a.z, b.z));
 }
-static inline af3 af3_matmul(const m3 *A, af3 v) /* affine_form.cpp:212-215 */
+static inline af3 af3_matmul(const m3 *A, af3 v) /* affine_form.cpp:103-106 */
 {
     af3 r;
     r.x = af_dot(V3(A->m[0][0], A->m[0][1], A->m[0][2]), v);
@@ -206,7 +206,7 @@ static void level_alloc(o_level *l, int m)
         l->ch[c] = (double *)calloc((size_t)m * m, sizeof(double));
 }
 
-static void leaf_level(o_level *out, const double *V, int nodes, int n_leaf) /* taylor_pyramid.cpp:154-176 */
+static void leaf_level(o_level *out, const double *V, int nodes, int n_leaf) /* taylor_pyramid.cpp:45-67 */
 {
     level_alloc(out, n_leaf);
     double w = 1.0 / n_leaf;
@@ -229,7 +229,7 @@ static void leaf_level(o_level *out, const double *V, int nodes, int n_leaf) /* 
     }
 }
 
-static void fold_level(o_level *out, const o_level *child) /* taylor_pyramid.cpp:186-247 */
+static void fold_level(o_level *out, const o_level *child) /* taylor_pyramid.cpp:77-138 */
 {
     int m = child->m / 2;
     level_alloc(out, m);
@@ -283,7 +283,7 @@ static void fold_level(o_level *out, const o_level *child) /* taylor_pyramid.cpp
     }
 }
 
-/* taylor_pyramid.cpp:129-148 and :260-310 (the direct construction). */
+/* taylor_pyramid.cpp:20-43 and :151-202 (the direct construction). */
 static void direct_level(o_level *out, const double *V, int nodes, int n_leaf, int level)
 {
     int k = 1 << level;
@@ -339,7 +339,7 @@ static void direct_level(o_level *out, const double *V, int nodes, int n_leaf, i
 
 o_pyramid *o_pyramid_build(const double *values, int nodes, double scale, double offset, int build)
 {
-    /* taylor_pyramid.cpp:324-360 */
+    /* taylor_pyramid.cpp:215-251 */
     int n = nodes - 1;
     if (!(n >= 1 && (n & (n - 1)) == 0))
         return NULL;
@@ -398,7 +398,7 @@ void o_pyramid_level(const o_pyramid *p, int level, double *out)
 
 typedef struct { double h0, gu, gv, r, ru, rv, h_min, h_max; } o_node;
 
-static o_node pyramid_node(const o_pyramid *p, int level, int64_t i, int64_t j) /* taylor_pyramid.cpp:368-383 */
+static o_node pyramid_node(const o_pyramid *p, int level, int64_t i, int64_t j) /* taylor_pyramid.cpp:259-274 */
 {
     o_node n;
     if (level >= p->n_levels) {
@@ -459,7 +459,7 @@ static inline double grid_value(const o_grid *g, int j, int i) { return g->value
 
 static void grid_cell(const o_grid *g, double x, double y, int *i, int *j, double *s, double *t)
 {
-    /* displaced_surface.cpp:364-379 */
+    /* displaced_surface.cpp:12-27 */
     if (g->repeat) {
         x -= floor(x);
         y -= floor(y);
@@ -476,7 +476,7 @@ static void grid_cell(const o_grid *g, double x, double y, int *i, int *j, doubl
     *t = fy - *j;
 }
 
-static double grid_h(const o_grid *g, double x, double y) /* displaced_surface.cpp:381-389 */
+static double grid_h(const o_grid *g, double x, double y) /* displaced_surface.cpp:29-37 */
 {
     int i, j;
     double s, t;
@@ -487,7 +487,7 @@ static double grid_h(const o_grid *g, double x, double y) /* displaced_surface.c
            g->offset;
 }
 
-static v2 grid_grad(const o_grid *g, double x, double y) /* displaced_surface.cpp:391-399 */
+static v2 grid_grad(const o_grid *g, double x, double y) /* displaced_surface.cpp:39-47 */
 {
     int i, j;
     double s, t;
@@ -506,7 +506,7 @@ typedef struct {
     double J[2][2];
 } o_tri;
 
-static int tri_init(o_tri *T, const double *r) /* displaced_surface.cpp:406-443 */
+static int tri_init(o_tri *T, const double *r) /* displaced_surface.cpp:54-91 */
 {
     v3 p0 = V3(r[0], r[1], r[2]), p1 = V3(r[3], r[4], r[5]), p2 = V3(r[6], r[7], r[8]);
     v3 m0 = V3(r[9], r[10], r[11]), m1 = V3(r[12], r[13], r[14]), m2 = V3(r[15], r[16], r[17]);
@@ -543,27 +543,27 @@ static int tri_init(o_tri *T, const double *r) /* displaced_surface.cpp:406-443 
     return 1;
 }
 
-static inline v3 tri_P(const o_tri *T, double s, double t) /* displaced_surface.h:300 */
+static inline v3 tri_P(const o_tri *T, double s, double t) /* displaced_surface.h:83 */
 {
     return add3(add3(T->q0, mul3(s, T->e1)), mul3(t, T->e2));
 }
-static inline v3 tri_M(const o_tri *T, double s, double t) /* displaced_surface.h:301 */
+static inline v3 tri_M(const o_tri *T, double s, double t) /* displaced_surface.h:84 */
 {
     return add3(add3(T->m0, mul3(s, T->Mu)), mul3(t, T->Mv));
 }
-static inline v2 tri_bary(const o_tri *T, double s, double t) /* displaced_surface.h:303 */
+static inline v2 tri_bary(const o_tri *T, double s, double t) /* displaced_surface.h:86 */
 {
     double x = s - T->t0.x, y = t - T->t0.y;
     return V2(T->J[0][0] * x + T->J[0][1] * y, T->J[1][0] * x + T->J[1][1] * y);
 }
-static inline v2 tri_param(const o_tri *T, double u, double v) /* displaced_surface.h:304 */
+static inline v2 tri_param(const o_tri *T, double u, double v) /* displaced_surface.h:87 */
 {
     return add2(add2(T->t0, mul2(u, sub2(T->t1, T->t0))), mul2(v, sub2(T->t2, T->t0)));
 }
 
 typedef struct { v3 N, Nu, Nv; } o_nframe;
 
-static o_nframe normal_frame_at(const o_tri *T, double s, double t) /* displaced_surface.cpp:451-460 */
+static o_nframe normal_frame_at(const o_tri *T, double s, double t) /* displaced_surface.cpp:99-108 */
 {
     v3 M = tri_M(T, s, t);
     double Mlen = norm3(M);
@@ -574,13 +574,13 @@ static o_nframe normal_frame_at(const o_tri *T, double s, double t) /* displaced
     return f;
 }
 
-static v3 displaced_position(const o_tri *T, const o_grid *g, double s, double t) /* displaced_surface.cpp:514-518 */
+static v3 displaced_position(const o_tri *T, const o_grid *g, double s, double t) /* displaced_surface.cpp:162-166 */
 {
     o_nframe f = normal_frame_at(T, s, t);
     return add3(tri_P(T, s, t), mul3(grid_h(g, s, t), f.N));
 }
 
-static double mean_edge(const o_tri *T) /* displaced_surface.cpp:520-523 */
+static double mean_edge(const o_tri *T) /* displaced_surface.cpp:168-171 */
 {
     return ((norm3(sub3(T->p1, T->p0)) + norm3(sub3(T->p2, T->p0))) + norm3(sub3(T->p2, T->p1))) / 3.0;
 }
@@ -614,7 +614,7 @@ static void uvtri_init(o_uvtri *U, v2 t0, v2 t1, v2 t2) /* uv_clip.cpp:10-25 */
     U->hi = max2(max2(t0, t1), t2);
 }
 
-static inline int uvtri_inside(const o_uvtri *U, v2 p) /* uv_clip.h:409-415 */
+static inline int uvtri_inside(const o_uvtri *U, v2 p) /* uv_clip.h:28-34 */
 {
     for (int k = 0; k < 3; ++k)
         if (dot2(U->n[k], p) < U->d[k])
@@ -752,7 +752,7 @@ static void node_bound(o_nodebound *nb, const o_tri *T, const o_frame *F, const 
     v2 c = mul2(0.5, add2(rect_lo, rect_hi));
     v2 hh = mul2(0.5, sub2(rect_hi, rect_lo));
     v2 half = V2(dmax(hh.x, 0.0), dmax(hh.y, 0.0));
-    /* normal_form, node_bounds.cpp:66-69 */
+    /* normal_form, node_bounds.cpp:65-68 */
     af3 N = AF3(add3(add3(T->m0, mul3(c.x, T->Mu)), mul3(c.y, T->Mv)), mul3(half.x, T->Mu), mul3(half.y, T->Mv));
     af3_normalize(&N);
     nb->m = af3_matmul(&F->to_tangent, N);
@@ -764,7 +764,7 @@ static void node_bound(o_nodebound *nb, const o_tri *T, const o_frame *F, const 
 static inline ivl IV(double lo, double hi) { ivl r = {lo, hi}; return r; }
 static inline ivl iv_add(ivl a, ivl b) { return IV(a.lo + b.lo, a.hi + b.hi); }
 static inline ivl iv_adds(ivl a, double b) { return IV(a.lo + b, a.hi + b); }
-static inline ivl iv_scale(double s, ivl a) /* affine_form.cpp:121-124 */
+static inline ivl iv_scale(double s, ivl a) /* affine_form.cpp:12-15 */
 {
     return s >= 0.0 ? IV(s * a.lo, s * a.hi) : IV(s * a.hi, s * a.lo);
 }
@@ -1417,7 +1417,7 @@ int o_scene_add_object(o_scene *s, const double *values, int W, double scale, do
             return -1;
         }
     }
-    for (int k = 0; k < n_tri; ++k) { /* displaced_intersector.cpp:666-679 */
+    for (int k = 0; k < n_tri; ++k) { /* displaced_intersector.cpp:466-479 */
         o_isect *X = &O->isects[k];
         isect_init(X, &O->tris[k], O->pyr, O->grid);
         triangle_height_range(&O->tris[k], O->pyr, &X->h_min, &X->h_max);
@@ -1526,7 +1526,7 @@ static double entry_key(const o_box *B, v3 o, v3 d, const double *inv, double t_
  * behind embree's filter functions, reduced to a binary texel mask): the
  * crossing's texture coordinate as compute_hit_texcoord forms it
  * (displaced_geometry.cpp:189-193) from the float barycentrics of
- * potential_hit (:21-34), BaseTriangle::param (displaced_surface.h:88) and
+ * potential_hit (:21-34), BaseTriangle::param (displaced_surface.h:87) and
  * DisplacedObject::object_uv (scene_spec.cpp:382-388) rounded to float,
  * then the mask texel under it with repeat; 0 rejects. */
 static int crossing_opaque(const o_scene *s, const o_tri *T, int g, const o_hit *h)
@@ -1552,7 +1552,7 @@ static int crossing_opaque(const o_scene *s, const o_tri *T, int g, const o_hit 
 
 /* The intersect / occluded callback's passes (displaced_geometry.cpp:53-106):
  * a crossing the filter rejects raises t_min to its t and the triangle is
- * walked again, at most max_filter_passes = 64 times (displaced_geometry.h:62). */
+ * walked again, at most max_filter_passes = 64 times (displaced_geometry.h:64). */
 static int isect_filtered(const o_scene *s, const o_isect *X, int g, v3 o, v3 d, double t_min, double t_max,
                           int bound, int slab_max_level, int leaf, o_hit *h, int64_t *st, int64_t *level_stats)
 {
@@ -1569,7 +1569,7 @@ static int isect_filtered(const o_scene *s, const o_isect *X, int g, v3 o, v3 d,
     return 0;
 }
 
-/* The flat loop of ObjectIntersector::intersect_flat (:778-799) over every
+/* The flat loop of ObjectIntersector::intersect_flat (:578-599) over every
  * object (order O_ORDER_INDEX); or (O_ORDER_NEAREST) the same loop over the
  * triangles whose boxes the ray meets, sorted by (key, index), each still
  * box-tested with the t_max of the ones before it. cand: n_tri scratch. */
@@ -1892,7 +1892,7 @@ typedef struct {
     v2 p[8];
 } o_clip;
 
-/* clip_square (uv_clip.cpp:61-90): Sutherland-Hodgman of the square (c, s)
+/* clip_square (uv_clip.cpp:56-83): Sutherland-Hodgman of the square (c, s)
  * against the domain's three inward half-planes. */
 static o_clip clip_square(const o_uvtri *U, v2 c, double s)
 {
@@ -1931,7 +1931,7 @@ typedef struct {
     int *interior;
 } o_texel_out;
 
-/* append_face / append_vertex (displaced_tessellation.cpp:60-95): three
+/* append_face / append_vertex (displaced_tessellation.cpp:61-99): three
  * unshared vertices per face, the normal oriented along the base face's
  * winding, b and c swapped under a mirrored chart. */
 static void texel_face(o_texel_out *o, v2 a, v2 b, v2 c, int interior)
@@ -1962,7 +1962,7 @@ static void texel_face(o_texel_out *o, v2 a, v2 b, v2 c, int interior)
 int64_t o_tessellate_texel(const o_scene *s, int tri, int m, int64_t cap, float *pos, float *uv, float *nrm,
                            double *st6, int *interior)
 {
-    /* append_texel_tessellation (displaced_tessellation.cpp:97-137) */
+    /* append_texel_tessellation (displaced_tessellation.cpp:101-136) */
     const o_isect *X = find_tri(s, tri, NULL);
     const o_uvtri *U = &X->domain;
     o_texel_out o = {X, chart_mirrored(X->tri), 0, cap, pos, uv, nrm, st6, interior};
@@ -2050,7 +2050,7 @@ static int64_t wrap_index(int64_t i, int m)
     return r < 0 ? r + m : r;
 }
 
-static double tile_mean(const o_tile *E, int level, int64_t i, int64_t j) /* emission_tile.cpp:91-110 */
+static double tile_mean(const o_tile *E, int level, int64_t i, int64_t j) /* emission_tile.cpp:99-118 */
 {
     if (level >= E->n_levels)
         return E->mean[E->n_levels - 1][0];
@@ -2064,7 +2064,7 @@ static double tile_sum(const o_tile *E, int level, int64_t i, int64_t j) /* emis
     return tile_mean(E, level, i, j) * (w * w);
 }
 
-/* FootprintChild / FootprintNode (descent_sampler.h:67-80). */
+/* FootprintChild / FootprintNode (descent_sampler.h:71-84). */
 typedef struct {
     int overlap;
     double area, mass;
@@ -2090,7 +2090,7 @@ struct o_emitter {
     double total_area, total_mass;
 };
 
-static double clip_area(const o_clip *P) /* uv_clip.cpp:51-59 */
+static double clip_area(const o_clip *P) /* uv_clip.cpp:46-54 */
 {
     double a = 0.0;
     for (int k = 0; k < P->n; ++k) {
@@ -2296,7 +2296,7 @@ typedef struct {
 
 static double rng_next(o_rng *r) { return r->k < r->n ? (double)r->u[r->k++] : 0.5; }
 
-static v2 sample_polygon(const o_clip *poly, double xi_tri, double xi1, double xi2) /* uv_clip.cpp:92-115 */
+static v2 sample_polygon(const o_clip *poly, double xi_tri, double xi1, double xi2) /* uv_clip.cpp:85-108 */
 {
     double areas[8];
     double total = 0.0;
@@ -2410,7 +2410,7 @@ static o_receiver *receiver_of(const double *recv, o_receiver *R)
 
 static double leaf_prob(const o_emitter *e, int64_t i, int64_t j, const o_receiver *rcv, o_fpchild *leaf)
 {
-    /* DescentSampler::leaf_prob (descent_sampler.cpp:292-326) */
+    /* DescentSampler::leaf_prob (descent_sampler.cpp:290-325) */
     int L = e->root_level;
     int64_t ri = i >> L, rj = j >> L;
     int64_t di = ri - e->root_i0, dj = rj - e->root_j0;
@@ -2452,7 +2452,7 @@ double o_emitter_leaf_prob(const o_emitter *e, int64_t i, int64_t j, const doubl
 
 double o_emitter_pdf_uv(const o_emitter *e, double u, double v, const double *recv)
 {
-    /* DescentSampler::pdf_uv (descent_sampler.cpp:344-354) */
+    /* DescentSampler::pdf_uv (descent_sampler.cpp:346-356) */
     int n = e->X->pyr->n_leaf;
     int64_t i = (int64_t)floor(u / (1.0 / n)), j = (int64_t)floor(v / (1.0 / n));
     o_receiver R;
@@ -2465,7 +2465,7 @@ double o_emitter_pdf_uv(const o_emitter *e, double u, double v, const double *re
 
 double o_emitter_pdf_area(const o_emitter *e, double u, double v, const double *recv)
 {
-    /* DescentSampler::pdf_area (descent_sampler.cpp:356-362) */
+    /* DescentSampler::pdf_area (descent_sampler.cpp:358-364) */
     double p = o_emitter_pdf_uv(e, u, v, recv);
     if (p == 0.0)
         return 0.0;

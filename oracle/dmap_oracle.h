@@ -33,7 +33,7 @@ typedef struct o_scene o_scene;
 
 /* Pyramid build modes (taylor_pyramid.h:41-45). */
 enum { O_BUILD_FOLD = 0, O_BUILD_DIRECT = 1 };
-/* Traversal options (traversal_options.h:587-608). */
+/* Traversal options (traversal_options.h:17-38). */
 enum { O_BOUND_BOX = 0, O_BOUND_SLAB = 1, O_BOUND_BOTH = 2 };
 enum { O_LEAF_NEWTON = 0, O_LEAF_TWO_TRIANGLE = 1 };
 /* Triangle order of a scene query: the reference's flat loop, or nearest box
@@ -57,17 +57,17 @@ enum {
  * triangle (scene-global index, -1 on a miss), object. */
 enum { O_HIT_DOUBLES = 12 };
 
-/* TaylorPyramid(values, nodes, scale, build, offset), taylor_pyramid.cpp:324-360. */
+/* TaylorPyramid(values, nodes, scale, build, offset), taylor_pyramid.cpp:215-251. */
 o_pyramid *o_pyramid_build(const double *values, int nodes, double scale, double offset, int build);
 void o_pyramid_free(o_pyramid *p);
 int o_pyramid_levels(const o_pyramid *p);
 int o_pyramid_n_leaf(const o_pyramid *p);
 /* Level l as 8 channel planes (h0, gu, gv, r, ru, rv, h_min, h_max), each m*m, [j*m + i]. */
 void o_pyramid_level(const o_pyramid *p, int level, double *out);
-/* TaylorPyramid::node (taylor_pyramid.cpp:368-383), 8 doubles. */
+/* TaylorPyramid::node (taylor_pyramid.cpp:259-274), 8 doubles. */
 void o_pyramid_node(const o_pyramid *p, int level, int64_t i, int64_t j, double *out8);
 
-/* A scene: objects in order, each an ObjectIntersector (displaced_intersector.cpp:666-679)
+/* A scene: objects in order, each an ObjectIntersector (displaced_intersector.cpp:466-479)
  * over triangles that share one height grid and its pyramid. */
 o_scene *o_scene_create(void);
 void o_scene_free(o_scene *s);
@@ -86,7 +86,7 @@ void o_scene_triangle_frame(const o_scene *s, int tri, double *out12);
 /* rays: n x 8 doubles (o, d, t_min, t_max). hits: n x O_HIT_DOUBLES.
  * stats: n x O_ST_COUNT int64 (may be NULL); level_stats: 32 int64 summed (may be NULL).
  * Flat loop over every triangle of every object, the walk of
- * ObjectIntersector::intersect_flat (displaced_intersector.cpp:778-799)
+ * ObjectIntersector::intersect_flat (displaced_intersector.cpp:578-599)
  * (order O_ORDER_INDEX), or the same triangles nearest box entry first
  * (O_ORDER_NEAREST). threads <= 0 uses every host core. Returns the number
  * of hits. */
@@ -106,9 +106,9 @@ int o_triangle_intersect(const o_scene *s, int tri, const double *ray8, int boun
  * slab pass, t0/t1 of node_interval (4 doubles) = 16 doubles. */
 void o_node_bound(const o_scene *s, int tri, int level, int64_t i, int64_t j, const double *ray8, int bound,
                   int slab_max_level, double *out16);
-/* displaced_position (displaced_surface.cpp:514-518) on triangle tri at (s, t). */
+/* displaced_position (displaced_surface.cpp:162-166) on triangle tri at (s, t). */
 void o_displaced_position(const o_scene *s, int tri, double sp, double tp, double *out3);
-/* BaseTriangle::param (displaced_surface.h:304). */
+/* BaseTriangle::param (displaced_surface.h:87). */
 void o_triangle_param(const o_scene *s, int tri, double u, double v, double *out2);
 /* DisplacedGeometry::surface_point (displaced_geometry.cpp:126-152) with the
  * object's uv map: out14 = p, ng, dpdu, dpdv, uv. */
@@ -121,7 +121,7 @@ void o_surface_point(const o_scene *s, int tri, double u, double v, const double
  * (3 uint32 indices, relative to the triangle's first vertex). */
 void o_tessellate_uniform(const o_scene *s, int tri, int n, float *pos, float *uv, float *nrm, uint32_t *idx);
 /* Texel-aligned tessellation with m x m sub-cells per leaf cell
- * (append_texel_tessellation, :97-137): returns the face count and writes
+ * (append_texel_tessellation, :101-136): returns the face count and writes
  * the first cap faces, three unshared vertices each (pos 9 floats, uv 6,
  * normals 9), the TexelFace st (6 doubles) and its interior flag. */
 int64_t o_tessellate_texel(const o_scene *s, int tri, int m, int64_t cap, float *pos, float *uv, float *nrm,

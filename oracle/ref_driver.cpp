@@ -239,7 +239,7 @@ static bool crossing_opaque(const r_scene *s, const BaseTriangle &tri, int g, co
 
 // A filtered scene: intersect_flat's loop (displaced_intersector.cpp:578-599)
 // with each triangle behind intersect_callback's passes
-// (displaced_geometry.cpp:53-78, max_filter_passes = 64 at displaced_geometry.h:62).
+// (displaced_geometry.cpp:53-78, max_filter_passes = 64 at displaced_geometry.h:64).
 static bool intersect_filtered(const r_scene *s, const RefObject &ob, const vec3d &o, const vec3d &d, double t_min,
                                double &t_max, const dmap::TraversalOptions &opt, dmap::DisplacedHit &hit, int &tri,
                                dmap::TraversalStats *st)

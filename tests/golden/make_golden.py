@@ -9,15 +9,18 @@ and three small known-answer maps from the reference's tests
 (tests/test_pyramid.py): a 33^2 random map at scale 0.4, the 17^2 step edge
 and the 17^2 ramp. Both build modes, every level, all eight channels.
 
-Run in a checkout that holds the reference (its path is the first argument,
-default /root/reference): python tests/golden/make_golden.py [REF_ROOT]
+Run in a checkout that holds the reference; its root is the first argument,
+else $DMAP_REF_ROOT, else /root/reference:
+python tests/golden/make_golden.py [REF_ROOT]
 """
 import sys
 from pathlib import Path
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+import os
+
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DMAP_REF_ROOT", "/root/reference"))
 sys.path.insert(0, str(REF / "code" / "python" / "poc"))
 from dmapref.pyramid import BUILDS, CHANNELS, TaylorPyramid  # noqa: E402
 

@@ -117,13 +117,39 @@ def test_budget_admission_and_rejection(world):
 def test_cancel_queued_request(world):
     ctx, devs, pools, pt = world
     srv = dm.Server(ctx, max_batch_rays=2048, max_inflight=1, slots=1)
+    srv.pause()  # admission held: every submitted request stays queued
     first = srv.submit_rays(devs["sphere"], pools["sphere"])[0]
     rest = [srv.submit_rays(devs["quad"], pools["quad"][:500])[0] for _ in range(6)]
     cancelled = rest[-1]
-    r = srv.cancel(cancelled)
-    assert r in (9, 0, 7)  # cancelled while queued, or already done / running
+    assert srv.cancel(cancelled) == 9  # DMAP_ERR_CANCELLED: it was still queued
+    assert srv.poll(cancelled) == 9
+    assert srv.poll(first) == 7  # DMAP_ERR_NOT_READY: held
+    srv.pause(False)
     assert srv.drain(120.0) == 0
     assert srv.poll(first) == 0
     assert all(srv.poll(i) == 0 for i in rest[:-1])
-    assert srv.poll(cancelled) == (9 if r == 9 else 0)
+    assert srv.poll(cancelled) == 9
+    assert srv.cancel(first) == 0  # done: cancel reports the request's own status
+    st = srv.stats()
+    assert st["cancelled"] == 1 and st["completed"] == 6
+    srv.close()
+
+
+def test_filter_cannot_change_under_served_requests(world):
+    """While a server holds a request on a scene, the scene's filter stays as
+    it was when the request was admitted; once the request is done (here:
+    cancelled) it can change."""
+    ctx, devs, pools, pt = world
+    scene = devs["quad"]
+    srv = dm.Server(ctx, max_batch_rays=2048, slots=1)
+    srv.pause()
+    rid = srv.submit_rays(scene, pools["quad"][:256])[0]
+    mask = np.ones((4, 4), np.uint8)
+    with pytest.raises(dm.DmapError) as e:
+        scene.set_opacity(mask)
+    assert e.value.status == 7  # DMAP_ERR_NOT_READY
+    assert srv.cancel(rid) == 9
+    scene.set_opacity(mask)
+    scene.set_opacity(None)
+    srv.pause(False)
     srv.close()

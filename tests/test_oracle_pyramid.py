@@ -72,7 +72,7 @@ def test_containment(oracle, case, build):
 
 
 def test_offset_shifts_value_channels_only(oracle):
-    """taylor_pyramid.cpp:348-359: a constant offset moves h0, h_min and h_max."""
+    """taylor_pyramid.cpp:239-250: a constant offset moves h0, h_min and h_max."""
     values, scale, _ = load("random_33")
     a = oracle.pyramid(values, scale, 0.0)
     b = oracle.pyramid(values, scale, 0.25)

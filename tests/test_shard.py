@@ -71,3 +71,61 @@ def test_gather_hits_gloo(world, n):
         assert p.exitcode == 0
     want = _fake_hits(0, n).tobytes()
     assert all(b == want for _, b in got)
+
+
+_REC = np.dtype([("rec", "<f8", 12)])
+
+
+def _scene_and_rays():
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+    import py_oracle
+    from dmap_b200 import scenes
+    import helpers
+    sc = helpers.small_sphere(16)
+    cpu = py_oracle.CpuScene(py_oracle.Oracle(), sc)
+    rays = np.concatenate([scenes.sphere_camera_rays(48, 27), helpers.near_surface_rays(cpu, 700)])
+    return cpu, rays
+
+
+def _query_rank(rank, world, port, q):
+    """One rank of a replicated-scene query: the whole scene, its share of
+    the rays answered through the CPU oracle, then the optional all-gather."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cpu, rays = _scene_and_rays()
+        lo, hi = shard_range(len(rays), rank, world)
+        h, _ = cpu.intersect(rays[lo:hi], order="nearest")
+        local = np.ascontiguousarray(h).view(_REC).reshape(-1)
+        q.put((rank, hi - lo, gather_hits(local, len(rays)).tobytes()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_query_equals_one_rank(world):
+    """Each rank answers its share of real rays over its replica of the
+    scene; the gathered answers equal one process answering them all."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_query_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    cpu, rays = _scene_and_rays()
+    h, _ = cpu.intersect(rays, order="nearest")
+    want = np.ascontiguousarray(h).view(_REC).reshape(-1).tobytes()
+    assert sum(n for _, n, _ in got) == len(rays)
+    assert all(b == want for _, _, b in got)
+    assert (h[:, 10] >= 0).sum() > 100  # the shares hold real hits
