@@ -53,17 +53,8 @@ def peaks():
 def build_scene(config: str, small: bool):
     if config == "quad":
         return scenes.quad_scene(128 if small else 512), scenes.quad_camera_rays(*(64, 64) if small else (256, 256))
-    n = 256 if small else 2048
-    k = 4
-    # parallel map generation: 96 independent seeded maps
-    def one(pid):
-        return scenes.sine_noise_heights(n, scenes.SEED + pid, 0.08, octaves=4)
-    with cf.ThreadPoolExecutor(min(16, os.cpu_count() or 4)) as ex:
-        maps = list(ex.map(one, range(6 * k * k)))
-    sc = scenes.cube_sphere_scene(1, k)   # geometry only, tiny maps replaced below
     texel = np.float16 if config == "sphere16" else np.float32
-    for pid, a in enumerate(sc.assets):
-        a.nodes = scenes.close_tile(maps[pid], repeat=False).astype(texel)
+    sc = scenes.sphere_benchmark_scene(256 if small else 2048, texel, min(16, os.cpu_count() or 4))
     w, h = (480, 270) if small else (1920, 1080)
     return sc, scenes.sphere_camera_rays(w, h)
 

@@ -197,6 +197,27 @@ def cube_sphere_scene(n: int = 2048, k: int = 4, seed: int = SEED, amplitude: fl
                  name=f"cube_sphere{k}x{k}x6_{n}", extent=2.0 * math.sqrt(3.0) * (1.0 + amplitude))
 
 
+def sphere_benchmark_scene(n: int = 2048, texel=np.float32, threads: int = 16) -> Scene:
+    """The GPU-scale plain-method scene: the radius-1 cube sphere of 96
+    patches, each its own n x n map of seeded sines + 4 octaves of value
+    noise (amplitude 0.08, seed + patch id), stored as `texel` (float32, or
+    float16 for the precision variant). The 96 maps are generated on
+    `threads` threads."""
+    import concurrent.futures as cf
+    k = 4
+
+    def one(pid):
+        return close_tile(sine_noise_heights(n, SEED + pid, 0.08, octaves=4), repeat=False).astype(texel)
+
+    with cf.ThreadPoolExecutor(max(1, threads)) as ex:
+        maps = list(ex.map(one, range(6 * k * k)))
+    sc = cube_sphere_scene(1, k)  # the geometry; its 1 x 1 maps are replaced
+    for pid, a in enumerate(sc.assets):
+        a.nodes = maps[pid]
+    sc.name = f"cube_sphere{k}x{k}x6_{n}"
+    return sc
+
+
 def ground_plane_asset(n: int = 4096, seed: int = SEED + 1000, amplitude: float = 0.2,
                        dtype=np.float32) -> Asset:
     return Asset(close_tile(ridged_heights(n, seed, amplitude), repeat=False).astype(dtype))

@@ -197,7 +197,7 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *o
 /*
  * The order in which a ray visits the triangles whose boxes it meets.
  * INDEX is ObjectIntersector::intersect's flat loop (displaced_intersector.cpp:
- * 778-799): triangles in index order, each walked with the t_max the ones
+ * 578-599): triangles in index order, each walked with the t_max the ones
  * before it left. NEAREST visits them by box entry distance (the FP64 slab
  * entry max(t_min, max_a min(ta, tb)), ta = (lo_a - o_a) * (1 / d_a), ties
  * to the lower index), as a BVH over the embree callbacks

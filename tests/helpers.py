@@ -91,3 +91,32 @@ def chart_scene(n=32, seed=7):
     tris = np.stack(tris)
     tris[:, 18:24] += rng.random(6) * 1e-3  # off the dyadic lattice
     return scenes.Scene([a0, a1], tris, np.array([0, 0, 1], np.int32), name=f"charts{n}", extent=3.0)
+
+
+def oracle_flat_loop_by_groups(oracle, scene, rays, group=16, threads=0):
+    """The reference's flat loop over every triangle of `scene`, in index
+    order, evaluated `group` assets at a time so that only one group's FP64
+    pyramids are held at once: each group's flat loop runs with the t_max the
+    earlier groups left (the hit's t, as the loop itself sets it), so the
+    chained result is the whole loop's, record for record. Triangles must be
+    grouped by asset in index order (tri_asset non-decreasing)."""
+    import py_oracle
+    ta = scene.tri_asset
+    assert (np.diff(ta) >= 0).all(), "triangles must be in asset order"
+    r = np.ascontiguousarray(rays, np.float64).copy()
+    best = np.zeros((len(r), py_oracle.HIT))
+    best[:, 0] = np.inf
+    best[:, 10:12] = -1  # triangle, object
+    for g0 in range(0, len(scene.assets), group):
+        keep = (ta >= g0) & (ta < g0 + group)
+        first = int(np.argmax(keep))
+        sub = scenes.Scene(scene.assets[g0:g0 + group], scene.tris[keep], (ta[keep] - g0).astype(np.int32))
+        cpu = py_oracle.CpuScene(oracle, sub)
+        h, _ = cpu.intersect(r, order="index", threads=threads)
+        del cpu
+        found = h[:, 10] >= 0
+        h[found, 10] += first
+        h[found, 11] += g0  # objects are assets in order
+        best[found] = h[found]
+        r[found, 7] = h[found, 0]
+    return best

@@ -127,3 +127,17 @@ def test_nearest_order_same_hits(oracle, quad, sphere, name):
     assert (np.abs(hi[hit, 0] - hn[hit, 0]) <= 4 * tol[tri]).all()
     assert (hi[hit, 0] == hn[hit, 0]).mean() > 0.99
     assert sn[:, 0].sum() <= si[:, 0].sum() and sn[:, 1].sum() <= si[:, 1].sum()
+
+
+def test_flat_loop_by_groups_equals_the_whole_loop(oracle):
+    """The chained evaluation the full-size tests use (a group of assets at
+    a time, each group's loop starting from the t_max the earlier groups
+    left) is the whole flat loop, record for record."""
+    sc = helpers.small_sphere(16)
+    cpu = py_oracle.CpuScene(oracle, sc)
+    rays = np.concatenate([helpers.near_surface_rays(cpu, 1500), scenes.sphere_camera_rays(40, 30)])
+    whole, _ = cpu.intersect(rays, order="index")
+    for g in (1, 2, 4):
+        chained = helpers.oracle_flat_loop_by_groups(oracle, sc, rays, group=g)
+        assert np.array_equal(chained.tobytes(), whole.tobytes())
+    assert (whole[:, 10] >= 0).sum() > 300
