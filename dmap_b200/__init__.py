@@ -51,7 +51,7 @@ HIT64 = np.dtype([("t", "<f8"), ("st", "<f8", 2), ("bary", "<f8", 2), ("ng", "<f
                   ("i", "<i4"), ("j", "<i4"), ("flags", "<i4")])
 STATS = ("triangle_tests", "node_tests", "leaf_tests", "sub_squares", "newton_iters", "node_tests_after_hit",
          "leaf_tests_after_hit", "reserved")
-HIT_FP64_LEAF, HIT_CAPPED = 1, 2
+HIT_FP64_LEAF, HIT_CAPPED, HIT_POLISHED = 1, 2, 4
 
 
 class DmapError(RuntimeError):
@@ -63,7 +63,8 @@ class DmapError(RuntimeError):
 class _Options(C.Structure):
     _fields_ = [("bound", C.c_int), ("slab_max_level", C.c_int), ("leaf", C.c_int), ("precision", C.c_int),
                 ("mode", C.c_int), ("polish_cond", C.c_double), ("schedule", C.c_int), ("rounds", C.c_int),
-                ("blocks_per_sm", C.c_int), ("order", C.c_int), ("node_visit_cap", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("order", C.c_int), ("node_visit_cap", C.c_int),
+                ("leaf_precision", C.c_int), ("graph", C.c_int)]
 
 
 class _Camera(C.Structure):
@@ -204,11 +205,14 @@ class TraversalOptions:
     blocks_per_sm: int = 5
     order: str = "nearest"
     node_visit_cap: int = 0
+    leaf_precision: str = "f64"
+    graph: bool = False
 
     def c(self) -> _Options:
         return _Options(BOUND[self.bound], self.slab_max_level, LEAF[self.leaf], PRECISION[self.precision],
                         MODE[self.mode], self.polish_cond, SCHEDULE[self.schedule], self.rounds,
-                        self.blocks_per_sm, ORDER[self.order], self.node_visit_cap)
+                        self.blocks_per_sm, ORDER[self.order], self.node_visit_cap,
+                        PRECISION[self.leaf_precision], int(self.graph))
 
 
 class Context:

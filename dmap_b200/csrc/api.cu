@@ -65,6 +65,10 @@ void dmap_destroy(dmap_context *ctx)
     cudaFree(ctx->hits_dev);
     cudaFree(ctx->stats_dev);
     cudaFree(ctx->status_dev);
+    for (auto &g : ctx->graphs)
+        cudaGraphExecDestroy(g.exec);
+    cudaFree(ctx->n_dev);
+    cudaFreeHost(ctx->n_host);
     wave_release(ctx->wave);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -88,6 +92,8 @@ void dmap_options_default(dmap_options *opt)
     opt->blocks_per_sm = 5;
     opt->order = DMAP_ORDER_NEAREST;
     opt->node_visit_cap = 0;
+    opt->leaf_precision = DMAP_PRECISION_F64;
+    opt->graph = 0;
 }
 
 // ---- assets ---------------------------------------------------------------
@@ -512,6 +518,15 @@ void dmap_scene_destroy(dmap_scene *s)
         return;
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
+    auto &gs = s->ctx->graphs;
+    for (size_t k = 0; k < gs.size();) {
+        if (gs[k].scene == s) {
+            cudaGraphExecDestroy(gs[k].exec);
+            gs.erase(gs.begin() + k);
+        } else {
+            ++k;
+        }
+    }
     cudaFree(s->assets_dev);
     cudaFree(s->tris_dev);
     cudaFree(s->tris32_dev);
@@ -625,6 +640,11 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
         return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: node_visit_cap must be >= 0");
     q.order = o.order;
     q.guard_cap = o.node_visit_cap > 0 ? o.node_visit_cap : (1 << 26);
+    if (o.leaf_precision != DMAP_PRECISION_F64 && o.leaf_precision != DMAP_PRECISION_F32)
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: leaf_precision is DMAP_PRECISION_F64 or _F32");
+    if (o.leaf_precision == DMAP_PRECISION_F32 && !(o.polish_cond >= 0.0))
+        return fail(ctx, DMAP_ERR_INVALID, "dmap_intersect: polish_cond must be >= 0");
+    q.leaf_precision = o.precision == DMAP_PRECISION_F32 ? o.leaf_precision : DMAP_PRECISION_F64;
     q.schedule = o.schedule;
     q.rounds = o.rounds;
     q.blocks_per_sm = o.blocks_per_sm;
@@ -695,6 +715,61 @@ dmap_status dmap_intersect(dmap_scene *s, const void *rays_dev, dmap_dtype ray_d
     return run_query(s, rays_dev, n, q, hits_dev, stats_dev, stream ? (cudaStream_t)stream : s->ctx->stream);
 }
 
+// The query's launches for up to `cap` rays captured once (the count read
+// from ctx->n_dev when a replay runs), or the cached graph of the same
+// scene, options and capacity on the same buffers.
+static dmap_status query_graph(dmap_scene *s, const dmapk::QueryOpts &q0, int64_t cap, cudaGraphExec_t *out)
+{
+    dmap_context *ctx = s->ctx;
+    char key[256];
+    snprintf(key, sizeof key, "b%d_s%d_l%d_m%d_p%.17g_r%d_h%d_sc%d_ro%d_bp%d_o%d_g%d_lp%d", q0.bound, q0.slab_max_level,
+             q0.leaf, q0.mode, q0.polish_cond, q0.ray_dtype, q0.hit_dtype, q0.schedule, q0.rounds, q0.blocks_per_sm,
+             q0.order, q0.guard_cap, q0.leaf_precision);
+    for (auto &g : ctx->graphs)
+        if (g.scene == s && g.capacity == cap && g.key == key && g.rays == ctx->rays_dev && g.hits == ctx->hits_dev &&
+            g.scratch == ctx->wave.state) {
+            *out = g.exec;
+            return DMAP_OK;
+        }
+    if (!ctx->n_dev) {
+        DMAP_CUDA(ctx, cudaMalloc(&ctx->n_dev, sizeof(long long)));
+        DMAP_CUDA(ctx, cudaMallocHost(&ctx->n_host, sizeof(long long)));
+    }
+    dmapk::QueryOpts q = q0;
+    q.n_dev = ctx->n_dev;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    DMAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+    const int64_t launches = ctx->launches.load();
+    dmap_status st = run_query(s, ctx->rays_dev, cap, q, ctx->hits_dev, nullptr, ctx->stream);
+    ctx->launches.store(launches); // counted per replay instead
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != DMAP_OK) {
+        if (graph)
+            cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "dmap_intersect_host: graph capture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "dmap_intersect_host: graph instantiate");
+    // entries captured on buffers since replaced are dropped here
+    auto &gs = ctx->graphs;
+    for (size_t k = 0; k < gs.size();) {
+        if (gs[k].rays != ctx->rays_dev || gs[k].hits != ctx->hits_dev || gs[k].scratch != ctx->wave.state) {
+            cudaGraphExecDestroy(gs[k].exec);
+            gs.erase(gs.begin() + k);
+        } else {
+            ++k;
+        }
+    }
+    gs.push_back({s, key, cap, ctx->rays_dev, ctx->hits_dev, ctx->wave.state, exec});
+    *out = exec;
+    return DMAP_OK;
+}
+
 dmap_status dmap_intersect_host(dmap_scene *s, const void *rays_host, dmap_dtype ray_dtype, int64_t n,
                                 const dmap_options *opt, void *hits_host, dmap_dtype hit_dtype, int64_t *stats_host)
 {
@@ -706,17 +781,45 @@ dmap_status dmap_intersect_host(dmap_scene *s, const void *rays_host, dmap_dtype
         return st;
     dmap_context *ctx = s->ctx;
     DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    // graph replay: FP32 path, no counters, no filter (whose mask may change)
+    const bool graph = opt && opt->graph && q.precision == DMAP_PRECISION_F32 && !stats_host && !q.op_mask;
+    int64_t cap = n;
+    if (graph) {
+        cap = 1024;
+        while (cap < n)
+            cap *= 2;
+    }
     size_t rb = (size_t)n * 8 * dtype_size(ray_dtype);
     size_t hb = (size_t)n * (hit_dtype == DMAP_F64 ? sizeof(dmap_hit64) : sizeof(dmap_hit32));
     size_t sb = stats_host ? (size_t)n * DMAP_ST_COUNT * sizeof(int64_t) : 0;
-    if ((st = grow(ctx, &ctx->rays_dev, &ctx->rays_cap, rb)) != DMAP_OK ||
-        (st = grow(ctx, &ctx->hits_dev, &ctx->hits_cap, hb)) != DMAP_OK ||
+    size_t rcap = (size_t)cap * 8 * dtype_size(ray_dtype);
+    size_t hcap = (size_t)cap * (hit_dtype == DMAP_F64 ? sizeof(dmap_hit64) : sizeof(dmap_hit32));
+    if ((st = grow(ctx, &ctx->rays_dev, &ctx->rays_cap, rcap)) != DMAP_OK ||
+        (st = grow(ctx, &ctx->hits_dev, &ctx->hits_cap, hcap)) != DMAP_OK ||
         (sb && (st = grow(ctx, &ctx->stats_dev, &ctx->stats_cap, sb)) != DMAP_OK))
         return st;
-    DMAP_CUDA(ctx, cudaMemcpyAsync(ctx->rays_dev, rays_host, rb, cudaMemcpyHostToDevice, ctx->stream));
-    if ((st = run_query(s, ctx->rays_dev, n, q, ctx->hits_dev, sb ? ctx->stats_dev : nullptr, ctx->stream)) !=
-        DMAP_OK)
-        return st;
+    if (graph) {
+        if (q.schedule == DMAP_SCHEDULE_WAVEFRONT && cap > ctx->wave.capacity) {
+            // the scratch is captured into the graph: grow it before capture
+            DMAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            if ((st = wave_reserve(ctx, ctx->wave, cap)) != DMAP_OK)
+                return st;
+        }
+        cudaGraphExec_t exec = nullptr;
+        if ((st = query_graph(s, q, cap, &exec)) != DMAP_OK)
+            return st;
+        *ctx->n_host = (long long)n;
+        DMAP_CUDA(ctx, cudaMemcpyAsync(ctx->n_dev, ctx->n_host, sizeof(long long), cudaMemcpyHostToDevice,
+                                       ctx->stream));
+        DMAP_CUDA(ctx, cudaMemcpyAsync(ctx->rays_dev, rays_host, rb, cudaMemcpyHostToDevice, ctx->stream));
+        DMAP_CUDA(ctx, cudaGraphLaunch(exec, ctx->stream));
+        ctx->launches += dmapk::walk32_launches(q);
+    } else {
+        DMAP_CUDA(ctx, cudaMemcpyAsync(ctx->rays_dev, rays_host, rb, cudaMemcpyHostToDevice, ctx->stream));
+        if ((st = run_query(s, ctx->rays_dev, n, q, ctx->hits_dev, sb ? ctx->stats_dev : nullptr, ctx->stream)) !=
+            DMAP_OK)
+            return st;
+    }
     DMAP_CUDA(ctx, cudaMemcpyAsync(hits_host, ctx->hits_dev, hb, cudaMemcpyDeviceToHost, ctx->stream));
     if (sb)
         DMAP_CUDA(ctx, cudaMemcpyAsync(stats_host, ctx->stats_dev, sb, cudaMemcpyDeviceToHost, ctx->stream));

@@ -35,6 +35,20 @@ struct dmap_context
     dmapk::WaveScratch wave; // the wavefront schedule's scratch, grown to the largest batch
     std::atomic<int64_t> launches{0};
     std::string error;
+    // CUDA graphs of dmap_intersect_host's query launches (dmap_options.graph):
+    // one per scene, options and power-of-two capacity, valid while the
+    // staging buffers and the wavefront scratch they were captured on stay
+    struct QueryGraph
+    {
+        const dmap_scene *scene;
+        std::string key;
+        int64_t capacity;
+        const void *rays, *hits, *scratch;
+        cudaGraphExec_t exec;
+    };
+    std::vector<QueryGraph> graphs;
+    long long *n_dev = nullptr;  // the ray count a replayed graph reads
+    long long *n_host = nullptr; // its pinned host staging
     // device staging for dmap_intersect_host
     void *rays_dev = nullptr, *hits_dev = nullptr;
     int64_t *stats_dev = nullptr;

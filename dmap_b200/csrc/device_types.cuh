@@ -133,6 +133,9 @@ struct Hit64
 #ifndef DMAP_HIT_CAPPED
 #define DMAP_HIT_CAPPED 2 // a walk cap of the query ran out for this ray
 #endif
+#ifndef DMAP_HIT_POLISHED
+#define DMAP_HIT_POLISHED 4 // an FP32 leaf root refined by FP64 Newton (ill-conditioned Jacobian)
+#endif
 
 // Per-ray counter slots (TraversalStats), as DMAP_ST_* of include/dmap_b200.h.
 enum

@@ -20,6 +20,7 @@ struct QueryOpts
     int blocks_per_sm;        // wavefront walk: resident 128-thread CTAs per SM
     int order = 1;            // DMAP_ORDER_*: 0 index order, 1 nearest box entry first
     int guard_cap = 1 << 26;  // FP32 walk: cells one triangle walk may visit before it gives up
+    int leaf_precision = 0;   // FP32 walk: DMAP_PRECISION_F64 (the reference's leaf) or _F32 (leaf32.cuh)
     // When set, the number of rays is read here on the device when the query
     // runs (at most the n the launch is given, which sizes grids and scratch):
     // stages of a device-driven pipeline pass counts they produced themselves.

@@ -28,7 +28,8 @@ std::string tune_key(const dmap_scene *s, const dmapk::QueryOpts &q, int64_t n)
         ++log2n;
     std::ostringstream k;
     k << "tri" << s->n_tri << "_assets" << s->assets.size() << "_texels" << texels << "_dt" << dtypes << "_mode"
-      << q.mode << "_bound" << q.bound << "_slab" << q.slab_max_level << "_n2^" << log2n;
+      << q.mode << "_bound" << q.bound << "_slab" << q.slab_max_level << "_order" << q.order << "_leaf"
+      << q.leaf_precision << "_n2^" << log2n;
     return k.str();
 }
 

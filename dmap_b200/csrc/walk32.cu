@@ -35,6 +35,7 @@
 // This translation unit is compiled with -fmad=false (the FP64 leaf must
 // round like the reference); FP32 code uses explicit fmaf where it wants one.
 #include "f32_node.cuh"
+#include "leaf32.cuh"
 #include "order.cuh"
 #include "filter.cuh"
 
@@ -173,10 +174,29 @@ __device__ __forceinline__ float far_bound(float t1) { return ru_add(ru_mul(t1, 
 
 // ---- simple schedule: one thread per ray ----------------------------------
 
+// A leaf cell the FP32 walk reached, in the simple schedule and the
+// inline-leaf walk: the cell's FP64 node test, then the certified leaf in the
+// query's leaf precision (FP64: the reference's leaf; FP32: leaf32.cuh).
+// flags: DMAP_HIT_* of the root.
+__device__ __noinline__ bool leaf_cell(const TriDev32 &T32, const TriDev &T, const AssetDev &g, const double *o,
+                                       const double *d, double t_min, double t_max, int i, int j, d64::hit64 &h,
+                                       int &flags, int64_t *st, const dmapk::QueryOpts &opt)
+{
+    if (opt.leaf_precision != 1) {
+        flags = DMAP_HIT_FP64_LEAF;
+        return leaf64(T, g, o, d, t_min, t_max, i, j, h, st, opt);
+    }
+    d64::v3 O = d64::V3(o[0], o[1], o[2]), D = d64::V3(d[0], d[1], d[2]);
+    if (!d64::leaf_cell_admitted(T, g, O, D, t_min, t_max, i, j, opt))
+        return false;
+    return l32::intersect_newton32(T, T32, g, O, D, t_min, t_max, i, j, opt.polish_cond, h, flags, st);
+}
+
 // DisplacedIntersector::intersect with the FP32 node test.
 __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const AssetDev &g, const double *o,
                                 const double *d, double t_min, double &t_max, const dmapk::QueryOpts &opt,
-                                d64::hit64 &hit, int64_t *st, float t_far, unsigned *status, bool &capped)
+                                d64::hit64 &hit, int &hflags, int64_t *st, float t_far, unsigned *status,
+                                bool &capped)
 {
     Ray32 r;
     tangent_ray(T, o, d, t_far, r);
@@ -220,8 +240,10 @@ __device__ bool triangle_walk32(const TriDev32 &T, const TriDev &T64, const Asse
                 ++lah;
             }
             d64::hit64 lh;
-            if (leaf64(T64, g, o, d, t_min, t_max, cur.i, cur.j, lh, st, opt) && lh.t < t_max) {
+            int lf = 0;
+            if (leaf_cell(T, T64, g, o, d, t_min, t_max, cur.i, cur.j, lh, lf, st, opt) && lh.t < t_max) {
                 hit = lh;
+                hflags = lf;
                 t_max = lh.t;
                 found = true;
                 nah = lah = 0;
@@ -259,7 +281,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
     int64_t st[DMAP_ST_N] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t *sp = stats ? st : nullptr;
     d64::hit64 best;
-    int best_tri = -1;
+    int best_tri = -1, best_flags = 0;
     bool found = false, capped = false;
     // the next triangle: index order, or (nearest) the smallest (key, index)
     // past the cursor among the candidates the ray still reaches
@@ -296,12 +318,13 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
         if (sp)
             ++st[DMAP_ST_TRI];
         d64::hit64 h;
+        int hf = 0;
         bool got = false;
         // the callbacks' filter passes (displaced_geometry.cpp:53-106); no filter: one walk
         double t_lo = t_min;
         for (int pass = 0; pass < (opt.op_mask ? dmapdev::kFilterPasses : 1); ++pass) {
             double tm = t_max;
-            if (!triangle_walk32(T, tris64[t], assets[T.asset], o, d, t_lo, tm, opt, h, sp, far_bound(t1), status,
+            if (!triangle_walk32(T, tris64[t], assets[T.asset], o, d, t_lo, tm, opt, h, hf, sp, far_bound(t1), status,
                                  capped))
                 break;
             if (dmapdev::crossing_opaque(opt, tris64[t], t, h.bary.x, h.bary.y)) {
@@ -312,6 +335,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
         }
         if (got) {
             best = h;
+            best_flags = hf;
             best_tri = t;
             t_max = h.t;
             found = true;
@@ -319,7 +343,7 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
                 break;
         }
     }
-    store_hit<H, Fp>(hits, k, found, best, best_tri, (found ? DMAP_HIT_FP64_LEAF : 0) | (capped ? DMAP_HIT_CAPPED : 0));
+    store_hit<H, Fp>(hits, k, found, best, best_tri, (found ? best_flags : 0) | (capped ? DMAP_HIT_CAPPED : 0));
     if (stats)
         for (int q = 0; q < DMAP_ST_N; ++q)
             stats[DMAP_ST_N * k + q] = st[q];
@@ -923,15 +947,15 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 if (INLINE_LEAF) {
                     // the last round: the few remaining rays finish here
                     d64::hit64 lh;
-                    if (leaf64(tris64[tri], assets[T.asset], o, d, t_min, t_max, cur.i, cur.j, lh,
-                               ST ? stl : nullptr, opt) &&
+                    int lf = 0;
+                    if (leaf_cell(T, tris64[tri], assets[T.asset], o, d, t_min, t_max, cur.i, cur.j, lh, lf,
+                                  ST ? stl : nullptr, opt) &&
                         lh.t < t_max) {
                         t_max = lh.t;
                         best_tri = tri;
                         flags |= kFoundInTri;
                         nah = lah = 0;
-                        store_hit<H, Fp>(hits, ray, true, lh, tri,
-                                         DMAP_HIT_FP64_LEAF | ((flags & kCapped) ? DMAP_HIT_CAPPED : 0));
+                        store_hit<H, Fp>(hits, ray, true, lh, tri, lf | ((flags & kCapped) ? DMAP_HIT_CAPPED : 0));
                         if (opt.mode == 1) {
                             flush_stats();
                             phase = NEED;
@@ -1177,6 +1201,157 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
     }
 }
 
+// The parked leaves of a round with the FP32 certified leaf (leaf32.cuh):
+// wave_leaf's schedule (one job per lane, a lane takes the next job when its
+// own is done, one search step per loop iteration) over the FP32 leaf state.
+#ifndef DMAP_LEAF32_MIN_BLOCKS
+#define DMAP_LEAF32_MIN_BLOCKS 1
+#endif
+template <bool ST, typename R, typename H, typename Fp>
+__global__ void __launch_bounds__(128, DMAP_LEAF32_MIN_BLOCKS)
+    wave_leaf32(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64,
+                const AssetDev *__restrict__ assets, const R *__restrict__ rays, dmapk::QueryOpts opt,
+                H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
+                const LeafJob *__restrict__ q_leaf, int round, int *__restrict__ q_out, unsigned long long *ctr)
+{
+    using namespace d64;
+    constexpr int kDepth = 5; // subdivision_depth
+    enum : int { NEED = 0, SETUP = 1, SEARCH = 2, DONE = 3 };
+    const int lane = threadIdx.x & 31;
+    const unsigned long long count = *round_ctr(ctr, round, 1);
+    unsigned long long *fetch = round_ctr(ctr, round, 2);
+    int phase = NEED;
+    unsigned long long item = 0;
+    int ray = 0, tri = 0, n_leaves = 0, q = 0, li = 0, lj = 0, sp = 0;
+    bool first = false, answered = false;
+    double t_min = 0.0, t_max = 0.0;
+    v3 O = V3(0.0, 0.0, 0.0), D = O;
+    l32::Leaf32 L;
+    l32::Ent32 stack[4 * kDepth + 4];
+    int64_t subs = 0, iters = 0;
+
+    for (;;) {
+        unsigned need = __ballot_sync(FULL, phase == NEED);
+        if (need) {
+            int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if (lane == leader)
+                base = atomicAdd(fetch, (unsigned long long)__popc(need));
+            base = __shfl_sync(FULL, base, leader);
+            if (phase == NEED) {
+                item = base + (unsigned long long)__popc(need & ((1u << lane) - 1u));
+                if (item >= count) {
+                    phase = DONE;
+                } else {
+                    const LeafJob &J = q_leaf[item];
+                    ray = J.ray;
+                    tri = J.tri;
+                    n_leaves = J.n;
+                    q = 0;
+                    if (n_leaves == 0) {
+                        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 3), 1ull);
+                        q_out[slot] = ray;
+                    } else {
+                        double o[3], d[3];
+                        load_ray(rays, ray, o, d, t_min, t_max);
+                        O = V3(o[0], o[1], o[2]);
+                        D = V3(d[0], d[1], d[2]);
+                        t_max = states[ray].t_max;
+                        answered = false;
+                        subs = iters = 0;
+                        phase = SETUP;
+                    }
+                }
+            }
+        }
+        if (__all_sync(FULL, phase == DONE))
+            break;
+        const TriDev &T = tris64[tri];
+        const AssetDev &g = assets[T.asset];
+        if (phase == SETUP) {
+            li = q_leaf[item].i[q];
+            lj = q_leaf[item].j[q];
+            l32::leaf_setup32(T, g, O, D, li, lj, L);
+            sp = 0;
+            stack[sp++] = {0.5f, 0.5f, -INFINITY, 0};
+            first = true;
+            phase = SEARCH;
+        }
+        bool expand = false, newton = false;
+        l32::Ent32 e = {0.0f, 0.0f, 0.0f, 0};
+        if (phase == SEARCH) {
+            while (sp > 0) {
+                e = stack[--sp];
+                if (first || (double)e.t_lo < t_max) {
+                    first = false;
+                    newton = e.depth == kDepth;
+                    expand = !newton;
+                    break;
+                }
+            }
+            if (!expand && !newton) {
+                if (++q < n_leaves && !answered) {
+                    phase = SETUP;
+                } else {
+                    if (ST) {
+                        stats[DMAP_ST_N * (int64_t)ray + DMAP_ST_SUB] += subs;
+                        stats[DMAP_ST_N * (int64_t)ray + DMAP_ST_NEWTON] += iters;
+                    }
+                    if (!answered) {
+                        unsigned long long slot = atomicAdd(round_ctr(ctr, round, 3), 1ull);
+                        q_out[slot] = ray;
+                    }
+                    phase = NEED;
+                }
+            }
+        }
+        __syncwarp();
+        if (expand) {
+            const TriDev32 &T32 = tris32[tri];
+            float r = __int_as_float((125 - e.depth) << 23); // half of the entry's rho = 0.5 * 2^-depth
+            l32::Ent32 ch[4];
+            int n = 0;
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) {
+                float ca = e.a + ((k & 1) ? r : -r), cb = e.b + ((k & 2) ? r : -r), tl;
+                ++subs;
+                if (l32::sub_square_bound32(T32, L, ca, cb, r, t_min, t_max, tl))
+                    ch[n++] = {ca, cb, tl, e.depth + 1};
+            }
+            for (int p = 1; p < n; ++p)
+                for (int k = p; k > 0 && ch[k].t_lo < ch[k - 1].t_lo; --k) {
+                    l32::Ent32 x = ch[k];
+                    ch[k] = ch[k - 1];
+                    ch[k - 1] = x;
+                }
+            for (int k = n - 1; k >= 0; --k)
+                stack[sp++] = ch[k];
+        }
+        __syncwarp();
+        if (newton) {
+            l32::Root32 root;
+            hit64 h;
+            int fl = 0;
+            if (l32::newton32(T, L, e.a, e.b, root, iters) &&
+                l32::accept_root(T, g, L.lo_s, L.lo_t, L.w, L.Q3, L.inv_dlen, O, D, t_min, t_max, li, lj, root,
+                                 opt.polish_cond, h, fl, iters)) {
+                t_max = h.t;
+                RayState &s = states[ray];
+                s.t_max = h.t;
+                s.best_tri = tri;
+                s.flags |= kFoundInTri;
+                s.nah = s.lah = 0;
+                store_hit<H, Fp>(hits, ray, true, h, tri, fl | ((s.flags & kCapped) ? DMAP_HIT_CAPPED : 0));
+                if (opt.mode == 1) {
+                    answered = true;
+                    sp = 0;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 int sm_count()
 {
     static int sms = 0;
@@ -1263,12 +1438,20 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
             break;
         int lgrid = sm_count() * 4;
         wave_filter<R><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, states, leaves, rd, ws.counters);
-        if (stats)
+        if (opt.leaf_precision == 1) { // the FP32 certified leaf
+            if (stats)
+                wave_leaf32<true, R, H, Fp><<<lgrid, 128, 0, stream>>>(t32, t64, assets, rr, opt, hh, stats, states,
+                                                                      leaves, rd, q_out, ws.counters);
+            else
+                wave_leaf32<false, R, H, Fp><<<lgrid, 128, 0, stream>>>(t32, t64, assets, rr, opt, hh, nullptr, states,
+                                                                       leaves, rd, q_out, ws.counters);
+        } else if (stats) {
             wave_leaf<true, R, H, Fp><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, hh, stats, states, leaves, rd,
                                                                 q_out, ws.counters);
-        else
+        } else {
             wave_leaf<false, R, H, Fp><<<lgrid, 128, 0, stream>>>(t64, assets, rr, opt, hh, nullptr, states, leaves,
                                                                  rd, q_out, ws.counters);
+        }
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;
     }

@@ -216,8 +216,8 @@ typedef struct dmap_options {
     int leaf;           /* DMAP_LEAF_*, default NEWTON */
     int precision;      /* DMAP_PRECISION_*, default F32 */
     int mode;           /* DMAP_MODE_*, default CLOSEST */
-    double polish_cond; /* reserved for an FP32 leaf with FP64 refinement above this cond(J) (default
-                           1e4); the library's leaves are FP64 throughout and ignore it */
+    double polish_cond; /* FP32 leaf: roots whose Newton Jacobian has cond(J) above this are refined by the
+                           reference's FP64 Newton (default 1e4) */
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
                            default 6; 0 = one walk with every leaf inline) */
@@ -227,6 +227,14 @@ typedef struct dmap_options {
                            2^26, far above any walk of a well-formed scene). A ray whose walk gives up keeps
                            what it found, its hit record gets DMAP_HIT_CAPPED, and the call reports
                            DMAP_ERR_LIMIT */
+    int leaf_precision; /* FP32 path's certified leaf: DMAP_PRECISION_F64 (default: the reference's leaf in
+                           double, every hit equal to the FP64 path's bit for bit) or DMAP_PRECISION_F32
+                           (the leaf's search and Newton in FP32 with outward-rounded sub-square bounds, FP64
+                           Newton polish above polish_cond; hits within the FP32 leaf's tolerance) */
+    int graph;          /* dmap_intersect_host on the FP32 path: 1 replays the query's launches (3 x rounds + 1
+                           kernels and their memsets) from a CUDA graph captured once per (scene, options,
+                           batch-size class) on the context, the ray count read on the device; the records
+                           equal those without it. 0 (default): launched one by one */
 } dmap_options;
 
 /* Fills the defaults above. */
@@ -247,8 +255,9 @@ typedef struct dmap_hit64 {
     int32_t tri, i, j, flags;
 } dmap_hit64;
 /* dmap_hit*.flags bits */
-#define DMAP_HIT_FP64_LEAF 1 /* the root came from the FP64 certified Newton leaf (every hit the library returns) */
+#define DMAP_HIT_FP64_LEAF 1 /* the root is an FP64 Newton root (the FP64 leaf, or an FP32 root polished in FP64) */
 #define DMAP_HIT_CAPPED 2   /* a device iteration cap ran out for this ray */
+#define DMAP_HIT_POLISHED 4 /* an FP32 leaf root refined by FP64 Newton (cond(J) > polish_cond) */
 
 /* Per-ray counters (TraversalStats, displaced_intersector.h:89-105), 8 int64 per ray. */
 #define DMAP_ST_TRIANGLE_TESTS 0

@@ -137,8 +137,9 @@ struct GpuObjectIntersector
     }
 
     // TraversalOptions (traversal_options.h:30-38) in the C ABI's terms: the
-    // FP32 walk (whose hits equal the FP64 walk's) for the Newton leaf, the
-    // FP64 path for the two-triangle leaf, the flat loop's triangle order.
+    // FP32 walk with the FP64 leaf (whose hits equal the FP64 walk's) for the
+    // Newton leaf, the FP64 path for the two-triangle leaf, the flat loop's
+    // triangle order.
     static dmap_options to_c(const TraversalOptions &o)
     {
         dmap_options c;
@@ -149,6 +150,7 @@ struct GpuObjectIntersector
         c.leaf = o.leaf == LeafMode::Newton ? DMAP_LEAF_NEWTON : DMAP_LEAF_TWO_TRIANGLE;
         c.precision = o.leaf == LeafMode::Newton ? DMAP_PRECISION_F32 : DMAP_PRECISION_F64;
         c.order = DMAP_ORDER_INDEX;
+        c.leaf_precision = DMAP_PRECISION_F64;
         return c;
     }
 
