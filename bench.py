@@ -491,7 +491,7 @@ def run_pathtrace(args, rank, world, local, dist):
     w, h, spp = (320, 180, 4) if args.small else (1280, 720, 16)
     view = scenes.path_tracer_view(w, h)
     opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm,
-                              order=args.order)
+                              order=args.order, leaf_precision=args.leaf)
 
     def render(seed):
         return dev.render(view, sc.emitter, spp=spp, max_depth=5, rr_depth=3, seed=seed, options=opt, use_graph=True)
@@ -864,7 +864,7 @@ def run_serve(args, rank, world, local, dist):
 
     rkw = dict(spp=4, max_depth=3, rr_depth=3)
     opt = dm.TraversalOptions(schedule=args.schedule, rounds=args.rounds, blocks_per_sm=args.blocks_per_sm,
-                              order=args.order)
+                              order=args.order, leaf_precision=args.leaf)
     # warm-up: every path once
     srv = dm.Server(ctx, hbm_budget_bytes=120 * 10 ** 9, slots=2, options=opt)
     for k in range(args.warmup):
@@ -910,7 +910,7 @@ def run_serve(args, rank, world, local, dist):
         through the host API (dmap_intersect_host / dmap_render without a
         graph) on the given schedule."""
         popt = dm.TraversalOptions(schedule=schedule, order=args.order, rounds=args.rounds,
-                                   blocks_per_sm=args.blocks_per_sm)
+                                   blocks_per_sm=args.blocks_per_sm, leaf_precision=args.leaf)
         lat, queries = [], 0
         t0 = time.perf_counter()
         for r in trace:
@@ -925,7 +925,7 @@ def run_serve(args, rank, world, local, dist):
                 rays = request_rays(r)
                 d = devs[r["scene"]] if r["kind"] == 0 else d_pt
                 d.intersect(rays, dm.TraversalOptions(schedule=schedule, order=args.order, rounds=args.rounds,
-                                                      blocks_per_sm=args.blocks_per_sm,
+                                                      blocks_per_sm=args.blocks_per_sm, leaf_precision=args.leaf,
                                                       mode="occluded" if r["kind"] == 2 else "closest"), np.float32)
                 queries += len(rays)
             lat.append((time.perf_counter() - t0 - r["t"]) * 1e3)

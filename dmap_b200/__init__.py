@@ -97,6 +97,9 @@ class _UvMap(C.Structure):
 EMITTER_POINT = np.dtype([("u", "<f8"), ("v", "<f8"), ("p", "<f8", 3), ("n", "<f8", 3), ("sqrt_det", "<f8"),
                           ("pdf_uv", "<f8"), ("pdf_area", "<f8"), ("tri", "<i4"), ("draws", "<i4")])
 DESCENT = {"area": 0, "product": 1, "product_geometry": 2}
+EMITTER_LIGHT = np.dtype([("u", "<f8"), ("v", "<f8"), ("y", "<f8", 3), ("n_y", "<f8", 3), ("wi", "<f8", 3),
+                          ("dist", "<f8"), ("pdf_area", "<f8"), ("pdf_omega", "<f8"), ("Le", "<f8"),
+                          ("tri", "<i4"), ("ok", "<i4")])
 
 # dmap_texel_face: triangle, interior, st[3][2]
 TEXEL_FACE = np.dtype([("triangle", np.int32), ("interior", np.int32), ("st", np.float64, (3, 2))])
@@ -165,6 +168,10 @@ def lib() -> C.CDLL:
             "dmap_emitter_pdf": (i32, [vp, vp, vp, vp, i64, vp, vp, vp]),
             "dmap_emitter_sample_host": (i32, [vp, vp, vp, i32, vp, i64, vp]),
             "dmap_emitter_pdf_host": (i32, [vp, vp, vp, vp, i64, vp, vp]),
+            "dmap_emitter_light": (i32, [vp, vp, vp, i64, vp, vp]),
+            "dmap_emitter_light_pdf": (i32, [vp, vp, vp, vp, vp, i64, vp, vp, vp]),
+            "dmap_emitter_light_host": (i32, [vp, vp, vp, i64, vp]),
+            "dmap_emitter_light_pdf_host": (i32, [vp, vp, vp, vp, vp, i64, vp, vp]),
             "dmap_server_create": (i32, [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]),
             "dmap_server_destroy": (None, [vp]),
             "dmap_server_submit_rays": (i32, [vp, vp, vp, i64, i32, vp, C.POINTER(C.c_uint64)]),
@@ -678,6 +685,33 @@ class Emitter:
                                                    None if r is None else r.ctypes.data, len(t), pu.ctypes.data,
                                                    pa.ctypes.data), "dmap_emitter_pdf_host")
         return pu, pa
+
+    def light(self, points, shade) -> np.ndarray:
+        """DisplacedEmitterLight::sample's conversion of sampled points
+        (EMITTER_POINT records, drawn with receivers = shade) seen from
+        shade (n, 6): EMITTER_LIGHT records."""
+        pts = np.ascontiguousarray(points, EMITTER_POINT)
+        sh = np.ascontiguousarray(shade, np.float64).reshape(len(pts), 6)
+        out = np.empty(len(pts), EMITTER_LIGHT)
+        self.ctx.check(lib().dmap_emitter_light_host(self.h, pts.ctypes.data, sh.ctypes.data, len(pts),
+                                                     out.ctypes.data), "dmap_emitter_light_host")
+        return out
+
+    def light_pdf(self, tri, shade, uv=None, wi=None):
+        """Solid-angle pdfs seen from shade (n, 6): at uv (n, 2), or with uv
+        None by the walk of triangle tri along wi (n, 3). Returns (pdf_omega
+        (n,), the (u, v) used (n, 2), NaN on a miss)."""
+        t = np.ascontiguousarray(tri, np.int32)
+        sh = np.ascontiguousarray(shade, np.float64).reshape(len(t), 6)
+        q = None if uv is None else np.ascontiguousarray(uv, np.float64).reshape(len(t), 2)
+        w = None if wi is None else np.ascontiguousarray(wi, np.float64).reshape(len(t), 3)
+        pw, hit = np.empty(len(t)), np.empty((len(t), 2))
+        self.ctx.check(lib().dmap_emitter_light_pdf_host(self.h, t.ctypes.data, sh.ctypes.data,
+                                                         None if q is None else q.ctypes.data,
+                                                         None if w is None else w.ctypes.data, len(t),
+                                                         pw.ctypes.data, hit.ctypes.data),
+                       "dmap_emitter_light_pdf_host")
+        return pw, hit
 
     def close(self):
         if getattr(self, "h", None) and getattr(self.ctx, "h", None):

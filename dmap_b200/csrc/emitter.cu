@@ -17,6 +17,7 @@
 // with the clipped polygon sampled after 32 misses.
 #include "api_internal.h"
 #include "f64_math.cuh"
+#include "f64_walk.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -505,63 +506,193 @@ __global__ void sample_kernel(Emit E, const int32_t *__restrict__ tri_of, const 
     }
 }
 
+// DescentSampler::pdf_uv and pdf_area at (u, v) of triangle tri
+// (descent_sampler.cpp:290-364); 0 outside the footprint.
+__device__ inline void pdf_at(const Emit &E, int tri, double u, double v, const Receiver &rcv, double &pu, double &pa)
+{
+    pu = pa = 0.0;
+    const TriDev &T = E.tris[tri];
+    const AssetDev &g = E.assets[T.asset];
+    const TriEmit &F = E.temit[tri];
+    // pdf_uv / leaf_prob (descent_sampler.cpp:290-356)
+    const int n_leaf = g.n_leaf;
+    const int64_t i = (int64_t)floor(u / (1.0 / n_leaf)), j = (int64_t)floor(v / (1.0 / n_leaf));
+    const int L = F.root_level;
+    const int64_t ri = i >> L, rj = j >> L, di = ri - F.root_i0, dj = rj - F.root_j0;
+    double P = 0.0;
+    FpChild cur = {OUTSIDE, -1, 0.0, 0.0};
+    if (di >= 0 && di <= 1 && dj >= 0 && dj <= 1) {
+        P = 1.0;
+        int64_t pi = 0, pj = 0;
+        for (int level = L + 1; level >= 1; --level) {
+            double p[4];
+            FpChild info[4];
+            child_probs(E, T, g, F, level, pi, pj, cur, rcv, p, info);
+            int c;
+            if (level > L) {
+                c = (int)(di | (dj << 1));
+                pi = ri;
+                pj = rj;
+            } else {
+                int64_t ci = i >> (level - 1), cj = j >> (level - 1);
+                c = (int)((ci - 2 * pi) | ((cj - 2 * pj) << 1));
+                pi = ci;
+                pj = cj;
+            }
+            P *= p[c];
+            cur = info[c];
+            if (P == 0.0)
+                break;
+        }
+    }
+    if (P != 0.0) {
+        pu = P / cur.area;
+        double h;
+        v2 gh;
+        grid_h_grad(g, u, v, h, gh);
+        double sqrt_det;
+        v3 fn;
+        pointwise_metric(T, u, v, h, gh.x, gh.y, sqrt_det, fn);
+        pa = pu / sqrt_det;
+    }
+}
+
 __global__ void pdf_kernel(Emit E, const int32_t *__restrict__ tri_of, const double *__restrict__ uv,
                            const double *__restrict__ recv, int64_t n, int n_tri, double *pdf_uv, double *pdf_area)
 {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int tri = tri_of[k];
         double pu = 0.0, pa = 0.0;
-        if (tri >= 0 && tri < n_tri) {
-            const TriDev &T = E.tris[tri];
-            const AssetDev &g = E.assets[T.asset];
-            const TriEmit &F = E.temit[tri];
-            const Receiver rcv = load_receiver(recv, k);
-            const double u = uv[2 * k], v = uv[2 * k + 1];
-            // pdf_uv / leaf_prob (descent_sampler.cpp:290-356)
-            const int n_leaf = g.n_leaf;
-            const int64_t i = (int64_t)floor(u / (1.0 / n_leaf)), j = (int64_t)floor(v / (1.0 / n_leaf));
-            const int L = F.root_level;
-            const int64_t ri = i >> L, rj = j >> L, di = ri - F.root_i0, dj = rj - F.root_j0;
-            double P = 0.0;
-            FpChild cur = {OUTSIDE, -1, 0.0, 0.0};
-            if (di >= 0 && di <= 1 && dj >= 0 && dj <= 1) {
-                P = 1.0;
-                int64_t pi = 0, pj = 0;
-                for (int level = L + 1; level >= 1; --level) {
-                    double p[4];
-                    FpChild info[4];
-                    child_probs(E, T, g, F, level, pi, pj, cur, rcv, p, info);
-                    int c;
-                    if (level > L) {
-                        c = (int)(di | (dj << 1));
-                        pi = ri;
-                        pj = rj;
-                    } else {
-                        int64_t ci = i >> (level - 1), cj = j >> (level - 1);
-                        c = (int)((ci - 2 * pi) | ((cj - 2 * pj) << 1));
-                        pi = ci;
-                        pj = cj;
-                    }
-                    P *= p[c];
-                    cur = info[c];
-                    if (P == 0.0)
-                        break;
-                }
-            }
-            if (P != 0.0) {
-                pu = P / cur.area;
-                double h;
-                v2 gh;
-                grid_h_grad(g, u, v, h, gh);
-                double sqrt_det;
-                v3 fn;
-                pointwise_metric(T, u, v, h, gh.x, gh.y, sqrt_det, fn);
-                pa = pu / sqrt_det;
-            }
-        }
+        if (tri >= 0 && tri < n_tri)
+            pdf_at(E, tri, uv[2 * k], uv[2 * k + 1], load_receiver(recv, k), pu, pa);
         pdf_uv[k] = pu;
         if (pdf_area)
             pdf_area[k] = pa;
+    }
+}
+
+// ---- DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) ----------
+// The sampler seen from a shading point (p, n): a sample as a direction,
+// distance and solid-angle pdf, and the pdf of a direction from the (u, v)
+// it reaches, directly or by the walk of the emitter's triangle
+// (DisplacedAreaLight::pdf, displaced_area_light.cpp:174-186). The receiver
+// is read by the receiver variant only, as the light passes it.
+constexpr double kMinCosY = 1e-7; // displaced_emitter_light.cpp:16
+
+__device__ inline Receiver shade_receiver(const Emit &E, const double *shade, int64_t k)
+{
+    Receiver R = load_receiver(shade, k);
+    R.on = R.on && E.variant == DMAP_DESCENT_PRODUCT_GEOMETRY;
+    return R;
+}
+
+// EmissionTile::texel (emission_tile.h:71): the level-0 mean, wrapped
+__device__ inline double tile_texel(const TileDev &E, int64_t i, int64_t j)
+{
+    const int64_t m = E.n_leaf;
+    int64_t ri = i % m, rj = j % m;
+    if (ri < 0)
+        ri += m;
+    if (rj < 0)
+        rj += m;
+    return E.mean[E.off[0] + rj * m + ri];
+}
+
+// DisplacedEmitterLight::pdf_omega_from_uv (:103-117)
+__device__ inline double pdf_omega_from_uv(const Emit &E, int tri, v3 p, const Receiver &rcv, double u, double v)
+{
+    double pu, pa;
+    pdf_at(E, tri, u, v, rcv, pu, pa);
+    if (pa <= 0.0)
+        return 0.0;
+    const TriDev &T = E.tris[tri];
+    const AssetDev &g = E.assets[T.asset];
+    double h;
+    v2 gh;
+    grid_h_grad(g, u, v, h, gh);
+    double sqrt_det;
+    v3 fn;
+    pointwise_metric(T, u, v, h, gh.x, gh.y, sqrt_det, fn);
+    v3 y = add3(tri_P(T, u, v), mul3(h, normal_frame_at(T, u, v).N));
+    v3 d = sub3(y, p);
+    double dist2 = dot3(d, d);
+    double cos_y = fabs(dot3(eigen_normalized(fn), div3(d, sqrt(dist2))));
+    if (cos_y < kMinCosY)
+        return 0.0;
+    return pa * dist2 / cos_y;
+}
+
+// DisplacedEmitterLight::sample (:58-90) on points the sampler drew
+__global__ void light_kernel(Emit E, const dmap_emitter_point *__restrict__ pts, const double *__restrict__ shade,
+                             int64_t n, int n_tri, dmap_emitter_light_sample *out)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const dmap_emitter_point s = pts[k];
+        dmap_emitter_light_sample o = {};
+        o.tri = s.tri;
+        if (s.tri >= 0 && s.tri < n_tri && s.draws >= 0) {
+            const double *q = shade + 6 * k;
+            v3 y = V3(s.p[0], s.p[1], s.p[2]), ny = V3(s.n[0], s.n[1], s.n[2]);
+            v3 d = sub3(y, V3(q[0], q[1], q[2]));
+            double dist = sqrt(dot3(d, d));
+            v3 wi = div3(d, dist);
+            double cos_y = fabs(dot3(ny, wi));
+            o.u = s.u;
+            o.v = s.v;
+            o.y[0] = y.x, o.y[1] = y.y, o.y[2] = y.z;
+            o.n_y[0] = ny.x, o.n_y[1] = ny.y, o.n_y[2] = ny.z;
+            o.wi[0] = wi.x, o.wi[1] = wi.y, o.wi[2] = wi.z;
+            o.dist = dist;
+            if (!(cos_y < kMinCosY)) {
+                const TileDev &tile = E.tiles[E.tris[s.tri].asset];
+                o.pdf_area = s.pdf_area;
+                o.pdf_omega = s.pdf_area * dist * dist / cos_y;
+                o.Le = tile_texel(tile, (int64_t)floor(s.u * tile.n_leaf), (int64_t)floor(s.v * tile.n_leaf));
+                o.ok = 1;
+            }
+        }
+        out[k] = o;
+    }
+}
+
+// pdf_omega_from_uv at given (u, v), or (uv NULL) at the crossing of the
+// triangle's walk from p along wi
+__global__ void light_pdf_kernel(Emit E, const int32_t *__restrict__ tri_of, const double *__restrict__ shade,
+                                 const double *__restrict__ uv, const double *__restrict__ wi, int64_t n, int n_tri,
+                                 double *pdf_omega, double *uv_hit)
+{
+    dmapk::QueryOpts opt{}; // TraversalOptions(): both bounds, slab at levels <= 1, the Newton leaf
+    opt.bound = DMAP_BOUND_BOTH;
+    opt.slab_max_level = 1;
+    opt.leaf = DMAP_LEAF_NEWTON;
+    opt.mode = DMAP_MODE_CLOSEST;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int tri = tri_of[k];
+        double pw = 0.0, hu = NAN, hv = NAN;
+        if (tri >= 0 && tri < n_tri) {
+            const double *q = shade + 6 * k;
+            const v3 p = V3(q[0], q[1], q[2]);
+            const Receiver rcv = shade_receiver(E, shade, k);
+            if (uv) {
+                hu = uv[2 * k];
+                hv = uv[2 * k + 1];
+                pw = pdf_omega_from_uv(E, tri, p, rcv, hu, hv);
+            } else {
+                const TriDev &T = E.tris[tri];
+                hit64 h;
+                if (triangle_intersect(T, E.assets[T.asset], p, V3(wi[3 * k], wi[3 * k + 1], wi[3 * k + 2]), 0.0,
+                                       INFINITY, opt, h, nullptr)) {
+                    hu = h.st.x;
+                    hv = h.st.y;
+                    pw = pdf_omega_from_uv(E, tri, p, rcv, hu, hv);
+                }
+            }
+        }
+        pdf_omega[k] = pw;
+        if (uv_hit) {
+            uv_hit[2 * k] = hu;
+            uv_hit[2 * k + 1] = hv;
+        }
     }
 }
 
@@ -798,6 +929,115 @@ dmap_status dmap_emitter_pdf_host(dmap_emitter *e, const int32_t *tri, const dou
     if (r != DMAP_OK)
         return r;
     return sync_and_check(ctx, "dmap_emitter_pdf_host");
+}
+
+
+dmap_status dmap_emitter_light(dmap_emitter *e, const dmap_emitter_point *points_dev, const double *shade_dev,
+                               int64_t n, dmap_emitter_light_sample *out_dev, void *stream)
+{
+    if (!e || n < 0 || (n > 0 && (!points_dev || !shade_dev || !out_dev)))
+        return fail(e ? e->scene->ctx : nullptr, DMAP_ERR_INVALID, "dmap_emitter_light: bad argument");
+    if (n == 0)
+        return DMAP_OK;
+    dmap_context *ctx = e->scene->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    light_kernel<<<grid_for(n), 128, 0, st>>>(emit_of(e), points_dev, shade_dev, n, e->scene->n_tri, out_dev);
+    DMAP_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    return DMAP_OK;
+}
+
+dmap_status dmap_emitter_light_pdf(dmap_emitter *e, const int32_t *tri_dev, const double *shade_dev,
+                                   const double *uv_dev, const double *wi_dev, int64_t n, double *pdf_omega_dev,
+                                   double *uv_hit_dev, void *stream)
+{
+    if (!e || n < 0 || (n > 0 && (!tri_dev || !shade_dev || !pdf_omega_dev || (!uv_dev && !wi_dev))))
+        return fail(e ? e->scene->ctx : nullptr, DMAP_ERR_INVALID, "dmap_emitter_light_pdf: bad argument");
+    if (n == 0)
+        return DMAP_OK;
+    dmap_context *ctx = e->scene->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    light_pdf_kernel<<<grid_for(n), 128, 0, st>>>(emit_of(e), tri_dev, shade_dev, uv_dev, wi_dev, n,
+                                                   e->scene->n_tri, pdf_omega_dev, uv_hit_dev);
+    DMAP_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    return DMAP_OK;
+}
+
+// Host forms: inputs and outputs staged through one stream-ordered block.
+dmap_status dmap_emitter_light_host(dmap_emitter *e, const dmap_emitter_point *points, const double *shade,
+                                    int64_t n, dmap_emitter_light_sample *out)
+{
+    if (!e || n < 0 || (n > 0 && (!points || !shade || !out)))
+        return fail(e ? e->scene->ctx : nullptr, DMAP_ERR_INVALID, "dmap_emitter_light_host: bad argument");
+    if (n == 0)
+        return DMAP_OK;
+    dmap_context *ctx = e->scene->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t a = 256, bp = sizeof(dmap_emitter_point) * n, bs = sizeof(double) * 6 * n,
+                 bo = sizeof(dmap_emitter_light_sample) * n;
+    const size_t os = (bp + a - 1) / a * a, oo = os + (bs + a - 1) / a * a;
+    char *buf = nullptr;
+    DMAP_CUDA(ctx, cudaMallocAsync((void **)&buf, oo + bo, st));
+    dmap_status r = DMAP_OK;
+    cudaError_t er = cudaMemcpyAsync(buf, points, bp, cudaMemcpyHostToDevice, st);
+    if (er == cudaSuccess)
+        er = cudaMemcpyAsync(buf + os, shade, bs, cudaMemcpyHostToDevice, st);
+    if (er != cudaSuccess)
+        r = cuda_fail(ctx, er, "dmap_emitter_light_host: copy");
+    if (r == DMAP_OK)
+        r = dmap_emitter_light(e, (const dmap_emitter_point *)buf, (const double *)(buf + os), n,
+                               (dmap_emitter_light_sample *)(buf + oo), st);
+    if (r == DMAP_OK && (er = cudaMemcpyAsync(out, buf + oo, bo, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        r = cuda_fail(ctx, er, "dmap_emitter_light_host: copy back");
+    cudaFreeAsync(buf, st);
+    if (r != DMAP_OK)
+        return r;
+    return sync_and_check(ctx, "dmap_emitter_light_host");
+}
+
+dmap_status dmap_emitter_light_pdf_host(dmap_emitter *e, const int32_t *tri, const double *shade, const double *uv,
+                                        const double *wi, int64_t n, double *pdf_omega, double *uv_hit)
+{
+    if (!e || n < 0 || (n > 0 && (!tri || !shade || !pdf_omega || (!uv && !wi))))
+        return fail(e ? e->scene->ctx : nullptr, DMAP_ERR_INVALID, "dmap_emitter_light_pdf_host: bad argument");
+    if (n == 0)
+        return DMAP_OK;
+    dmap_context *ctx = e->scene->ctx;
+    DMAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t a = 256, bt = sizeof(int32_t) * n, bs = sizeof(double) * 6 * n,
+                 bu = uv ? sizeof(double) * 2 * n : 0, bw = wi ? sizeof(double) * 3 * n : 0, bp = sizeof(double) * n,
+                 bh = sizeof(double) * 2 * n;
+    auto up = [&](size_t x) { return (x + a - 1) / a * a; };
+    const size_t os = up(bt), ou = os + up(bs), ow = ou + up(bu), op = ow + up(bw), oh = op + up(bp);
+    char *buf = nullptr;
+    DMAP_CUDA(ctx, cudaMallocAsync((void **)&buf, oh + bh, st));
+    dmap_status r = DMAP_OK;
+    cudaError_t er = cudaMemcpyAsync(buf, tri, bt, cudaMemcpyHostToDevice, st);
+    if (er == cudaSuccess)
+        er = cudaMemcpyAsync(buf + os, shade, bs, cudaMemcpyHostToDevice, st);
+    if (er == cudaSuccess && bu)
+        er = cudaMemcpyAsync(buf + ou, uv, bu, cudaMemcpyHostToDevice, st);
+    if (er == cudaSuccess && bw)
+        er = cudaMemcpyAsync(buf + ow, wi, bw, cudaMemcpyHostToDevice, st);
+    if (er != cudaSuccess)
+        r = cuda_fail(ctx, er, "dmap_emitter_light_pdf_host: copy");
+    if (r == DMAP_OK)
+        r = dmap_emitter_light_pdf(e, (const int32_t *)buf, (const double *)(buf + os),
+                                   bu ? (const double *)(buf + ou) : nullptr, bw ? (const double *)(buf + ow) : nullptr,
+                                   n, (double *)(buf + op), (double *)(buf + oh), st);
+    if (r == DMAP_OK && ((er = cudaMemcpyAsync(pdf_omega, buf + op, bp, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                         (uv_hit && (er = cudaMemcpyAsync(uv_hit, buf + oh, bh, cudaMemcpyDeviceToHost, st)) !=
+                                        cudaSuccess)))
+        r = cuda_fail(ctx, er, "dmap_emitter_light_pdf_host: copy back");
+    cudaFreeAsync(buf, st);
+    if (r != DMAP_OK)
+        return r;
+    return sync_and_check(ctx, "dmap_emitter_light_pdf_host");
 }
 
 } // extern "C"

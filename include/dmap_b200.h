@@ -442,6 +442,50 @@ dmap_status dmap_emitter_pdf_host(dmap_emitter *emitter, const int32_t *tri, con
                                   const double *receivers, int64_t n, double *pdf_uv, double *pdf_area);
 
 /*
+ * The displaced emitter as a light seen from shading points
+ * (DisplacedEmitterLight, displaced_emitter_light.cpp:20-117; the light of
+ * an emitter created with variant AREA / PRODUCT / PRODUCT_GEOMETRY is the
+ * reference's AreaDescent / ProductDescent / ReceiverDescent, the last with
+ * emitter_cosine 0 as the reference's light sets it). shade: 6 doubles per
+ * query, the shading point p and its unit normal n.
+ *
+ * dmap_emitter_light replaces DisplacedEmitterLight::sample (:58-90): it
+ * turns the points dmap_emitter_sample drew (with receivers = shade, which
+ * the receiver variant reads) into light samples: direction wi from p to
+ * the point, distance, pdf_area, solid-angle pdf_omega = pdf_area dist^2 /
+ * |n_y . wi|, the emission texel Le; ok = 0 for a draw below the reference's
+ * min |n_y . wi| = 1e-7 (its pdfs and Le are then 0).
+ *
+ * dmap_emitter_light_pdf replaces DisplacedEmitterLight::pdf_omega_from_uv
+ * (:103-117) at uv (2 doubles per query), or with uv NULL the pdf of a
+ * direction by the walk (DisplacedAreaLight::pdf,
+ * displaced_area_light.cpp:174-186, in object space): triangle tri walked
+ * from p along wi (3 doubles per query) with the reference's FP64
+ * DisplacedIntersector::intersect over (0, inf), the pdf at the crossing's
+ * (s, t); 0 on a miss. uv_hit (2 doubles per query, may be NULL) receives
+ * the (u, v) used, NaN on a miss. Asynchronous on stream.
+ */
+typedef struct dmap_emitter_light_sample {
+    double u, v;
+    double y[3], n_y[3]; /* the point and its unit normal */
+    double wi[3];        /* unit direction from the shading point to y */
+    double dist;
+    double pdf_area, pdf_omega, Le;
+    int32_t tri, ok;
+} dmap_emitter_light_sample;
+dmap_status dmap_emitter_light(dmap_emitter *emitter, const dmap_emitter_point *points_dev, const double *shade_dev,
+                               int64_t n, dmap_emitter_light_sample *out_dev, void *stream);
+dmap_status dmap_emitter_light_pdf(dmap_emitter *emitter, const int32_t *tri_dev, const double *shade_dev,
+                                   const double *uv_dev, const double *wi_dev, int64_t n, double *pdf_omega_dev,
+                                   double *uv_hit_dev, void *stream);
+/* The same two on host buffers (synchronous). */
+dmap_status dmap_emitter_light_host(dmap_emitter *emitter, const dmap_emitter_point *points, const double *shade,
+                                    int64_t n, dmap_emitter_light_sample *out);
+dmap_status dmap_emitter_light_pdf_host(dmap_emitter *emitter, const int32_t *tri, const double *shade,
+                                        const double *uv, const double *wi, int64_t n, double *pdf_omega,
+                                        double *uv_hit);
+
+/*
  * Schedule autotuner (no counterpart in the reference). Times the wavefront
  * schedule's launch shapes (rounds x blocks_per_sm) with `base`'s other
  * options on the first min(n, 2^22) of the caller's device rays and returns

@@ -2476,3 +2476,71 @@ double o_emitter_pdf_area(const o_emitter *e, double u, double v, const double *
     pointwise_metric(e->X->tri, u, v, h, gh.x, gh.y, &sqrt_det, &fn);
     return p / sqrt_det;
 }
+
+/* ---- DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) ---------
+ * The descent sampler as a light seen from a shading point (p, n): a sample
+ * converted to a direction, distance and solid-angle pdf, and the pdf of a
+ * direction from the (u, v) it reaches. The light's sampler is the
+ * emitter's: AreaDescent / ProductDescent / ReceiverDescent for variants
+ * 0 / 1 / 2, the receiver read only by the last (whose emitter cosine the
+ * light turns off: create the emitter with emitter_cosine 0). */
+#define O_MIN_COS_Y 1e-7 /* displaced_emitter_light.cpp:16 */
+
+int o_emitter_light_sample(const o_emitter *e, const float *u, int n_u, const double *shade6, double *out16)
+{
+    /* DisplacedEmitterLight::sample (:58-90) */
+    double s[11];
+    o_emitter_sample(e, u, n_u, e->variant == 2 ? shade6 : NULL, s);
+    v3 p = V3(shade6[0], shade6[1], shade6[2]);
+    v3 y = V3(s[2], s[3], s[4]), ny = V3(s[5], s[6], s[7]);
+    v3 d = sub3(y, p);
+    double dist = sqrt(dot3(d, d));
+    v3 wi = div3(d, dist);
+    double cos_y = fabs(dot3(ny, wi));
+    double o[16] = {s[0], s[1], y.x, y.y, y.z, ny.x, ny.y, ny.z, wi.x, wi.y, wi.z, dist, 0.0, 0.0, 0.0, 0.0};
+    if (!(cos_y < O_MIN_COS_Y)) {
+        int n = e->tile.n_leaf;
+        o[12] = s[10];
+        o[13] = s[10] * dist * dist / cos_y;
+        o[14] = tile_mean(&e->tile, 0, (int64_t)floor(s[0] * n), (int64_t)floor(s[1] * n)); /* Le_at, :47-51 */
+        o[15] = 1.0;
+    }
+    memcpy(out16, o, sizeof(o));
+    return o[15] != 0.0;
+}
+
+double o_emitter_light_pdf_uv(const o_emitter *e, const double *shade6, double u, double v)
+{
+    /* DisplacedEmitterLight::pdf_omega_from_uv (:103-117) */
+    double pa = o_emitter_pdf_area(e, u, v, e->variant == 2 ? shade6 : NULL);
+    if (pa <= 0.0)
+        return 0.0;
+    const o_tri *T = e->X->tri;
+    double h = grid_h(e->X->field, u, v);
+    v2 gh = grid_grad(e->X->field, u, v);
+    double sqrt_det;
+    v3 fn;
+    pointwise_metric(T, u, v, h, gh.x, gh.y, &sqrt_det, &fn);
+    v3 y = add3(tri_P(T, u, v), mul3(h, normal_frame_at(T, u, v).N));
+    v3 d = sub3(y, V3(shade6[0], shade6[1], shade6[2]));
+    double dist2 = dot3(d, d);
+    double cos_y = fabs(dot3(eigen_normalized(fn), div3(d, sqrt(dist2))));
+    if (cos_y < O_MIN_COS_Y)
+        return 0.0;
+    return pa * dist2 / cos_y;
+}
+
+double o_emitter_light_pdf_walk(const o_emitter *e, const double *shade6, const double *wi3, double *uv_out)
+{
+    /* the pdf of a direction by its walk (DisplacedAreaLight::pdf,
+     * displaced_area_light.cpp:174-186, in object space): the triangle's
+     * walk from p along wi, then the pdf at the crossing's (s, t) */
+    o_hit h;
+    uv_out[0] = uv_out[1] = NAN;
+    if (!isect_intersect(e->X, V3(shade6[0], shade6[1], shade6[2]), V3(wi3[0], wi3[1], wi3[2]), 0.0, INFINITY, 2, 1,
+                         0, &h, NULL, NULL))
+        return 0.0;
+    uv_out[0] = h.st.x;
+    uv_out[1] = h.st.y;
+    return o_emitter_light_pdf_uv(e, shade6, h.st.x, h.st.y);
+}

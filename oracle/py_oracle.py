@@ -87,6 +87,10 @@ class _Lib:
         self._em_pdf_uv = f("emitter_pdf_uv", C.c_double, C.c_void_p, C.c_double, C.c_double, _dp)
         self._em_pdf_area = f("emitter_pdf_area", C.c_double, C.c_void_p, C.c_double, C.c_double, _dp)
         self._em_leaf_prob = f("emitter_leaf_prob", C.c_double, C.c_void_p, C.c_int64, C.c_int64, _dp)
+        self._em_light_sample = f("emitter_light_sample", C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_int, _dp,
+                                  _dp)
+        self._em_light_pdf_uv = f("emitter_light_pdf_uv", C.c_double, C.c_void_p, _dp, C.c_double, C.c_double)
+        self._em_light_pdf_walk = f("emitter_light_pdf_walk", C.c_double, C.c_void_p, _dp, _dp, _dp)
         if self.prefix == "o_":
             self._sc_isect = f("scene_intersect", C.c_int64, C.c_void_p, _dp, C.c_int64, C.c_int, C.c_int, C.c_int,
                                _dp, _lp, _lp, C.c_int, C.c_int)
@@ -295,3 +299,23 @@ class CpuEmitter:
 
     def leaf_prob(self, i, j, receiver=None):
         return self.lib._em_leaf_prob(self.h, i, j, _ptr(self._recv(receiver)))
+
+    # DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) seen from
+    # shade = (p, n), 6 doubles
+    def light_sample(self, u, shade):
+        """(16 values u, v, y, n_y, wi, dist, pdf_area, pdf_omega, Le, ok)."""
+        uu = np.ascontiguousarray(u, np.float32)
+        out = np.empty(16)
+        self.lib._em_light_sample(self.h, _ptr(uu, C.POINTER(C.c_float)), len(uu),
+                                  _ptr(np.ascontiguousarray(shade, np.float64)), _ptr(out))
+        return out
+
+    def light_pdf_uv(self, shade, u, v):
+        return self.lib._em_light_pdf_uv(self.h, _ptr(np.ascontiguousarray(shade, np.float64)), u, v)
+
+    def light_pdf_walk(self, shade, wi):
+        """(pdf_omega, uv of the walk's crossing, NaN on a miss)."""
+        uv = np.empty(2)
+        pdf = self.lib._em_light_pdf_walk(self.h, _ptr(np.ascontiguousarray(shade, np.float64)),
+                                          _ptr(np.ascontiguousarray(wi, np.float64)), _ptr(uv))
+        return pdf, uv

@@ -7,6 +7,7 @@
 #include "taylor_pyramid.h"
 #include "displaced_tessellation.h"
 #include "descent_sampler.h"
+#include "displaced_emitter_light.h"
 
 #include "../dmap_oracle.h"
 
@@ -415,6 +416,9 @@ struct r_emitter
 {
     std::unique_ptr<dmap::EmissionTile> tile;
     std::unique_ptr<dmap::DescentSampler> s;
+    // the same sampler as the reference's light wrapper builds it
+    std::unique_ptr<dmap::DisplacedEmitterLight> light;
+    const dmap::DisplacedIntersector *X = nullptr;
 };
 
 static dmap::Receiver receiver_of(const double *r)
@@ -440,6 +444,11 @@ r_emitter *r_emitter_create(const r_scene *s, int tri, const double *texels, int
                                            : dmap::DescentWeight::ProductGeometry;
     e->s = std::make_unique<dmap::DescentSampler>(*X->tri, X->field, *X->pyramid, *e->tile, w, beta);
     e->s->emitter_cosine = emitter_cosine != 0;
+    dmap::EmitterSamplerKind kind = variant == 0   ? dmap::EmitterSamplerKind::AreaDescent
+                                    : variant == 1 ? dmap::EmitterSamplerKind::ProductDescent
+                                                   : dmap::EmitterSamplerKind::ReceiverDescent;
+    e->light = std::make_unique<dmap::DisplacedEmitterLight>(*X->tri, X->field, *X->pyramid, *e->tile, kind, beta);
+    e->X = X;
     return e;
 }
 
@@ -489,6 +498,44 @@ double r_emitter_leaf_prob(const r_emitter *e, int64_t i, int64_t j, const doubl
     if (recv)
         r = receiver_of(recv);
     return e->s->leaf_prob(i, j, recv ? &r : nullptr);
+}
+
+// DisplacedEmitterLight::sample (displaced_emitter_light.cpp:58-90) from
+// shade6 = (p, n), its random numbers replayed from u.
+int r_emitter_light_sample(const r_emitter *e, const float *u, int n_u, const double *shade6, double *out16)
+{
+    ks::RNG rng;
+    rng.u = u;
+    rng.n = n_u;
+    dmap::EmitterLightSample s =
+        e->light->sample(vec3d(shade6[0], shade6[1], shade6[2]), vec3d(shade6[3], shade6[4], shade6[5]), rng, nullptr);
+    double v[16] = {s.u, s.v, s.y[0], s.y[1], s.y[2], s.n_y[0], s.n_y[1], s.n_y[2], s.wi[0], s.wi[1], s.wi[2],
+                    s.dist, s.ok ? s.pdf_area : 0.0, s.ok ? s.pdf_omega : 0.0, s.ok ? s.Le : 0.0, s.ok ? 1.0 : 0.0};
+    std::memcpy(out16, v, sizeof(v));
+    return s.ok ? 1 : 0;
+}
+
+// DisplacedEmitterLight::pdf_omega_from_uv (displaced_emitter_light.cpp:103-117).
+double r_emitter_light_pdf_uv(const r_emitter *e, const double *shade6, double u, double v)
+{
+    return e->light->pdf_omega_from_uv(vec3d(shade6[0], shade6[1], shade6[2]),
+                                       vec3d(shade6[3], shade6[4], shade6[5]), u, v);
+}
+
+// DisplacedAreaLight::pdf's walk (displaced_area_light.cpp:174-186) in object
+// space: the triangle's own DisplacedIntersector::intersect from p along wi,
+// then pdf_omega_from_uv at the crossing.
+double r_emitter_light_pdf_walk(const r_emitter *e, const double *shade6, const double *wi3, double *uv_out)
+{
+    dmap::DisplacedHit h;
+    uv_out[0] = uv_out[1] = NAN;
+    if (!e->X->intersect(vec3d(shade6[0], shade6[1], shade6[2]), vec3d(wi3[0], wi3[1], wi3[2]), 0.0, INFINITY,
+                         dmap::TraversalOptions(), h))
+        return 0.0;
+    uv_out[0] = h.st[0];
+    uv_out[1] = h.st[1];
+    return e->light->pdf_omega_from_uv(vec3d(shade6[0], shade6[1], shade6[2]),
+                                       vec3d(shade6[3], shade6[4], shade6[5]), h.st[0], h.st[1]);
 }
 
 } // extern "C"

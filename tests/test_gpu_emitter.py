@@ -87,3 +87,57 @@ def test_emitter_errors(ctx):
     em_area = dm.Emitter(dev64, None, "area")  # uniform emission, area weights
     out = em_area.sample(np.zeros(4, np.int32), np.random.default_rng(1).random((4, 40)).astype(np.float32))
     assert (out["draws"] > 0).all() and (out["pdf_uv"] > 0).all()
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+@pytest.mark.parametrize("variant", ["area", "product", "product_geometry"])
+def test_light_wrapper_equals_oracle(ctx, oracle, name, variant):
+    """The emitter as a light (DisplacedEmitterLight): device light samples,
+    the solid-angle pdf from (u, v) and by the walk of the emitter's triangle
+    (DisplacedAreaLight::pdf) equal the oracle's, which equal the
+    reference's own classes (test_oracle_emitter.py)."""
+    sc = SCENES[name]()
+    tex = _texels(sc, 6)
+    cos = variant != "product_geometry"
+    dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=True)
+    em = dm.Emitter(dev, tex, variant, beta=0.05, emitter_cosine=cos)
+    cpu = py_oracle.CpuScene(oracle, sc)
+    ems = [py_oracle.CpuEmitter(cpu, t, tex[sc.tri_asset[t]], variant, beta=0.05, emitter_cosine=cos)
+           for t in range(cpu.n_tri)]
+    rng = np.random.default_rng(12)
+    per = 40
+    n = per * cpu.n_tri
+    tri = np.repeat(np.arange(cpu.n_tri, dtype=np.int32), per)
+    u = rng.random((n, 96)).astype(np.float32)
+    centre = sc.tris[:, 0:3].mean(axis=0)
+    p = centre + (rng.random((n, 3)) - 0.5) * 3.0
+    nn = rng.normal(size=(n, 3))
+    nn /= np.linalg.norm(nn, axis=1, keepdims=True)
+    shade = np.concatenate([p, nn], axis=1)
+    pts = em.sample(tri, u, shade if variant == "product_geometry" else None)
+    ls = em.light(pts, shade)
+    fields = ("u", "v", "y", "n_y", "wi", "dist", "pdf_area", "pdf_omega", "Le")
+    ok = 0
+    for k in range(n):
+        want = ems[tri[k]].light_sample(u[k], shade[k])
+        got = np.concatenate([np.atleast_1d(ls[k][f]) for f in fields] + [[float(ls[k]["ok"])]])
+        if want[15]:
+            assert np.array_equal(got, want), k
+            ok += 1
+        else:
+            assert ls[k]["ok"] == 0 and np.array_equal(got[:12], want[:12]), k
+    assert ok > n // 2
+    # the solid-angle pdf at the sampled (u, v) and at arbitrary points
+    uv = np.stack([ls["u"], ls["v"]], axis=1)
+    uv[1::2] = rng.random((n // 2, 2)) * 1.2 - 0.1
+    pw, hit = em.light_pdf(tri, shade, uv=uv)
+    want = np.array([ems[tri[k]].light_pdf_uv(shade[k], *uv[k]) for k in range(n)])
+    assert np.array_equal(pw, want)
+    # by the walk along the sampled directions, and along random ones
+    wi = ls["wi"].copy()
+    wi[1::2] = nn[1::2]
+    pw, hit = em.light_pdf(tri, shade, wi=wi)
+    for k in range(n):
+        w_pdf, w_uv = ems[tri[k]].light_pdf_walk(shade[k], wi[k])
+        assert pw[k] == w_pdf and np.array_equal(hit[k], w_uv, equal_nan=True), k
+    assert (pw > 0).sum() > n // 4

@@ -88,3 +88,48 @@ def test_sampler_without_emitter_cosine(oracle, reference):
             a, ka = eo.sample(u, RECV)
             b, kb = er.sample(u, RECV)
             assert ka == kb and np.array_equal(a, b)
+
+
+def _shade_points(rng, n, centre, spread=1.5):
+    """Shading points around a scene with unit normals."""
+    p = centre + (rng.random((n, 3)) - 0.5) * 2.0 * spread
+    nn = rng.normal(size=(n, 3))
+    nn /= np.linalg.norm(nn, axis=1, keepdims=True)
+    return np.concatenate([p, nn], axis=1)
+
+
+@pytest.mark.parametrize("variant", ["area", "product", "product_geometry"])
+def test_light_wrapper_equals_reference(oracle, reference, scene, variant):
+    """DisplacedEmitterLight (displaced_emitter_light.cpp:20-117): light
+    samples seen from shading points, the solid-angle pdf from (u, v), and
+    the pdf of a direction by the walk of the emitter's triangle
+    (DisplacedAreaLight::pdf, displaced_area_light.cpp:174-186), the
+    oracle's restatement against the reference's own classes."""
+    so, sr = py_oracle.CpuScene(oracle, scene), py_oracle.CpuScene(reference, scene)
+    rng = np.random.default_rng(21)
+    cos = variant != "product_geometry"  # the light wrapper turns the receiver variant's emitter cosine off
+    centre = scene.tris[:, 0:3].mean(axis=0)
+    walked = 0
+    for t in range(so.n_tri):
+        tex = _texels(scene.assets[scene.tri_asset[t]].n_leaf, 300 + t)
+        eo = py_oracle.CpuEmitter(so, t, tex, variant, beta=0.05, emitter_cosine=cos)
+        er = py_oracle.CpuEmitter(sr, t, tex, variant, beta=0.05, emitter_cosine=cos)
+        shades = _shade_points(rng, 40, centre)
+        for k, sh in enumerate(shades):
+            u = rng.random(96).astype(np.float32)
+            a, b = eo.light_sample(u, sh), er.light_sample(u, sh)
+            if b[15]:
+                assert np.array_equal(a, b), (t, k)
+                # the pdf of the sampled direction from its (u, v) is the sample's
+                # (the two sides round differently: dist^2 against dist * dist)
+                pu = eo.light_pdf_uv(sh, a[0], a[1])
+                assert pu == er.light_pdf_uv(sh, a[0], a[1]) and abs(pu - a[13]) <= 1e-12 * a[13]
+                pw_o, uv_o = eo.light_pdf_walk(sh, a[8:11])
+                pw_r, uv_r = er.light_pdf_walk(sh, a[8:11])
+                assert pw_o == pw_r and np.array_equal(uv_o, uv_r, equal_nan=True)
+                walked += pw_o > 0.0
+            else:
+                assert a[15] == 0.0 and np.array_equal(a[:12], b[:12])
+            uv = rng.random(2) * 1.2 - 0.1
+            assert eo.light_pdf_uv(sh, *uv) == er.light_pdf_uv(sh, *uv)
+    assert walked > 10
