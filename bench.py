@@ -287,7 +287,7 @@ def main():
                     help="keep --rounds / --blocks-per-sm instead of the autotuner's choice")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--schedule", default="wavefront", choices=["wavefront", "simple"])
-    ap.add_argument("--leaf", default="f64", choices=["f64", "f32"],
+    ap.add_argument("--leaf", default="f32", choices=["f64", "f32"],
                     help="the FP32 path's certified leaf: the reference's FP64 leaf or the FP32 leaf")
     ap.add_argument("--order", default="nearest", choices=["nearest", "index"],
                     help="triangle order: nearest box entry first, or the reference's flat loop")

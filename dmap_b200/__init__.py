@@ -212,7 +212,7 @@ class TraversalOptions:
     blocks_per_sm: int = 5
     order: str = "nearest"
     node_visit_cap: int = 0
-    leaf_precision: str = "f64"
+    leaf_precision: str = "f32"
     graph: bool = False
 
     def c(self) -> _Options:

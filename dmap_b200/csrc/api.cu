@@ -92,7 +92,7 @@ void dmap_options_default(dmap_options *opt)
     opt->blocks_per_sm = 5;
     opt->order = DMAP_ORDER_NEAREST;
     opt->node_visit_cap = 0;
-    opt->leaf_precision = DMAP_PRECISION_F64;
+    opt->leaf_precision = DMAP_PRECISION_F32;
     opt->graph = 0;
 }
 
@@ -655,20 +655,7 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.cluster_tri = s->cluster_tri_dev;
     q.cluster_box = s->cluster_box_dev;
     q.cluster_tree = s->cluster_tree_dev;
-    if (s->op_mask_dev) {
-        if (o.precision == DMAP_PRECISION_F32 && o.schedule == DMAP_SCHEDULE_WAVEFRONT)
-            return fail(ctx, DMAP_ERR_UNSUPPORTED,
-                        "dmap_intersect: a scene with an opacity filter runs DMAP_SCHEDULE_SIMPLE or FP64 precision");
-        q.op_mask = s->op_mask_dev;
-        q.op_tri = s->op_tri_dev;
-        q.op_w = s->op_w;
-        q.op_h = s->op_h;
-        q.op_flip = s->op_map.flip_v;
-        q.op_scale[0] = s->op_map.uv_scale[0];
-        q.op_scale[1] = s->op_map.uv_scale[1];
-        q.op_offset[0] = s->op_map.uv_offset[0];
-        q.op_offset[1] = s->op_map.uv_offset[1];
-    }
+    apply_filter(s, q);
     return DMAP_OK;
 }
 

@@ -138,6 +138,27 @@ inline EncodeTiledFn encode_tiled()
     return fn;
 }
 
+// A scene's opacity filter in a query's options: the mask, the triangles it
+// covers and the uv map; a filtered FP32 query runs the one-thread-per-ray
+// schedule, whose triangle walks take the filter's passes (the wavefront's
+// leaf rounds commit crossings as they find them).
+inline void apply_filter(const dmap_scene *s, dmapk::QueryOpts &q)
+{
+    if (!s->op_mask_dev)
+        return;
+    if (q.precision == DMAP_PRECISION_F32)
+        q.schedule = DMAP_SCHEDULE_SIMPLE;
+    q.op_mask = s->op_mask_dev;
+    q.op_tri = s->op_tri_dev;
+    q.op_w = s->op_w;
+    q.op_h = s->op_h;
+    q.op_flip = s->op_map.flip_v;
+    q.op_scale[0] = s->op_map.uv_scale[0];
+    q.op_scale[1] = s->op_map.uv_scale[1];
+    q.op_offset[0] = s->op_map.uv_offset[0];
+    q.op_offset[1] = s->op_map.uv_offset[1];
+}
+
 inline dmap_status sync_and_check(dmap_context *ctx, const char *what)
 {
     DMAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -270,11 +270,16 @@ __device__ __noinline__ bool accept_root(const TriDev &T, const AssetDev &g, dou
     float fro = R.J00 * R.J00 + R.J01 * R.J01 + R.J10 * R.J10 + R.J11 * R.J11;
     float det = fabsf(R.J00 * R.J11 - R.J01 * R.J10);
     if (fro > (float)polish_cond * det) { // cond(J) <= |J|_F^2 / |det J|
+        // the reference's Newton from the FP32 root, its t judged here: a
+        // root at or beyond t_max is the one the search already holds (found
+        // again from another start) or a farther one
         hit64 h;
         int64_t it = 0;
-        bool ok = newton_from(T, g, o, d, t_min, t_max, i, j, st, h, it);
+        bool ok = newton_from(T, g, o, d, t_min, INFINITY, i, j, st, h, it);
         iters += it;
         if (ok) {
+            if (h.t >= t_max)
+                return false;
             hit = h;
             flags = DMAP_HIT_FP64_LEAF | DMAP_HIT_POLISHED;
             return true;

@@ -401,8 +401,6 @@ dmap_status render_begin(dmap_scene *s, const dmap_render_desc *desc, const dmap
         return fail(ctx, DMAP_ERR_INVALID, "dmap_render: non-finite camera, emitter or material");
     if (record && record->capacity > 0 && (!record->rays || !record->kind || !record->tri || !record->t))
         return fail(ctx, DMAP_ERR_INVALID, "dmap_render: record buffers missing");
-    if (s->op_mask_dev)
-        return fail(ctx, DMAP_ERR_UNSUPPORTED, "dmap_render: the path tracer does not run a scene's opacity filter");
     dmapk::QueryOpts q;
     dmap_status st = check_query(s, DMAP_F32, 0, opt, DMAP_F32, q);
     if (st != DMAP_OK)

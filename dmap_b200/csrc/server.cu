@@ -238,6 +238,7 @@ struct dmap_server
             qq.cluster_box = first->scene->cluster_box_dev;
             qq.cluster_tree = first->scene->cluster_tree_dev;
             qq.ray_dtype = qq.hit_dtype = 0;
+            apply_filter(first->scene, qq); // a filtered scene's batch runs the filter's passes
             dmap_scene *s = first->scene;
             if (e == cudaSuccess)
                 e = dmapk::launch_walk32(s->tris32_dev, s->tris_dev, s->n_tri, s->assets_dev, sl.rays_d, at, qq,
@@ -466,8 +467,6 @@ dmap_status dmap_server_submit_rays(dmap_server *S, dmap_scene *scene, const flo
     if (!S || !scene || !id || n < 0 || (n > 0 && (!rays_host || !hits_host)) ||
         (mode != DMAP_MODE_CLOSEST && mode != DMAP_MODE_OCCLUDED) || scene->ctx != S->ctx)
         return DMAP_ERR_INVALID;
-    if (scene->op_mask_dev) // the server's wavefront launches do not run the filter
-        return DMAP_ERR_UNSUPPORTED;
     auto r = std::make_unique<Request>();
     r->kind = Kind::Rays;
     r->scene = scene;
@@ -497,8 +496,6 @@ dmap_status dmap_server_submit_render(dmap_server *S, dmap_scene *scene, const d
 {
     if (!S || !scene || !desc || !rgb_host || !id || scene->ctx != S->ctx)
         return DMAP_ERR_INVALID;
-    if (scene->op_mask_dev)
-        return DMAP_ERR_UNSUPPORTED;
     const dmap_camera &C = desc->camera;
     if (C.width <= 0 || C.height <= 0 || desc->spp <= 0 || desc->max_depth < 1)
         return DMAP_ERR_INVALID;

@@ -185,8 +185,8 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *o
 #define DMAP_LEAF_TWO_TRIANGLE 1
 #define DMAP_PRECISION_F64 0 /* the reference's double arithmetic, operation for operation */
 /* FP32 walk, bounds widened outward so it admits every cell the FP64 walk
- * admits; each leaf cell re-tested and its leaf run in FP64 with the
- * reference's arithmetic, so every hit equals the FP64 path's */
+ * admits; each leaf cell re-tested with the reference's FP64 node test, its
+ * leaf run in the precision dmap_options.leaf_precision selects */
 #define DMAP_PRECISION_F32 1
 #define DMAP_MODE_CLOSEST 0  /* closest hit in (t_min, t_max): rtcIntersect1 / intersect_callback */
 #define DMAP_MODE_OCCLUDED 1 /* any hit in (t_min, t_max): rtcOccluded1 / occluded_callback */
@@ -227,10 +227,11 @@ typedef struct dmap_options {
                            2^26, far above any walk of a well-formed scene). A ray whose walk gives up keeps
                            what it found, its hit record gets DMAP_HIT_CAPPED, and the call reports
                            DMAP_ERR_LIMIT */
-    int leaf_precision; /* FP32 path's certified leaf: DMAP_PRECISION_F64 (default: the reference's leaf in
-                           double, every hit equal to the FP64 path's bit for bit) or DMAP_PRECISION_F32
-                           (the leaf's search and Newton in FP32 with outward-rounded sub-square bounds, FP64
-                           Newton polish above polish_cond; hits within the FP32 leaf's tolerance) */
+    int leaf_precision; /* FP32 path's certified leaf: DMAP_PRECISION_F32 (default: the leaf's search and
+                           Newton in FP32 with outward-rounded sub-square bounds, FP64 Newton polish above
+                           polish_cond; the same hit set, t within 1e-5 of the scene extent) or
+                           DMAP_PRECISION_F64 (the reference's leaf in double: every hit equal to the FP64
+                           path's bit for bit, as the drop-in adapters set it) */
     int graph;          /* dmap_intersect_host on the FP32 path: 1 replays the query's launches (3 x rounds + 1
                            kernels and their memsets) from a CUDA graph captured once per (scene, options,
                            batch-size class) on the context, the ray count read on the device; the records
@@ -325,10 +326,9 @@ dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, d
  * tri_flags_host (n_tri bytes, NULL = every triangle) marks the triangles
  * the map covers (the object whose material carries it); the others accept
  * every crossing. mask_host NULL removes the filter. The mask is copied.
- * Queries on a filtered scene run the one-thread-per-ray schedules
- * (DMAP_PRECISION_F64, or DMAP_PRECISION_F32 with DMAP_SCHEDULE_SIMPLE);
- * the wavefront schedule, dmap_render and the server return
- * DMAP_ERR_UNSUPPORTED for it. While a server holds requests on the scene
+ * FP32 queries on a filtered scene (dmap_intersect*, dmap_render and
+ * the server alike) run the one-thread-per-ray schedule, whose triangle
+ * walks take the filter's passes, whatever schedule the options name. While a server holds requests on the scene
  * (queued or running), the filter cannot change: this call returns
  * DMAP_ERR_NOT_READY until they are done (dmap_server_drain); do not call it
  * concurrently with a submit on the same scene.

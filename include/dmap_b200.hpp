@@ -55,6 +55,9 @@ struct TraversalOptions
     // false: ObjectIntersector's flat loop, triangles in index order (the
     // drop-in default); true: nearest box entry first (DMAP_ORDER_NEAREST)
     bool nearest = false;
+    // false: the reference's FP64 certified leaf, every hit the reference's
+    // (the drop-in default); true: the FP32 leaf (hits within its tolerance)
+    bool fp32_leaf = false;
 
     dmap_options c() const
     {
@@ -65,6 +68,7 @@ struct TraversalOptions
         o.leaf = (int)leaf;
         o.precision = fp64 || leaf == LeafMode::TwoTriangle ? DMAP_PRECISION_F64 : DMAP_PRECISION_F32;
         o.order = nearest ? DMAP_ORDER_NEAREST : DMAP_ORDER_INDEX;
+        o.leaf_precision = fp32_leaf ? DMAP_PRECISION_F32 : DMAP_PRECISION_F64;
         return o;
     }
 };

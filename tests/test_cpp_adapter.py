@@ -47,7 +47,7 @@ def test_adapter_answers_equal_python_binding(tmp_path):
     out = np.fromfile(tmp_path / "o.f64").reshape(-1, 12)
     ctx = dm.Context(0)
     dev = dm.Scene.from_synthetic(ctx, sc)
-    h = dev.intersect(rays, dm.TraversalOptions(order="index"), np.float64)  # the adapter's flat-loop default
+    h = dev.intersect(rays, dm.TraversalOptions(order="index", leaf_precision="f64"), np.float64)  # the adapter's flat-loop default
     hit = h["tri"] >= 0
     assert hit.sum() > 100
     assert np.array_equal(out[:, 1].astype(np.int32), h["tri"])

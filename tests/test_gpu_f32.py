@@ -21,7 +21,7 @@ def ctx():
 
 def _check(cpu, dev, rays, bound="both", k=1, order="nearest", **kw):
     ho, so = cpu.intersect(rays, bound, k, stats=True, order=order)
-    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, precision="f32", order=order, **kw), np.float64,
+    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, precision="f32", order=order, **kw, leaf_precision="f64"), np.float64,
                            stats=True)
     assert np.array_equal(hd["tri"] >= 0, ho[:, 10] >= 0), "hit/miss set differs"
     hit = ho[:, 10] >= 0
@@ -69,8 +69,8 @@ def test_f32_schedules_agree_bitwise(ctx, oracle):
     sc = helpers.small_sphere(32)
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
     rays = np.concatenate([scenes.sphere_camera_rays(64, 36), helpers.near_surface_rays(cpu, 1500)])
-    a, sa = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront"), np.float64, stats=True)
-    b, sb = dev.intersect(rays, dm.TraversalOptions(schedule="simple"), np.float64, stats=True)
+    a, sa = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", leaf_precision="f64"), np.float64, stats=True)
+    b, sb = dev.intersect(rays, dm.TraversalOptions(schedule="simple", leaf_precision="f64"), np.float64, stats=True)
     assert np.array_equal(a["tri"], b["tri"])
     hit = a["tri"] >= 0
     assert np.array_equal(a["t"][hit], b["t"][hit]) and np.array_equal(a["ng"][hit], b["ng"][hit])
@@ -106,7 +106,7 @@ def test_f32_never_miss(ctx, oracle):
     sc = helpers.small_sphere(32)
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
     rays, t_s, miss_dist, _ = helpers.aimed_rays(cpu, 4000, seed=91)
-    h = dev.intersect(rays, dm.TraversalOptions(precision="f32"))
+    h = dev.intersect(rays, dm.TraversalOptions(precision="f32", leaf_precision="f64"))
     ok = miss_dist < 1e-6
     assert (h["tri"][ok] >= 0).all()
 
@@ -117,7 +117,7 @@ def test_f32_occluded(ctx, oracle):
     rays = helpers.near_surface_rays(cpu, 3000)
     rays[:, 7] = np.where(np.arange(len(rays)) % 2 == 0, 1.0, np.inf)
     ho, _ = cpu.intersect(rays)
-    h = dev.intersect(rays, dm.TraversalOptions(precision="f32", mode="occluded"))
+    h = dev.intersect(rays, dm.TraversalOptions(precision="f32", mode="occluded", leaf_precision="f64"))
     assert np.array_equal(h["tri"] >= 0, ho[:, 10] >= 0)
 
 
@@ -151,8 +151,8 @@ def test_f32_many_triangles_block_mask(ctx, oracle, n, k):
     for order in ("nearest", "index"):
         n_hit, _ = _check(cpu, dev, rays, order=order)
         assert n_hit > 1000
-        a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", order=order), np.float64)
-        b = dev.intersect(rays, dm.TraversalOptions(schedule="simple", order=order), np.float64)
+        a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", order=order, leaf_precision="f64"), np.float64)
+        b = dev.intersect(rays, dm.TraversalOptions(schedule="simple", order=order, leaf_precision="f64"), np.float64)
         assert a.tobytes() == b.tobytes()
 
 
@@ -170,8 +170,8 @@ def test_f32_many_triangles_block_tree(ctx, oracle, k):
     for order in ("nearest", "index"):
         n_hit, _ = _check(cpu, dev, rays, order=order)
         assert n_hit > 1000
-        a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", order=order), np.float64)
-        b = dev.intersect(rays, dm.TraversalOptions(schedule="simple", order=order), np.float64)
+        a = dev.intersect(rays, dm.TraversalOptions(schedule="wavefront", order=order, leaf_precision="f64"), np.float64)
+        b = dev.intersect(rays, dm.TraversalOptions(schedule="simple", order=order, leaf_precision="f64"), np.float64)
         assert a.tobytes() == b.tobytes()
-    occ = dev.intersect(rays, dm.TraversalOptions(mode="occluded"), np.float64)
+    occ = dev.intersect(rays, dm.TraversalOptions(mode="occluded", leaf_precision="f64"), np.float64)
     assert np.array_equal(occ["tri"] >= 0, a["tri"] >= 0)

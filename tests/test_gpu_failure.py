@@ -60,7 +60,7 @@ def test_unanswerable_rays_are_misses(world, path, mode):
     good = np.setdiff1d(np.arange(len(mixed)), slots)
     mixed[slots] = bad
     mixed[good] = rays
-    opt = dm.TraversalOptions(mode=mode, **path)
+    opt = dm.TraversalOptions(mode=mode, **path, leaf_precision="f64")
     h_mixed = dev.intersect(mixed, opt)
     h_alone = dev.intersect(rays, opt)
     assert (h_mixed["tri"][slots] == -1).all() and np.isinf(h_mixed["t"][slots]).all()
@@ -78,7 +78,7 @@ def test_degenerate_t_range_is_a_miss(world):
     r = rays[:64].copy()
     r[:, 6], r[:, 7] = 2.0, 1.0   # t_min > t_max: nothing to find
     for path in PATHS:
-        h = dev.intersect(r, dm.TraversalOptions(**path))
+        h = dev.intersect(r, dm.TraversalOptions(**path, leaf_precision="f64"))
         assert (h["tri"] == -1).all()
 
 
@@ -101,10 +101,10 @@ def test_walk_cap_runs_out_and_flags_its_rays(world, schedule):
     away[:, 0], away[:, 3], away[:, 7] = 10.0, 1.0, np.inf
     rays = np.ascontiguousarray(np.concatenate([rays, away]), np.float32)
     base = dict(precision="f32", schedule=schedule, rounds=3, blocks_per_sm=4)
-    st0, full = _raw_intersect(dev, rays, dm.TraversalOptions(**base))
+    st0, full = _raw_intersect(dev, rays, dm.TraversalOptions(**base, leaf_precision="f64"))
     assert st0 == 0
     assert not (full["flags"] & dm.HIT_CAPPED).any()
-    st, capped = _raw_intersect(dev, rays, dm.TraversalOptions(node_visit_cap=6, **base))
+    st, capped = _raw_intersect(dev, rays, dm.TraversalOptions(node_visit_cap=6, **base, leaf_precision="f64"))
     assert st == 6  # DMAP_ERR_LIMIT
     flagged = (capped["flags"] & dm.HIT_CAPPED) != 0
     assert flagged.sum() > len(rays) // 2 and not flagged[-16:].any()
@@ -112,11 +112,11 @@ def test_walk_cap_runs_out_and_flags_its_rays(world, schedule):
     keep = ~flagged
     assert np.array_equal(capped[keep].tobytes(), full[keep].tobytes())
     # the context is usable again, and the status does not stick
-    st2, again = _raw_intersect(dev, rays, dm.TraversalOptions(**base))
+    st2, again = _raw_intersect(dev, rays, dm.TraversalOptions(**base, leaf_precision="f64"))
     assert st2 == 0 and np.array_equal(again.tobytes(), full.tobytes())
 
 
 def test_negative_cap_is_rejected(world):
     ctx, cpu, dev, rays = world
-    st, _ = _raw_intersect(dev, np.ascontiguousarray(rays[:8], np.float32), dm.TraversalOptions(node_visit_cap=-1))
+    st, _ = _raw_intersect(dev, np.ascontiguousarray(rays[:8], np.float32), dm.TraversalOptions(node_visit_cap=-1, leaf_precision="f64"))
     assert st == 1  # DMAP_ERR_INVALID

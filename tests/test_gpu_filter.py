@@ -31,7 +31,7 @@ def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, or
     so.set_opacity(m, scale, off, flip, flags)
     dev.set_opacity(m, scale, off, flip, flags)
     ho, _ = so.intersect(rays, order=order)
-    opt = dm.TraversalOptions(precision=precision, schedule="simple", order=order)
+    opt = dm.TraversalOptions(precision=precision, schedule="simple", order=order, leaf_precision="f64")
     hd = dev.intersect(rays, opt, np.float64)
     hit = ho[:, 10] >= 0
     assert hit.sum() > 100
@@ -46,7 +46,7 @@ def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, or
     assert (so.intersect(rays, order=order)[0][:, 10] != ho[:, 10]).sum() > 20
     # occlusion through the filter: occluded exactly where the filtered closest query hits
     occ = dev.intersect(rays, dm.TraversalOptions(precision=precision, schedule="simple", order=order,
-                                                  mode="occluded"), np.float64)
+                                                  mode="occluded", leaf_precision="f64"), np.float64)
     assert np.array_equal(occ["tri"] >= 0, hit)
     # the filter removed: the device query is the unfiltered one again
     dev.set_opacity(None)
@@ -54,28 +54,36 @@ def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, or
     assert np.array_equal(dev.intersect(rays, opt, np.float64)["tri"], h0[:, 10].astype(np.int32))
 
 
-def test_filtered_scene_refusals(ctx):
+def test_filtered_scene_on_every_path(ctx):
+    """A filtered scene runs its filter's passes on every path: a wavefront
+    query takes the one-thread-per-ray schedule (the filter's), the server
+    serves it, the path tracer renders it; each equals the explicit simple
+    schedule's answer."""
     sc = scenes.quad_scene(16)
     dev = dm.Scene.from_synthetic(ctx, sc)
-    rays = scenes.quad_camera_rays(8, 8)
+    rays = scenes.quad_camera_rays(24, 24)
     dev.set_opacity(checker(4))
-    with pytest.raises(dm.DmapError) as e:
-        dev.intersect(rays, dm.TraversalOptions(), np.float64)  # the FP32 wavefront schedule
-    assert e.value.status == dm.ERR_UNSUPPORTED
-    dev.intersect(rays, dm.TraversalOptions(schedule="simple"), np.float64)
-    srv = dm.Server(ctx, max_batch_rays=1024, slots=1)
-    with pytest.raises(dm.DmapError) as e:
-        srv.submit_rays(dev, rays)
-    assert e.value.status == dm.ERR_UNSUPPORTED
+    simple = dev.intersect(rays, dm.TraversalOptions(schedule="simple", leaf_precision="f64"), np.float32)
+    wave = dev.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), np.float32)
+    assert wave.tobytes() == simple.tobytes()
+    unfiltered = dm.Scene.from_synthetic(ctx, sc).intersect(rays, dm.TraversalOptions(leaf_precision="f64"),
+                                                             np.float32)
+    assert (unfiltered["tri"] != simple["tri"]).sum() > 10  # the filter culled crossings
+    srv = dm.Server(ctx, max_batch_rays=1024, slots=1, options=dm.TraversalOptions(leaf_precision="f64"))
+    rid, out = srv.submit_rays(dev, rays)
+    assert srv.wait(rid, 60.0) == 0
+    assert out.tobytes() == simple.tobytes()
+    srv.close()
     pt = scenes.with_ground_and_emitter(helpers.small_sphere(16, patches=(0,)), 16)
     dpt = dm.Scene.from_synthetic(ctx, pt)
     dpt.set_opacity(checker(4))
-    with pytest.raises(dm.DmapError) as e:
-        dpt.render(scenes.path_tracer_view(8, 8), pt.emitter, options=dm.TraversalOptions(schedule="simple"))
-    assert e.value.status == dm.ERR_UNSUPPORTED
+    view = scenes.path_tracer_view(16, 12)
+    a, sa, _ = dpt.render(view, pt.emitter, options=dm.TraversalOptions(leaf_precision="f64"))
+    b, sb, _ = dpt.render(view, pt.emitter, options=dm.TraversalOptions(schedule="simple", leaf_precision="f64"))
+    assert np.array_equal(a, b) and sa["extension_rays"] == sb["extension_rays"]
     for bad in (dict(mask=np.zeros((0, 3), np.uint8)), dict(mask=checker(4), uv_scale=(0.0, 1.0)),
                 dict(mask=checker(4), uv_scale=(np.inf, 1.0))):
         with pytest.raises((dm.DmapError, ValueError)):
             dev.set_opacity(**bad)
     dev.set_opacity(None)
-    dev.intersect(rays, dm.TraversalOptions(), np.float64)
+    dev.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), np.float64)

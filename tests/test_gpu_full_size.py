@@ -63,7 +63,7 @@ def test_quad_512_all_camera_rays(oracle):
     cpu = py_oracle.CpuScene(oracle, sc)
     for order in ("index", "nearest"):
         ho, _ = cpu.intersect(rays, order=order, threads=THREADS)
-        h = dev.intersect(rays, dm.TraversalOptions(precision="f32", order=order))
+        h = dev.intersect(rays, dm.TraversalOptions(precision="f32", order=order, leaf_precision="f64"))
         n = _equal_records(h, ho, f"quad 512, {order} order")
         assert n > 20000  # the 45 degree view sees the quad in about a third of its pixels
     _release(ctx, dev)
@@ -77,7 +77,7 @@ def sphere():
 def _bench_rays(dev, prim):
     """The benchmark's ray list: primaries, then one bounce per primary hit
     from the FP64 path's hits in the flat loop's order."""
-    h0 = dev.intersect(prim, dm.TraversalOptions(precision="f64", order="index"))
+    h0 = dev.intersect(prim, dm.TraversalOptions(precision="f64", order="index", leaf_precision="f64"))
     hit = h0["tri"] >= 0
     bounce = scenes.bounce_rays(prim[hit], h0["t"][hit], h0["ng"][hit])
     return np.concatenate([prim, bounce]).astype(np.float32), int(hit.sum())
@@ -91,8 +91,8 @@ def test_sphere_2048_benchmark_rays(oracle, sphere):
     assert len(rays) == len(prim) + n_prim_hits
     # every ray: the product path (both orders) equals the FP64 device path
     for order in ("nearest", "index"):
-        h32 = dev.intersect(rays, dm.TraversalOptions(precision="f32", order=order))
-        h64 = dev.intersect(rays, dm.TraversalOptions(precision="f64", order=order))
+        h32 = dev.intersect(rays, dm.TraversalOptions(precision="f32", order=order, leaf_precision="f64"))
+        h64 = dev.intersect(rays, dm.TraversalOptions(precision="f64", order=order, leaf_precision="f64"))
         assert np.array_equal(h32["tri"], h64["tri"]), f"{order}: FP32 and FP64 hit sets differ"
         hit = h64["tri"] >= 0
         for f in FIELDS:
@@ -100,7 +100,7 @@ def test_sphere_2048_benchmark_rays(oracle, sphere):
     # a stride sample through the CPU oracle's flat loop over all 96 patches
     sample = np.ascontiguousarray(rays[::97])
     ho = helpers.oracle_flat_loop_by_groups(oracle, sphere, sample, group=16, threads=THREADS)
-    h = dev.intersect(sample, dm.TraversalOptions(precision="f32", order="index"))
+    h = dev.intersect(sample, dm.TraversalOptions(precision="f32", order="index", leaf_precision="f64"))
     n = _equal_records(h, ho, "sphere 96 x 2048^2")
     assert n > len(sample) // 4 and len(sample) > 25000
     _release(ctx, dev)
@@ -114,7 +114,7 @@ def test_sphere_2048_f16_grazing_rays(oracle, sphere):
     dev = dm.Scene.from_synthetic(ctx, sc16)
     p, m = scenes.base_points(sc16, 60_000, seed=scenes.SEED + 7)
     rays = scenes.grazing_rays(p, m, seed=scenes.SEED + 8)
-    h = dev.intersect(rays, dm.TraversalOptions(precision="f32", order="index"))
+    h = dev.intersect(rays, dm.TraversalOptions(precision="f32", order="index", leaf_precision="f64"))
     ho = helpers.oracle_flat_loop_by_groups(oracle, sc16, rays, group=16, threads=THREADS)
     n = _equal_records(h, ho, "sphere 96 x 2048^2 FP16, grazing")
     # rays aimed at the base surface mostly find the displaced one

@@ -58,8 +58,8 @@ def test_instance_equals_object_space(world):
         local = rays.copy()
         local[:, 0:3] = (rays[:, 0:3] - t) @ R     # R^T (o - t)
         local[:, 3:6] = rays[:, 3:6] @ R           # R^T d
-        hw = inst.intersect(rays, dm.TraversalOptions(), np.float64)
-        ho = obj.intersect(local, dm.TraversalOptions(), np.float64)
+        hw = inst.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), np.float64)
+        ho = obj.intersect(local, dm.TraversalOptions(leaf_precision="f64"), np.float64)
         hit = ho["tri"] >= 0
         assert hit.sum() > 500
         same = (hw["tri"] >= 0) == hit
@@ -81,12 +81,12 @@ def test_instances_take_the_nearest(world):
     inst = dm.Scene.instanced(ctx, assets, sc.tris, sc.tri_asset, [0, n_tri], [0, 0, 0], M)
     assert inst.n_tri == 3 * n_tri
     rays = np.concatenate([_rays_at(sc, m, 1000, 2 + k) for k, m in enumerate(Ms)])
-    h = inst.intersect(rays, dm.TraversalOptions(), np.float64)
+    h = inst.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), np.float64)
     best_t = np.full(len(rays), np.inf)
     best_tri = np.full(len(rays), -1)
     for k, m in enumerate(Ms):
         one = dm.Scene.instanced(ctx, assets, sc.tris, sc.tri_asset, [0, n_tri], [0], m)
-        hk = one.intersect(rays, dm.TraversalOptions(), np.float64)
+        hk = one.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), np.float64)
         closer = (hk["tri"] >= 0) & (hk["t"] < best_t)
         best_t[closer] = hk["t"][closer]
         best_tri[closer] = hk["tri"][closer] + k * n_tri

@@ -69,7 +69,7 @@ def test_device_pyramid_bf16_equals_oracle(ctx, oracle, build):
 
 def _compare(cpu, dev, rays, bound="both", k=1, leaf="newton", order="nearest"):
     ho, so = cpu.intersect(rays, bound, k, leaf, stats=True, order=order)
-    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, leaf, precision="f64", order=order), np.float64,
+    hd, sd = dev.intersect(rays, dm.TraversalOptions(bound, k, leaf, precision="f64", order=order, leaf_precision="f64"), np.float64,
                            stats=True)
     assert np.array_equal(hd["tri"], ho[:, 10].astype(np.int32))
     hit = ho[:, 10] >= 0
@@ -132,7 +132,7 @@ def test_f64_float64_rays(sphere_pair):
     rays = helpers.near_surface_rays(cpu, 500).astype(np.float64)
     rays[:, 0:3] += 1e-9  # not representable in float32
     ho, _ = cpu.intersect(rays)
-    hd = dev.intersect(rays, dm.TraversalOptions(precision="f64"), np.float64)
+    hd = dev.intersect(rays, dm.TraversalOptions(precision="f64", leaf_precision="f64"), np.float64)
     assert np.array_equal(hd["t"], ho[:, 0])
 
 
@@ -142,8 +142,8 @@ def test_f64_occluded_matches_closest(sphere_pair):
     cpu, dev = sphere_pair
     rays = np.concatenate([scenes.sphere_camera_rays(48, 27), helpers.near_surface_rays(cpu, 800)])
     rays[:, 7] = np.where(np.arange(len(rays)) % 2 == 0, 2.0, np.inf)
-    closest = dev.intersect(rays, dm.TraversalOptions(precision="f64"))
-    occl = dev.intersect(rays, dm.TraversalOptions(precision="f64", mode="occluded"))
+    closest = dev.intersect(rays, dm.TraversalOptions(precision="f64", leaf_precision="f64"))
+    occl = dev.intersect(rays, dm.TraversalOptions(precision="f64", mode="occluded", leaf_precision="f64"))
     assert np.array_equal(closest["tri"] >= 0, occl["tri"] >= 0)
 
 
@@ -174,7 +174,7 @@ def test_direct_build_walk_equals_oracle(ctx, oracle):
     rays = np.concatenate([scenes.quad_camera_rays(48, 48), helpers.near_surface_rays(cpu, 1500)])
     _compare(cpu, dev, rays)
     ho, _ = cpu.intersect(rays)
-    h32 = dev.intersect(rays, dm.TraversalOptions(precision="f32"), np.float64)
+    h32 = dev.intersect(rays, dm.TraversalOptions(precision="f32", leaf_precision="f64"), np.float64)
     assert np.array_equal(h32["tri"], ho[:, 10].astype(np.int32))
     hit = ho[:, 10] >= 0
     assert np.array_equal(h32["t"][hit], ho[hit, 0])

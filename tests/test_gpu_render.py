@@ -13,6 +13,8 @@ import py_oracle
 
 pytestmark = pytest.mark.gpu
 
+F64_LEAF = dm.TraversalOptions(leaf_precision="f64")  # replayed hits equal the oracle's bit for bit
+
 VIEW = scenes.path_tracer_view(48, 27)
 
 
@@ -27,7 +29,7 @@ def pt(oracle):
 
 def test_render_ray_replay(pt):
     sc, ctx, dev, cpu = pt
-    img, st, rec = dev.render(VIEW, sc.emitter, spp=2, record=200_000)
+    img, st, rec = dev.render(VIEW, sc.emitter, spp=2, record=200_000, options=F64_LEAF)
     assert rec["count"] == st["extension_rays"] + st["shadow_rays"] == len(rec["kind"])
     assert st["paths"] == 2 * VIEW["width"] * VIEW["height"]
     rays = rec["rays"].astype(np.float64)
@@ -50,10 +52,10 @@ def test_render_ray_replay(pt):
 def test_render_invariant_to_batching_graph_and_schedule(pt):
     sc, ctx, dev, cpu = pt
     wh = VIEW["width"] * VIEW["height"]
-    a, sa, _ = dev.render(VIEW, sc.emitter, spp=4, use_graph=True)
-    b, sb, _ = dev.render(VIEW, sc.emitter, spp=4, use_graph=False, paths_per_batch=wh)
-    c, sc_, _ = dev.render(VIEW, sc.emitter, spp=4, use_graph=True, paths_per_batch=2 * wh)
-    d, sd, _ = dev.render(VIEW, sc.emitter, spp=4, options=dm.TraversalOptions(schedule="simple"))
+    a, sa, _ = dev.render(VIEW, sc.emitter, spp=4, use_graph=True, options=F64_LEAF)
+    b, sb, _ = dev.render(VIEW, sc.emitter, spp=4, use_graph=False, paths_per_batch=wh, options=F64_LEAF)
+    c, sc_, _ = dev.render(VIEW, sc.emitter, spp=4, use_graph=True, paths_per_batch=2 * wh, options=F64_LEAF)
+    d, sd, _ = dev.render(VIEW, sc.emitter, spp=4, options=dm.TraversalOptions(schedule="simple", leaf_precision="f64"))
     assert sa["batches"] == 1 and sb["batches"] == 4 and sc_["batches"] == 2
     for img, st in ((b, sb), (c, sc_), (d, sd)):
         assert np.array_equal(a, img)
@@ -62,13 +64,13 @@ def test_render_invariant_to_batching_graph_and_schedule(pt):
 
 def test_render_depth_and_roulette(pt):
     sc, ctx, dev, cpu = pt
-    _, s1, _ = dev.render(VIEW, sc.emitter, spp=2, max_depth=1)
-    _, s5, _ = dev.render(VIEW, sc.emitter, spp=2, max_depth=5, rr_depth=3)
-    _, s5n, _ = dev.render(VIEW, sc.emitter, spp=2, max_depth=5, rr_depth=5)
+    _, s1, _ = dev.render(VIEW, sc.emitter, spp=2, max_depth=1, options=F64_LEAF)
+    _, s5, _ = dev.render(VIEW, sc.emitter, spp=2, max_depth=5, rr_depth=3, options=F64_LEAF)
+    _, s5n, _ = dev.render(VIEW, sc.emitter, spp=2, max_depth=5, rr_depth=5, options=F64_LEAF)
     assert s1["extension_rays"] == s1["paths"]
     assert s1["extension_rays"] < s5["extension_rays"] <= s5n["extension_rays"] <= 5 * s5n["paths"]
     assert s5["shadow_rays"] <= s5["extension_rays"]
     # a different seed, a different image of the same scene
-    a, _, _ = dev.render(VIEW, sc.emitter, spp=2, seed=1)
-    b, _, _ = dev.render(VIEW, sc.emitter, spp=2, seed=2)
+    a, _, _ = dev.render(VIEW, sc.emitter, spp=2, seed=1, options=F64_LEAF)
+    b, _, _ = dev.render(VIEW, sc.emitter, spp=2, seed=2, options=F64_LEAF)
     assert not np.array_equal(a, b) and abs(a.mean() - b.mean()) < 0.5 * max(a.mean(), b.mean())

@@ -25,7 +25,7 @@ def world(oracle):
 def test_surface_points_equal_oracle(world, hit_dtype, uvmap):
     ctx, cpu, dev = world
     rays = np.concatenate([scenes.sphere_camera_rays(64, 36), helpers.near_surface_rays(cpu, 1500)])
-    hits = dev.intersect(rays, dm.TraversalOptions(), hit_dtype)
+    hits = dev.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), hit_dtype)
     sp = dev.surface_points(hits, *uvmap)
     hit = hits["tri"] >= 0
     assert hit.sum() > 300
