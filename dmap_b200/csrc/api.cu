@@ -307,11 +307,9 @@ static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, in
         cudaFree(s->assets_dev);
         cudaFree(s->tris_dev);
         cudaFree(s->tris32_dev);
-        cudaFree(s->block_box_dev);
-        cudaFree(s->block_tree_dev);
-        cudaFree(s->cluster_tri_dev);
-        cudaFree(s->cluster_box_dev);
-        cudaFree(s->cluster_tree_dev);
+        cudaFree(s->bvh_nodes_dev);
+        cudaFree(s->bvh_tri_dev);
+        cudaFree(s->bvh_range_dev);
         delete s;
         return st;
     };
@@ -334,51 +332,15 @@ static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, in
     if (st != DMAP_OK)
         return cleanup(st);
     if (n_tri > 256) {
-        // the object box of each block of 32 consecutive triangles, from the
+        // the triangle tree of the candidate orders (bvh.cu), over the
         // outward FP32 boxes the walk tests
         std::vector<TriDev32> t32(n_tri);
         if ((e = cudaMemcpy(t32.data(), s->tris32_dev, sizeof(TriDev32) * n_tri, cudaMemcpyDeviceToHost)))
             return cleanup(cuda_fail(ctx, e, "dmap_scene_create: readback"));
-        const int nb = (n_tri + 31) / 32;
-        // boxes of groups of 32 triangles taken in the order `tri_of`
-        auto group_boxes = [&](const std::vector<int> &tri_of) {
-            std::vector<float> bb((size_t)6 * nb);
-            for (int b = 0; b < nb; ++b)
-                for (int a3 = 0; a3 < 3; ++a3) {
-                    float lo = INFINITY, hi = -INFINITY;
-                    for (int k = 32 * b; k < std::min(n_tri, 32 * b + 32); ++k) {
-                        lo = std::min(lo, t32[tri_of[k]].box_lo[a3]);
-                        hi = std::max(hi, t32[tri_of[k]].box_hi[a3]);
-                    }
-                    bb[6 * b + a3] = lo;
-                    bb[6 * b + 3 + a3] = hi;
-                }
-            return bb;
-        };
-        // more than 8192 triangles: a complete binary tree over those boxes,
-        // heap layout, unions bottom-up (exact in float); leaves past the last
-        // group stay empty and are never entered
-        int L = 0;
-        while ((1 << L) < nb)
-            ++L;
-        const int P = 1 << L;
-        auto group_tree = [&](const std::vector<float> &bb) {
-            std::vector<float> tree((size_t)12 * P);
-            for (int v = 0; v < 2 * P; ++v)
-                for (int a3 = 0; a3 < 3; ++a3) {
-                    tree[6 * v + a3] = INFINITY;
-                    tree[6 * v + 3 + a3] = -INFINITY;
-                }
-            for (int b = 0; b < nb; ++b)
-                for (int q = 0; q < 6; ++q)
-                    tree[6 * (P + b) + q] = bb[6 * b + q];
-            for (int v = P - 1; v >= 1; --v)
-                for (int a3 = 0; a3 < 3; ++a3) {
-                    tree[6 * v + a3] = std::min(tree[6 * (2 * v) + a3], tree[6 * (2 * v + 1) + a3]);
-                    tree[6 * v + 3 + a3] = std::max(tree[6 * (2 * v) + 3 + a3], tree[6 * (2 * v + 1) + 3 + a3]);
-                }
-            return tree;
-        };
+        std::vector<float> nodes, tri_box;
+        std::vector<int> range;
+        if (dmapk::build_bvh(t32.data(), n_tri, nodes, tri_box, range) < 0)
+            return cleanup(fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: triangle tree too deep"));
         auto upload = [&](void **dst, const void *src, size_t bytes, const char *what) -> dmap_status {
             cudaError_t er;
             if ((er = cudaMalloc(dst, bytes)) || (er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice)))
@@ -386,56 +348,14 @@ static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, in
             return DMAP_OK;
         };
         dmap_status us;
-        // blocks of consecutive triangles (the index order)
-        std::vector<int> ident(n_tri);
-        for (int k = 0; k < n_tri; ++k)
-            ident[k] = k;
-        const std::vector<float> bb = group_boxes(ident);
-        if ((us = upload((void **)&s->block_box_dev, bb.data(), sizeof(float) * bb.size(),
-                         "dmap_scene_create: block boxes")) != DMAP_OK)
+        if ((us = upload((void **)&s->bvh_nodes_dev, nodes.data(), sizeof(float) * nodes.size(),
+                         "dmap_scene_create: triangle tree")) != DMAP_OK ||
+            (us = upload((void **)&s->bvh_tri_dev, tri_box.data(), sizeof(float) * tri_box.size(),
+                         "dmap_scene_create: triangle tree boxes")) != DMAP_OK ||
+            (us = upload((void **)&s->bvh_range_dev, range.data(), sizeof(int) * range.size(),
+                         "dmap_scene_create: triangle tree index ranges")) != DMAP_OK)
             return cleanup(us);
-        // spatial clusters (the nearest-first order): the triangles sorted by
-        // the Morton code of their box centres, 10 bits per axis over the
-        // scene's box, ties to the lower index
-        float slo[3] = {INFINITY, INFINITY, INFINITY}, shi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int k = 0; k < n_tri; ++k)
-            for (int a3 = 0; a3 < 3; ++a3) {
-                slo[a3] = std::min(slo[a3], t32[k].box_lo[a3]);
-                shi[a3] = std::max(shi[a3], t32[k].box_hi[a3]);
-            }
-        std::vector<std::pair<uint32_t, int>> code(n_tri);
-        for (int k = 0; k < n_tri; ++k) {
-            uint32_t m = 0;
-            for (int a3 = 0; a3 < 3; ++a3) {
-                const double c = 0.5 * ((double)t32[k].box_lo[a3] + (double)t32[k].box_hi[a3]);
-                const double ext = (double)shi[a3] - (double)slo[a3];
-                double f = ext > 0.0 ? (c - (double)slo[a3]) / ext : 0.0;
-                const uint32_t q = (uint32_t)std::min(1023.0, std::max(0.0, f * 1023.0));
-                for (int bit = 0; bit < 10; ++bit)
-                    m |= ((q >> bit) & 1u) << (3 * bit + (2 - a3));
-            }
-            code[k] = {m, k};
-        }
-        std::sort(code.begin(), code.end());
-        std::vector<int> perm(n_tri);
-        for (int k = 0; k < n_tri; ++k)
-            perm[k] = code[k].second;
-        const std::vector<float> cb = group_boxes(perm);
-        if ((us = upload((void **)&s->cluster_tri_dev, perm.data(), sizeof(int) * perm.size(),
-                         "dmap_scene_create: clusters")) != DMAP_OK ||
-            (us = upload((void **)&s->cluster_box_dev, cb.data(), sizeof(float) * cb.size(),
-                         "dmap_scene_create: cluster boxes")) != DMAP_OK)
-            return cleanup(us);
-        if (nb > 256) {
-            const std::vector<float> bt = group_tree(bb), ct = group_tree(cb);
-            if ((us = upload((void **)&s->block_tree_dev, bt.data(), sizeof(float) * bt.size(),
-                             "dmap_scene_create: block tree")) != DMAP_OK ||
-                (us = upload((void **)&s->cluster_tree_dev, ct.data(), sizeof(float) * ct.size(),
-                             "dmap_scene_create: cluster tree")) != DMAP_OK)
-                return cleanup(us);
-            s->tree_leaves = P;
-            s->tree_log2 = L;
-        }
+        s->bvh_n_nodes = (int)(nodes.size() / 16);
     }
     s->tris_host.resize(n_tri);
     if ((e = cudaMemcpy(s->tris_host.data(), s->tris_dev, sizeof(TriDev) * n_tri, cudaMemcpyDeviceToHost)))
@@ -530,11 +450,9 @@ void dmap_scene_destroy(dmap_scene *s)
     cudaFree(s->assets_dev);
     cudaFree(s->tris_dev);
     cudaFree(s->tris32_dev);
-    cudaFree(s->block_box_dev);
-    cudaFree(s->block_tree_dev);
-    cudaFree(s->cluster_tri_dev);
-    cudaFree(s->cluster_box_dev);
-    cudaFree(s->cluster_tree_dev);
+    cudaFree(s->bvh_nodes_dev);
+    cudaFree(s->bvh_tri_dev);
+    cudaFree(s->bvh_range_dev);
     cudaFree(s->op_mask_dev);
     cudaFree(s->op_tri_dev);
     delete s;
@@ -648,13 +566,10 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.schedule = o.schedule;
     q.rounds = o.rounds;
     q.blocks_per_sm = o.blocks_per_sm;
-    q.block_box = s->block_box_dev;
-    q.block_tree = s->block_tree_dev;
-    q.tree_leaves = s->tree_leaves;
-    q.tree_log2 = s->tree_log2;
-    q.cluster_tri = s->cluster_tri_dev;
-    q.cluster_box = s->cluster_box_dev;
-    q.cluster_tree = s->cluster_tree_dev;
+    q.bvh_nodes = reinterpret_cast<const float4 *>(s->bvh_nodes_dev);
+    q.bvh_tri = reinterpret_cast<const float4 *>(s->bvh_tri_dev);
+    q.bvh_range = reinterpret_cast<const int4 *>(s->bvh_range_dev);
+    q.bvh_n_nodes = s->bvh_n_nodes;
     apply_filter(s, q);
     return DMAP_OK;
 }

@@ -75,12 +75,10 @@ struct dmap_scene
     AssetDev *assets_dev = nullptr;
     TriDev *tris_dev = nullptr;
     TriDev32 *tris32_dev = nullptr;
-    float *block_box_dev = nullptr; // more than 256 triangles: boxes of blocks of 32 (QueryOpts::block_box)
-    float *block_tree_dev = nullptr; // more than 8192 triangles: the tree over those boxes (QueryOpts::block_tree)
-    int tree_leaves = 0, tree_log2 = 0;
-    int *cluster_tri_dev = nullptr;    // more than 256 triangles: spatial clusters for the nearest-first order
-    float *cluster_box_dev = nullptr;
-    float *cluster_tree_dev = nullptr;
+    float *bvh_nodes_dev = nullptr; // more than 256 triangles: the triangle tree the candidate orders walk
+    float *bvh_tri_dev = nullptr;
+    int *bvh_range_dev = nullptr;
+    int bvh_n_nodes = 0;
     std::vector<TriDev> tris_host;
     bool all_f64 = true;
     // the opacity filter (dmap_scene_set_opacity); op_mask_dev null: none

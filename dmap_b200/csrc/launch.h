@@ -4,6 +4,7 @@
 #include "device_types.cuh"
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 namespace dmapk
 {
@@ -25,20 +26,13 @@ struct QueryOpts
     // runs (at most the n the launch is given, which sizes grids and scratch):
     // stages of a device-driven pipeline pass counts they produced themselves.
     const long long *n_dev = nullptr;
-    // Scenes of more than 256 triangles: the object box of every block of 32
-    // consecutive triangles (6 floats, outward), for the walk's candidate mask.
-    const float *block_box = nullptr;
-    // Scenes of more than 8192 triangles: the complete binary tree over those
-    // block boxes in heap layout (node 1 the root, 6 floats per node, leaves
-    // tree_leaves .. 2 tree_leaves - 1 in block order; tree_leaves = 2^tree_log2).
-    const float *block_tree = nullptr;
-    int tree_leaves = 0, tree_log2 = 0;
-    // The same for the nearest-first order over spatial clusters: cluster c
-    // holds triangles cluster_tri[32c .. 32c + 31] (Morton order of their box
-    // centres), with its box and, past 8192 triangles, the tree over them.
-    const int *cluster_tri = nullptr;
-    const float *cluster_box = nullptr;
-    const float *cluster_tree = nullptr;
+    // Scenes of more than 256 triangles: the tree over the triangles' FP32
+    // boxes that both candidate orders walk (bvh.cuh gives the layout), bvh_n_nodes
+    // inner nodes of 4 float4, 2 float4 per triangle list position.
+    const float4 *bvh_nodes = nullptr;
+    const float4 *bvh_tri = nullptr;
+    const int4 *bvh_range = nullptr;
+    int bvh_n_nodes = 0;
     // The scene's opacity filter (dmap_scene_set_opacity): op_h rows of op_w
     // mask texels, 0 transparent; op_tri flags the triangles it covers
     // (nullptr: every one); the object uv map of the crossings' coordinates.
@@ -89,6 +83,13 @@ constexpr int kChartRecord = 37;
 cudaError_t launch_setup(const double *tris_dev, int stride, const int *tri_asset_dev,
                          const dmapdev::AssetDev *assets_dev, int n_tri, dmapdev::TriDev *out,
                          dmapdev::TriDev32 *out32, unsigned *status, cudaStream_t stream);
+
+// The tree over the triangles' FP32 boxes for the candidate orders
+// (bvh.cu; the layout is bvh.cuh's): 16 floats per inner node, 8 per
+// triangle list position, 4 ints of child index ranges per inner node. Returns the tree's depth, or -1 when it would not
+// fit the traversal stack.
+int build_bvh(const dmapdev::TriDev32 *t32, int n_tri, std::vector<float> &nodes, std::vector<float> &tri_box,
+              std::vector<int> &range);
 
 // The FP64 walk, one thread per ray over every triangle (walk64.cu).
 cudaError_t launch_walk64(const dmapdev::TriDev *tris, int n_tri, const dmapdev::AssetDev *assets, const void *rays,

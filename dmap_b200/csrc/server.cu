@@ -230,13 +230,10 @@ struct dmap_server
             // one query over the whole batch
             dmapk::QueryOpts qq = q;
             qq.mode = first->mode;
-            qq.block_box = first->scene->block_box_dev;
-            qq.block_tree = first->scene->block_tree_dev;
-            qq.tree_leaves = first->scene->tree_leaves;
-            qq.tree_log2 = first->scene->tree_log2;
-            qq.cluster_tri = first->scene->cluster_tri_dev;
-            qq.cluster_box = first->scene->cluster_box_dev;
-            qq.cluster_tree = first->scene->cluster_tree_dev;
+            qq.bvh_nodes = reinterpret_cast<const float4 *>(first->scene->bvh_nodes_dev);
+            qq.bvh_tri = reinterpret_cast<const float4 *>(first->scene->bvh_tri_dev);
+            qq.bvh_range = reinterpret_cast<const int4 *>(first->scene->bvh_range_dev);
+            qq.bvh_n_nodes = first->scene->bvh_n_nodes;
             qq.ray_dtype = qq.hit_dtype = 0;
             apply_filter(first->scene, qq); // a filtered scene's batch runs the filter's passes
             dmap_scene *s = first->scene;

@@ -35,6 +35,7 @@
 // This translation unit is compiled with -fmad=false (the FP64 leaf must
 // round like the reference); FP32 code uses explicit fmaf where it wants one.
 #include "f32_node.cuh"
+#include "bvh.cuh"
 #include "leaf32.cuh"
 #include "order.cuh"
 #include "filter.cuh"
@@ -59,84 +60,8 @@ using dmapdev::TriDev32;
 #define DMAP_STALE_CAP 32
 #endif
 
-// The smallest candidate-mode (TOPM below) whose nearest-order picks test a
-// triangle's float box before its FP64 key.
-#ifndef DMAP_BOX_FIRST_TOPM
-#define DMAP_BOX_FIRST_TOPM 1
-#endif
-
-constexpr int kGroupList = 24; // groups a ray's nearest-order list holds
 constexpr int kMaskWords = 8; // scenes of up to 256 triangles take the object-box candidate mask
 constexpr unsigned FULL = 0xffffffffu;
-
-// The triangle's object box, widened, against the float ray (rounded from
-// the caller's): where the exact ray is inside the box, |t d| <= |o| + |box|,
-// so the float ray is within u (2|o| + |box|) of it. On a pass t1 is the
-// exit parameter, rounded up.
-// box_pass that also returns the entry distance t0: the box is widened
-// outward by more than the float rounding of the slab products, so t0 is a
-// lower bound of the exact entry of any box inside it.
-__device__ __forceinline__ bool box_range(const float *box_lo, const float *box_hi, const float *of, const float *df,
-                                          const float *invf, float &t0, float &t1)
-{
-    bool ok = true;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float bmag = fmaxf(fabsf(box_lo[a]), fabsf(box_hi[a]));
-        float pad = ru_mul(2.0f * G, ru_add(ru_fma(2.0f, fabsf(of[a]), bmag), 1.0f));
-        float lo = __fsub_rd(box_lo[a], pad), hi = __fadd_ru(box_hi[a], pad);
-        if (df[a] != 0.0f) {
-            float ta = (lo - of[a]) * invf[a], tb = (hi - of[a]) * invf[a];
-            t0 = fmaxf(t0, fminf(ta, tb));
-            t1 = fminf(t1, fmaxf(ta, tb));
-        } else if (of[a] < lo || of[a] > hi) {
-            ok = false;
-        }
-    }
-    return ok && !(t0 > t1 + tol32(fmaxf(fabsf(t0), fabsf(t1))));
-}
-
-__device__ __forceinline__ bool box_pass(const float *box_lo, const float *box_hi, const float *of, const float *df,
-                                         const float *invf, float t0, float &t1)
-{
-    return box_range(box_lo, box_hi, of, df, invf, t0, t1);
-}
-
-__device__ __forceinline__ bool object_box(const TriDev32 &T, const float *of, const float *df, const float *invf,
-                                           float t0, float &t1)
-{
-    return box_pass(T.box_lo, T.box_hi, of, df, invf, t0, t1);
-}
-
-// Scenes of more than 8192 triangles: the first block >= b, in index
-// order, whose box the ray meets within [t0, t1]. A left-to-right walk of
-// the complete binary tree over the block boxes (heap layout, node 1 the
-// root, leaves P..2P-1 in block order) that skips every subtree whose box
-// the ray misses and every subtree past the last block; each node is
-// entered at most once per call. Blocks come out in index order, so the
-// flat loop's semantics hold (the boxes only prune). -1 when there is none.
-__device__ inline int tree_next(const float *__restrict__ tree, int P, int log2P, int nb, int b, const float *of,
-                                const float *df, const float *invf, float t0, float t1)
-{
-    int v = P + b;
-    for (int guard = 0; guard <= 2 * P; ++guard) {
-        const int depth = 31 - __clz(v);
-        const int start = (v << (log2P - depth)) - P; // the subtree's first block
-        float tt = t1;
-        if (start < nb && box_pass(tree + 6 * v, tree + 6 * v + 3, of, df, invf, t0, tt)) {
-            if (v >= P)
-                return v - P;
-            v = 2 * v;
-        } else {
-            while (v & 1)
-                v >>= 1;
-            if (v == 0)
-                return -1;
-            ++v;
-        }
-    }
-    return -1;
-}
 
 // The tangent-space ray of a triangle: transformed in double, rounded to
 // float, and E covering, for t in [0, t_far], the distance between the float
@@ -283,15 +208,32 @@ __global__ void __launch_bounds__(128) walk32_simple(const TriDev32 *__restrict_
     d64::hit64 best;
     int best_tri = -1, best_flags = 0;
     bool found = false, capped = false;
-    // the next triangle: index order, or (nearest) the smallest (key, index)
-    // past the cursor among the candidates the ray still reaches
+    // the next triangle: the smallest (key, index) past the cursor among the
+    // candidates the ray still reaches, the key being the index (index
+    // order) or the box entry (nearest)
     double inv[3], ckey = -INFINITY;
     int cidx = -1;
     d64::ray_inverse(d, inv);
+    // scenes of more than 256 triangles: the triangle tree (bvh.cuh)
+    const d32::BvhView bvh = {opt.bvh_nodes, opt.bvh_tri, opt.bvh_range, opt.bvh_n_nodes};
+    d32::NearBuf nbuf;
+    nbuf.n = -1;
+    nbuf.pos = 0;
     for (int step = 0; step < n_tri; ++step) {
         int t = step;
         float t1 = __double2float_ru(t_max);
-        if (opt.order == 1) {
+        if (bvh.nodes) {
+            bool err = false;
+            const float tmin_f = __double2float_rd(t_min);
+            t = opt.order == 1 ? d32::near_next<true>(nbuf, bvh, tris32, tris64, o, d, inv, t_min, of, df, invf,
+                                                      tmin_f, t1, ckey, cidx, t1, err)
+                               : d32::near_next<false>(nbuf, bvh, tris32, tris64, o, d, inv, t_min, of, df, invf,
+                                                       tmin_f, t1, ckey, cidx, t1, err);
+            if (err)
+                atomicOr(status, dmapdev::kStatusCapped);
+            if (t < 0)
+                break;
+        } else if (opt.order == 1) {
             const float tmf = t1;
             double bk = 0.0;
             int bt = -1;
@@ -396,7 +338,7 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // One lane's walk from its parked or fresh state to the next leaf (parked,
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
-template <bool ST, bool INLINE_LEAF, int TOPM, bool NEAR, typename R, typename H, typename Fp>
+template <bool ST, bool INLINE_LEAF, bool TREE, bool NEAR, typename R, typename H, typename Fp>
 __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
@@ -406,23 +348,13 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
 {
     enum : int { NEED = 0, TOP = 1, WALK = 2, DONE = 3 };
     const int lane = threadIdx.x & 31;
-    // the candidate mask: one bit per triangle (up to 256 triangles), or
-    // (TOPM 1) one bit per block of 32 consecutive triangles (up to 8192),
-    // visited in order; (TOPM 2) no mask, the block tree instead
-    // (the launcher takes TOPM 0 only for scenes of up to 256 triangles, so
-    // the flat loops below are never compiled into the hot kernels)
-    constexpr bool use_blocks = TOPM == 1;
-    constexpr bool use_mask = TOPM <= 1;
-    // the nearest-first order takes its candidates by spatial clusters (the
-    // triangles of cluster c: cluster_tri[32c ..]), the index order by blocks
-    // of consecutive triangles
-    const bool clustered = NEAR && opt.cluster_tri != nullptr;
-    const float *const item_box = clustered ? opt.cluster_box : opt.block_box;
-    const float *const item_tree = clustered ? opt.cluster_tree : opt.block_tree;
-    const int n_items = use_blocks ? (n_tri + 31) / 32 : n_tri;
-    // nearest order: test a candidate's float box before its FP64 key (the
-    // group scans of large scenes, where most of a group's boxes miss)
-    constexpr bool kBoxFirst = TOPM >= DMAP_BOX_FIRST_TOPM;
+    // the candidates: scenes of up to 256 triangles take a mask of one bit
+    // per triangle whose box the ray meets (built by the warp at the ray's
+    // start), larger scenes (TREE) the triangle tree (bvh.cuh), in either
+    // order; the launcher takes the mask only for up to 256 triangles, so its
+    // loops are never compiled into the kernels of larger scenes
+    constexpr bool use_mask = !TREE;
+    const d32::BvhView bvh = {opt.bvh_nodes, opt.bvh_tri, opt.bvh_range, opt.bvh_n_nodes};
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
     if (round == 0 && opt.n_dev && (unsigned long long)*opt.n_dev < count)
@@ -435,11 +367,11 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     int tri = 0, best_tri = -1, root = 0, si = 0, sj = 0, nah = 0, lah = 0, flags = 0, guard = 0;
     double ckey = -INFINITY;
     int cidx = -1;
-    // nearest order over groups (TOPM >= 1): the ray's sorted group list;
-    // n_gl -1: not built for this ray, kGroupList + 1: more groups than fit
-    int gl_b[kGroupList];
-    float gl_e[kGroupList];
-    int n_gl = -1;
+    // the triangle tree (TREE): the lane's buffered candidates, refilled
+    // from the ray's cursor for each ray it takes
+    d32::NearBuf nbuf;
+    nbuf.n = -1;
+    nbuf.pos = 0;
     Ray32 r;
     Cell32 cur = {0, 0, 0}, end = {0, 0, 0};
     unsigned mask[kMaskWords];
@@ -507,7 +439,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 } else {
                     ray = round == 0 ? (int)item : q_in[item];
                     load_ray(rays, ray, o, d, t_min, t_max);
-                    n_gl = -1;
+                    nbuf.n = -1;
 #pragma unroll
                     for (int a = 0; a < 3; ++a) {
                         of[a] = (float)o[a];
@@ -579,10 +511,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 for (int w = 0; w < kMaskWords; ++w) {
                     int t = 32 * w + lane;
                     float t1 = s_tmax;
-                    bool pass = t < n_items &&
-                                (use_blocks ? box_pass(item_box + 6 * t, item_box + 6 * t + 3, so, sd, sv,
-                                                       s_tmin, t1)
-                                            : object_box(tris32[t], so, sd, sv, s_tmin, t1));
+                    bool pass = t < n_tri && object_box(tris32[t], so, sd, sv, s_tmin, t1);
                     unsigned bits = __ballot_sync(FULL, pass);
                     if (lane == src) {
 #pragma unroll
@@ -607,142 +536,28 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 double bk = 0.0;
                 int bt = -1;
                 const float tmf = __double2float_ru(t_max);
-                // takes t when it is the best so far; true when t is still a
-                // candidate past the cursor (box-first order: its box passes)
-                auto consider = [&](int t) -> bool {
-                    float tt = tmf;
-                    if (kBoxFirst) {
-                        // the float box first: its entry e is a lower bound of
-                        // the key, so past the best key the FP64 key is not needed
-                        float e = tmin_f;
-                        if (!box_range(tris32[t].box_lo, tris32[t].box_hi, of, df, invf, e, tt))
-                            return false;
-                        if (bt >= 0 && (double)e > bk)
-                            return true; // key > best key > cursor
-                    }
-                    const double key = d64::entry_key(tris64[t], o, d, inv, t_min);
-                    if (!d64::after_cursor(key, t, ckey, cidx))
-                        return false;
-                    if (!d64::before_best(key, t, bk, bt))
-                        return true;
-                    if (!kBoxFirst && !object_box(tris32[t], of, df, invf, tmin_f, tt))
-                        return false;
-                    bk = key;
-                    bt = t;
-                    t1 = tt;
-                    return true;
-                };
-                if (TOPM >= 1) {
-                    // blocks: first the candidate block with the nearest
-                    // entry, then the others unless their entry (a lower
-                    // bound of their triangles' keys) is beyond the best key
-                    const int nb = (n_tri + 31) >> 5;
-                    auto blocks = [&](auto &&fn) {
-                        if (TOPM == 2) {
-                            for (int b = 0; b < nb; ++b) {
-                                b = tree_next(item_tree, opt.tree_leaves, opt.tree_log2, nb, b, of, df, invf,
-                                              tmin_f, tmf);
-                                if (b < 0)
-                                    break;
-                                fn(b);
-                            }
-                        } else {
-#pragma unroll 1
-                            for (int w = 0; w < kMaskWords; ++w) {
-                                unsigned bits = mask[0];
-#pragma unroll
-                                for (int q = 1; q < kMaskWords; ++q)
-                                    bits = w == q ? mask[q] : bits;
-                                while (bits) {
-                                    const int b = 32 * w + __ffs(bits) - 1;
-                                    bits &= bits - 1;
-                                    if (b < nb)
-                                        fn(b);
-                                }
-                            }
-                        }
+                if (TREE) {
+                    bool err = false;
+                    bt = d32::near_next<true>(nbuf, bvh, tris32, tris64, o, d, inv, t_min, of, df, invf, tmin_f, tmf,
+                                        ckey, cidx, t1, err);
+                    bk = ckey;
+                    if (err)
+                        atomicOr(status, dmapdev::kStatusCapped);
+                } else {
+                    // takes t when it is the best so far: one bit per
+                    // triangle whose box the ray met, each re-tested with
+                    // the current t_max
+                    auto consider = [&](int t) {
+                        const double key = d64::entry_key(tris64[t], o, d, inv, t_min);
+                        if (!d64::after_cursor(key, t, ckey, cidx) || !d64::before_best(key, t, bk, bt))
+                            return;
+                        float tt = tmf;
+                        if (!object_box(tris32[t], of, df, invf, tmin_f, tt))
+                            return;
+                        bk = key;
+                        bt = t;
+                        t1 = tt;
                     };
-                    auto entry = [&](int b, float &e) {
-                        float t0 = tmin_f, t1b = tmf;
-                        const bool ok = box_range(item_box + 6 * b, item_box + 6 * b + 3, of, df, invf, t0,
-                                                  t1b);
-                        e = t0;
-                        return ok;
-                    };
-                    // the groups the ray reaches, sorted by entry bound (up to
-                    // kGroupList of them), built at the ray's first pick in
-                    // this launch and kept for its later picks: t_max only
-                    // shrinks, so no other group becomes reachable, and each
-                    // pick re-tests a listed group's box before it scans it.
-                    // Groups are scanned nearest first until a group's bound
-                    // passes the best key (the bound is a lower bound of its
-                    // triangles' keys). Past kGroupList groups: the nearest
-                    // group first, then every group whose bound is not beyond
-                    // the best key, enumerated at every pick.
-                    if (n_gl < 0) {
-                        n_gl = 0;
-                        blocks([&](int b) {
-                            float e;
-                            if (n_gl > kGroupList || !entry(b, e))
-                                return;
-                            if (n_gl == kGroupList) {
-                                n_gl = kGroupList + 1;
-                                return;
-                            }
-                            int k = n_gl++;
-                            for (; k > 0; --k) { // insertion: slots below n_gl are set
-                                const float prev = gl_e[k - 1];
-                                if (!(prev > e))
-                                    break;
-                                gl_e[k] = prev;
-                                gl_b[k] = gl_b[k - 1];
-                            }
-                            gl_e[k] = e;
-                            gl_b[k] = b;
-                        });
-                    }
-                    // true when a triangle of group b is still a candidate
-                    auto scan = [&](int b) {
-                        bool left = false;
-                        for (int q = 32 * b, stop = min(n_tri, 32 * b + 32); q < stop; ++q)
-                            if (consider(clustered ? opt.cluster_tri[q] : q))
-                                left = true;
-                        return left;
-                    };
-                    if (n_gl <= kGroupList) {
-                        for (int k = 0; k < n_gl; ++k) {
-                            if (gl_b[k] < 0) // spent
-                                continue;
-                            if (bt >= 0 && (double)gl_e[k] > bk)
-                                break;
-                            // a group no longer reached with the current t_max,
-                            // or without a candidate past the cursor, stays so:
-                            // t_max only shrinks and the cursor only advances
-                            float e;
-                            if (!entry(gl_b[k], e) || !scan(gl_b[k]))
-                                gl_b[k] = -1;
-                        }
-                    } else {
-                        int b0 = -1;
-                        float e0 = INFINITY;
-                        blocks([&](int b) {
-                            float e;
-                            if (entry(b, e) && (b0 < 0 || e < e0)) {
-                                b0 = b;
-                                e0 = e;
-                            }
-                        });
-                        if (b0 >= 0) {
-                            scan(b0);
-                            blocks([&](int b) {
-                                float e;
-                                if (b == b0 || !entry(b, e) || (bt >= 0 && (double)e > bk))
-                                    return;
-                                scan(b);
-                            });
-                        }
-                    }
-                } else if (use_mask) {
 #pragma unroll 1
                     for (int w = 0; w < kMaskWords; ++w) {
                         unsigned bits = mask[0];
@@ -752,18 +567,10 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                         while (bits) {
                             const int item = 32 * w + __ffs(bits) - 1;
                             bits &= bits - 1;
-                            if (use_blocks) {
-                                const int stop = min(n_tri, 32 * item + 32);
-                                for (int t = 32 * item; t < stop; ++t)
-                                    consider(t);
-                            } else if (item < n_tri) {
+                            if (item < n_tri)
                                 consider(item);
-                            }
                         }
                     }
-                } else {
-                    for (int t = 0; t < n_tri; ++t)
-                        consider(t);
                 }
                 if (bt >= 0) {
                     tri = bt;
@@ -773,58 +580,23 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 } else {
                     tri = n_tri;
                 }
-            } else if (use_blocks) {
-                // the next block whose box the ray met, then its triangles in order
-                while (tri < n_tri) {
-                    int blk = tri >> 5, w = blk >> 5;
-                    unsigned bits = mask[0];
-#pragma unroll
-                    for (int q = 1; q < kMaskWords; ++q)
-                        bits = w == q ? mask[q] : bits;
-                    bits &= ~0u << (blk & 31);
-                    if (!bits) {
-                        tri = (w + 1) << 10;
-                        continue;
-                    }
-                    int nb = (w << 5) + __ffs(bits) - 1;
-                    if (nb != blk)
-                        tri = nb << 5;
-                    const int stop = min(n_tri, (nb + 1) << 5);
-                    for (; tri < stop; ++tri) {
-                        t1 = __double2float_ru(t_max);
-                        if (object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
-                            hit_box = true;
-                            break;
-                        }
-                    }
-                    if (hit_box)
-                        break;
+            } else if (TREE) {
+                // index order: the smallest index from tri on whose box the
+                // ray still meets
+                bool err = false;
+                double ck = tri - 1;
+                int ci = tri - 1;
+                const int t = d32::near_next<false>(nbuf, bvh, tris32, tris64, o, d, nullptr, t_min, of, df, invf,
+                                                    tmin_f, __double2float_ru(t_max), ck, ci, t1, err);
+                if (err)
+                    atomicOr(status, dmapdev::kStatusCapped);
+                if (t >= 0) {
+                    tri = t;
+                    hit_box = true;
+                } else {
+                    tri = n_tri;
                 }
-            } else if (TOPM == 2) {
-                // blocks in order from the tree, then their triangles in order
-                const int nb = (n_tri + 31) >> 5;
-                while (tri < n_tri) {
-                    if ((tri & 31) == 0) {
-                        const int blk = tree_next(opt.block_tree, opt.tree_leaves, opt.tree_log2, nb, tri >> 5, of, df,
-                                                  invf, tmin_f, __double2float_ru(t_max));
-                        if (blk < 0) {
-                            tri = n_tri;
-                            break;
-                        }
-                        tri = blk << 5;
-                    }
-                    const int stop = min(n_tri, (tri | 31) + 1);
-                    for (; tri < stop; ++tri) {
-                        t1 = __double2float_ru(t_max);
-                        if (object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
-                            hit_box = true;
-                            break;
-                        }
-                    }
-                    if (hit_box)
-                        break;
-                }
-            } else if (use_mask) {
+            } else {
                 while (tri < n_tri) {
                     int w = tri >> 5;
                     unsigned bits = mask[0];
@@ -843,14 +615,6 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                         break;
                     }
                     ++tri;
-                }
-            } else {
-                for (; tri < n_tri; ++tri) {
-                    t1 = __double2float_ru(t_max);
-                    if (object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
-                        hit_box = true;
-                        break;
-                    }
                 }
             }
             if (!hit_box) {
@@ -1399,38 +1163,33 @@ cudaError_t launch(const TriDev32 *t32, const TriDev *t64, int n_tri, const Asse
         const int *q_in = ws.queue[(rd + 1) & 1];
         int *q_out = ws.queue[rd & 1];
         bool last = rd == rounds;
-        // the block mask has its own instances so that scenes of up to 256
-        // triangles keep the smaller kernel
-        // (and scenes of more than 8192 triangles walk the block tree)
-        const int topm = n_tri > 32 * kMaskWords && opt.block_box && n_tri <= 32 * 32 * kMaskWords ? 1
-                         : n_tri > 32 * 32 * kMaskWords && opt.block_tree                          ? 2
-                                                                                                    : 0;
-        if (topm == 0 && n_tri > 32 * kMaskWords)
-            return cudaErrorInvalidValue; // a scene without its block boxes (every scene has them)
-        // (the triangle order is a template argument too, so each instance
-        // carries the code of one order only)
+        // scenes of more than 256 triangles take the triangle tree; each
+        // candidate mode and each triangle order has its own instances, so
+        // every kernel carries one order's candidate code, and scenes of up
+        // to 256 triangles keep the smaller kernel
         const bool nearest = opt.order == 1;
-#define DMAP_WALK_LAUNCH(ST_, IL_, TM_, NR_)                                                                        \
-    wave_walk<ST_, IL_, TM_, NR_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,      \
+        const bool tree = n_tri > 32 * kMaskWords;
+        if (tree && !opt.bvh_nodes)
+            return cudaErrorInvalidValue; // a scene without its triangle tree (every such scene has one)
+#define DMAP_WALK_LAUNCH(ST_, IL_, TR_, NR_)                                                                        \
+    wave_walk<ST_, IL_, TR_, NR_, R, H, Fp><<<grid, 128, 0, stream>>>(t32, t64, n_tri, assets, rr, n, opt, hh,      \
                                                                       ST_ ? stats : nullptr, states, q_in, rd,    \
                                                                       leaves, ws.counters, status)
-#define DMAP_WALK_ORDER(ST_, IL_, TM_)                                                                              \
-    (nearest ? DMAP_WALK_LAUNCH(ST_, IL_, TM_, true) : DMAP_WALK_LAUNCH(ST_, IL_, TM_, false))
-#define DMAP_WALK_TOPM(ST_, IL_)                                                                                    \
-    (topm == 1 ? DMAP_WALK_ORDER(ST_, IL_, 1) : topm == 2 ? DMAP_WALK_ORDER(ST_, IL_, 2) : DMAP_WALK_ORDER(ST_, IL_, 0))
+#define DMAP_WALK_MODE(ST_, IL_)                                                                                    \
+    (tree ? (nearest ? DMAP_WALK_LAUNCH(ST_, IL_, true, true) : DMAP_WALK_LAUNCH(ST_, IL_, true, false))           \
+          : (nearest ? DMAP_WALK_LAUNCH(ST_, IL_, false, true) : DMAP_WALK_LAUNCH(ST_, IL_, false, false)))
         if (stats) {
             if (last)
-                DMAP_WALK_TOPM(true, true);
+                DMAP_WALK_MODE(true, true);
             else
-                DMAP_WALK_TOPM(true, false);
+                DMAP_WALK_MODE(true, false);
         } else {
             if (last)
-                DMAP_WALK_TOPM(false, true);
+                DMAP_WALK_MODE(false, true);
             else
-                DMAP_WALK_TOPM(false, false);
+                DMAP_WALK_MODE(false, false);
         }
-#undef DMAP_WALK_TOPM
-#undef DMAP_WALK_ORDER
+#undef DMAP_WALK_MODE
 #undef DMAP_WALK_LAUNCH
         if ((e = cudaGetLastError()) != cudaSuccess)
             return e;

@@ -139,10 +139,10 @@ def test_f32_grazing_rays_f16(ctx, oracle):
 
 
 @pytest.mark.parametrize("n,k", [(16, 8), (8, 24)])
-def test_f32_many_triangles_block_mask(ctx, oracle, n, k):
-    """Scenes of more than 256 triangles (768 and 6912) take the per-ray mask
-    of 32-triangle blocks; hits equal the oracle's flat loop and the simple
-    schedule's."""
+def test_f32_many_triangles_tree(ctx, oracle, n, k):
+    """Scenes of more than 256 triangles (768 and 6912) take their candidates
+    from the triangle tree in both orders; hits equal the oracle's loops and
+    the simple schedule's."""
     sc = scenes.cube_sphere_scene(n, k)
     assert len(sc.tris) > 256
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
@@ -157,11 +157,10 @@ def test_f32_many_triangles_block_mask(ctx, oracle, n, k):
 
 
 @pytest.mark.parametrize("k", [30, 40])
-def test_f32_many_triangles_block_tree(ctx, oracle, k):
-    """Scenes of more than 8192 triangles (10800 and 19200: 338 and 600
-    blocks, trees of 512 and 1024 leaves with empty padding) walk the tree
-    over the 32-triangle blocks' boxes; hits equal the oracle's in both
-    triangle orders, and the simple schedule's."""
+def test_f32_many_triangles_large_tree(ctx, oracle, k):
+    """Scenes of 10800 and 19200 triangles (deeper trees): hits equal the
+    oracle's in both triangle orders, and the simple schedule's; occlusion
+    agrees with the closest hits."""
     sc = scenes.cube_sphere_scene(8, k)
     assert len(sc.tris) > 8192
     cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
@@ -175,3 +174,26 @@ def test_f32_many_triangles_block_tree(ctx, oracle, k):
         assert a.tobytes() == b.tobytes()
     occ = dev.intersect(rays, dm.TraversalOptions(mode="occluded", leaf_precision="f64"), np.float64)
     assert np.array_equal(occ["tri"] >= 0, a["tri"] >= 0)
+
+
+@pytest.mark.parametrize("k", [16, 48])
+def test_f32_nearest_tree_refills(ctx, oracle, k):
+    """The nearest order over more than 256 triangles takes its candidates
+    from the triangle tree, eight at a time: rays grazing a cube sphere of
+    small patches (3072 and 27648 triangles) pass over more than eight
+    triangle boxes, so the buffer is refilled past its last entry; every
+    hit record equals the oracle's nearest-order loop, on both schedules,
+    the FP32 leaf within its tolerance of it."""
+    sc = scenes.cube_sphere_scene(8, k, amplitude=0.08 * 4 / k)
+    cpu, dev = py_oracle.CpuScene(oracle, sc), dm.Scene.from_synthetic(ctx, sc)
+    p, m = scenes.base_points(sc, 3000, seed=91)
+    rays = np.concatenate([scenes.grazing_rays(p, m, seed=92), helpers.near_surface_rays(cpu, 1500),
+                           scenes.sphere_camera_rays(64, 36)])
+    ho, so = cpu.intersect(rays, stats=True, order="nearest")
+    assert so[:, 0].max() > 8, "no ray walked more than eight triangles"
+    for schedule in ("wavefront", "simple"):
+        n_hit, _ = _check(cpu, dev, rays, order="nearest", schedule=schedule)
+        assert n_hit > 1000
+    h32 = dev.intersect(rays, dm.TraversalOptions(order="nearest"), np.float64)
+    from test_gpu_leaf32 import judge
+    judge(h32, ho, rays, sc.extent)
