@@ -1,11 +1,12 @@
 """Builds libdmap_b200.so in place: every CUDA source for sm_100a with nvcc.
 
 The translation units with FP64 arithmetic that must round like the
-reference (pyramid.cu, setup.cu, walk64.cu, walk32.cu for its FP64 leaf,
-shade.cu, tess.cu, emitter.cu)
+reference (pyramid.cu, setup.cu, walk64.cu, walk32_exact.cu for the paths
+that run the FP64 leaf, shade.cu, tess.cu, emitter.cu)
 are compiled with -fmad=false so that each double operation rounds on its
 own, as the reference's CPU build does; FP32 code there asks for fused
-multiply-adds explicitly (fmaf, __fmaf_ru).
+multiply-adds explicitly (fmaf, __fmaf_ru). walk32.cu (the FP32 walk and
+leaf rounds) is compiled with contraction.
 Usage: python -m dmap_b200.build [-j N] [--force]
 """
 from __future__ import annotations
@@ -25,7 +26,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libdmap_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-I", str(CSRC)]
-EXACT_FP64 = {"pyramid.cu", "setup.cu", "walk64.cu", "walk32.cu", "shade.cu", "tess.cu", "emitter.cu"}
+EXACT_FP64 = {"pyramid.cu", "setup.cu", "walk64.cu", "walk32_exact.cu", "shade.cu", "tess.cu", "emitter.cu"}
 
 
 def nvcc() -> str:

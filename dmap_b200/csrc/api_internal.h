@@ -137,15 +137,14 @@ inline EncodeTiledFn encode_tiled()
 }
 
 // A scene's opacity filter in a query's options: the mask, the triangles it
-// covers and the uv map; a filtered FP32 query runs the one-thread-per-ray
-// schedule, whose triangle walks take the filter's passes (the wavefront's
-// leaf rounds commit crossings as they find them).
+// covers and the uv map. The one-thread-per-ray schedule takes the filter's
+// passes in its triangle walks; the wavefront answers without them and
+// hands every ray that took a crossing the filter rejects to that schedule
+// (walk32.cuh).
 inline void apply_filter(const dmap_scene *s, dmapk::QueryOpts &q)
 {
     if (!s->op_mask_dev)
         return;
-    if (q.precision == DMAP_PRECISION_F32)
-        q.schedule = DMAP_SCHEDULE_SIMPLE;
     q.op_mask = s->op_mask_dev;
     q.op_tri = s->op_tri_dev;
     q.op_w = s->op_w;
@@ -192,6 +191,7 @@ inline void wave_release(dmapk::WaveScratch &w)
     cudaFree(w.queue[1]);
     cudaFree(w.leaves);
     cudaFree(w.counters);
+    cudaFree(w.rerun);
     w = dmapk::WaveScratch{};
 }
 
@@ -207,8 +207,8 @@ inline dmap_status wave_reserve(dmap_context *ctx, dmapk::WaveScratch &w, int64_
         (e = cudaMalloc((void **)&w.queue[0], sizeof(int) * n)) != cudaSuccess ||
         (e = cudaMalloc((void **)&w.queue[1], sizeof(int) * n)) != cudaSuccess ||
         (e = cudaMalloc(&w.leaves, dmapk::wave_leaf_bytes() * n)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&w.counters, sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1))) !=
-            cudaSuccess) {
+        (e = cudaMalloc((void **)&w.counters, sizeof(unsigned long long) * dmapk::kWaveCounters)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&w.rerun, sizeof(int) * n)) != cudaSuccess) {
         wave_release(w);
         return cuda_fail(ctx, e, "wavefront scratch");
     }
@@ -219,8 +219,8 @@ inline dmap_status wave_reserve(dmap_context *ctx, dmapk::WaveScratch &w, int64_
 // Device bytes of a wavefront scratch for n rays.
 inline size_t wave_bytes(int64_t n)
 {
-    return (dmapk::wave_state_bytes() + 2 * sizeof(int) + dmapk::wave_leaf_bytes()) * (size_t)n +
-           sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1);
+    return (dmapk::wave_state_bytes() + 3 * sizeof(int) + dmapk::wave_leaf_bytes()) * (size_t)n +
+           sizeof(unsigned long long) * dmapk::kWaveCounters;
 }
 
 // Validates dmap_options into the kernels' QueryOpts (api.cu).

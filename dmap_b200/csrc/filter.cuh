@@ -4,8 +4,9 @@
 // rejects raises t_lo to the crossing's t and the triangle is walked again,
 // at most max_filter_passes times (displaced_geometry.h:64). The filter is
 // ks's opacity map reduced to a binary texel mask over the object's texture
-// coordinates. Included by translation units compiled with -fmad=false, so
-// the texture coordinate is the reference's to the bit.
+// coordinates. Every double operation is an explicitly rounded intrinsic, so
+// the texture coordinate is the reference's to the bit in any translation
+// unit, contracted or not.
 #pragma once
 #include "device_types.cuh"
 #include "launch.h"
@@ -25,13 +26,16 @@ __device__ inline bool crossing_opaque(const dmapk::QueryOpts &q, const TriDev &
     // compute_hit_texcoord (:189-193): BaseTriangle::param (displaced_surface.h:87)
     // and DisplacedObject::object_uv (scene_spec.cpp:382-388), rounded to float
     const double u = (double)(float)bu, v = (double)(float)bv;
-    const double s = (T.t0[0] + u * (T.t1[0] - T.t0[0])) + v * (T.t2[0] - T.t0[0]);
-    const double t = (T.t0[1] + u * (T.t1[1] - T.t0[1])) + v * (T.t2[1] - T.t0[1]);
-    double x = (s - q.op_offset[0]) / q.op_scale[0], y = (t - q.op_offset[1]) / q.op_scale[1];
+    const double s = __dadd_rn(__dadd_rn(T.t0[0], __dmul_rn(u, __dsub_rn(T.t1[0], T.t0[0]))),
+                               __dmul_rn(v, __dsub_rn(T.t2[0], T.t0[0])));
+    const double t = __dadd_rn(__dadd_rn(T.t0[1], __dmul_rn(u, __dsub_rn(T.t1[1], T.t0[1]))),
+                               __dmul_rn(v, __dsub_rn(T.t2[1], T.t0[1])));
+    double x = __ddiv_rn(__dsub_rn(s, q.op_offset[0]), q.op_scale[0]);
+    double y = __ddiv_rn(__dsub_rn(t, q.op_offset[1]), q.op_scale[1]);
     if (q.op_flip)
-        y = 1.0 - y;
+        y = __dsub_rn(1.0, y);
     // the texel under the float texture coordinate, repeated outside [0, 1)
-    const double fx = (double)(float)x * q.op_w, fy = (double)(float)y * q.op_h;
+    const double fx = __dmul_rn((double)(float)x, (double)q.op_w), fy = __dmul_rn((double)(float)y, (double)q.op_h);
     if (!(fabs(fx) < 1e15 && fabs(fy) < 1e15))
         return true;
     long long i = (long long)floor(fx) % q.op_w, j = (long long)floor(fy) % q.op_h;

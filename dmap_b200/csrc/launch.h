@@ -43,16 +43,21 @@ struct QueryOpts
 };
 
 constexpr int kMaxRounds = 32;
+// Counters of a wavefront scratch: 4 per round (kMaxRounds + 1 rounds), then
+// the length of the filter's rerun list.
+constexpr int kWaveCounters = 4 * (kMaxRounds + 1) + 1;
 
 // Device scratch of the wavefront schedule for up to `capacity` rays: the
 // parked walk states, two ray queues (resume in / resume out), the leaf
-// jobs, and 4 counters per round (kMaxRounds + 1 rounds).
+// jobs, the counters, and the rays a filtered scene answers again on the
+// filter's own schedule (a crossing the filter rejects was taken).
 struct WaveScratch
 {
     void *state = nullptr;
     int *queue[2] = {nullptr, nullptr};
     void *leaves = nullptr;
     unsigned long long *counters = nullptr;
+    int *rerun = nullptr;
     int64_t capacity = 0;
 };
 size_t wave_state_bytes();

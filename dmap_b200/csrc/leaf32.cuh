@@ -255,7 +255,7 @@ __device__ inline bool newton32(const TriDev &T, const Leaf32 &L, float a, float
 // w) and the ray's Q3 and 1/|d| come from the leaf's setup. flags gets
 // DMAP_HIT_FP64_LEAF | DMAP_HIT_POLISHED when the reported root is the FP64
 // Newton root. Kept out of line: it runs once per accepted root.
-__device__ __noinline__ bool accept_root(const TriDev &T, const AssetDev &g, double lo_s, double lo_t, double w,
+static __device__ __noinline__ bool accept_root(const TriDev &T, const AssetDev &g, double lo_s, double lo_t, double w,
                                          double Q3, double inv_dlen, v3 o, v3 d, double t_min, double t_max,
                                          int64_t i, int64_t j, Root32 R, double polish_cond, hit64 &hit, int &flags,
                                          int64_t &iters)

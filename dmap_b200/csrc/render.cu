@@ -313,7 +313,7 @@ struct RenderJob
         graph = nullptr;
         void *all[] = {ray[0], ray[1], path[0], path[1], hit, shit, beta, Lp, srays, scontrib, accum, spath,
                        cnt, p0, totals, rec_n, rec_rays, rec_t, rec_kind, rec_tri,
-                       wave.state, wave.queue[0], wave.queue[1], wave.leaves, wave.counters};
+                       wave.state, wave.queue[0], wave.queue[1], wave.leaves, wave.counters, wave.rerun};
         for (void *p : all)
             if (p)
                 cudaFreeAsync(p, stream);
@@ -494,7 +494,8 @@ dmap_status render_begin(dmap_scene *s, const dmap_render_desc *desc, const dmap
     alloc((void **)&J->wave.queue[0], sizeof(int) * P);
     alloc((void **)&J->wave.queue[1], sizeof(int) * P);
     alloc(&J->wave.leaves, dmapk::wave_leaf_bytes() * P);
-    alloc((void **)&J->wave.counters, sizeof(unsigned long long) * 4 * (dmapk::kMaxRounds + 1));
+    alloc((void **)&J->wave.counters, sizeof(unsigned long long) * dmapk::kWaveCounters);
+    alloc((void **)&J->wave.rerun, sizeof(int) * P);
     J->wave.capacity = P;
     if (e != cudaSuccess) {
         J->release(stream);

@@ -205,7 +205,11 @@ dmap_status dmap_scene_triangle_info(const dmap_scene *scene, int tri, double *o
  * beyond the current hit: the walk starts with a tight t_max, so far
  * triangles cost a box test instead of a walk. Both find the nearest
  * certified root; the returned t may differ in the last bits where the walks
- * run with different t_max.
+ * run with different t_max. Scenes of more than 256 triangles find their
+ * candidates in either order through a tree over the triangles' boxes built
+ * by dmap_scene_create (the reference's embree BVH over rtc_bounds,
+ * displaced_intersector.cpp:454-464); the visiting order is the same as a
+ * scan over every triangle.
  */
 #define DMAP_ORDER_INDEX 0
 #define DMAP_ORDER_NEAREST 1

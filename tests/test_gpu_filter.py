@@ -1,8 +1,10 @@
 """The opacity filter on the device (dmap_scene_set_opacity) against the
 oracle's restatement, which is pinned to the intersect callback's passes run
-over the reference's own intersector (test_oracle_filter.py): the FP64 path
-and the FP32 one-thread-per-ray walk, closest and occlusion queries, both
-triangle orders; and the calls that refuse a filtered scene."""
+over the reference's own intersector (test_oracle_filter.py): the FP64 path,
+the FP32 one-thread-per-ray walk and the FP32 wavefront (which hands the rays
+that took a rejected crossing to the one-thread-per-ray walk), closest and
+occlusion queries, both triangle orders; and the calls that refuse a
+filtered scene."""
 import numpy as np
 import pytest
 
@@ -20,9 +22,9 @@ def ctx():
 
 
 @pytest.mark.parametrize("name,mapname", [("quad", "identity"), ("charts", "scaled"), ("sphere", "scaled")])
-@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("precision,schedule", [("f64", "simple"), ("f32", "simple"), ("f32", "wavefront")])
 @pytest.mark.parametrize("order", ["nearest", "index"])
-def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, order):
+def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, schedule, order):
     sc, so, rays = scene_and_rays(name, oracle)
     dev = dm.Scene.from_synthetic(ctx, sc, keep_f64=True)
     scale, off, flip = MAPS[mapname]
@@ -31,7 +33,7 @@ def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, or
     so.set_opacity(m, scale, off, flip, flags)
     dev.set_opacity(m, scale, off, flip, flags)
     ho, _ = so.intersect(rays, order=order)
-    opt = dm.TraversalOptions(precision=precision, schedule="simple", order=order, leaf_precision="f64")
+    opt = dm.TraversalOptions(precision=precision, schedule=schedule, order=order, leaf_precision="f64")
     hd = dev.intersect(rays, opt, np.float64)
     hit = ho[:, 10] >= 0
     assert hit.sum() > 100
@@ -45,7 +47,7 @@ def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, or
     so.set_opacity(None)
     assert (so.intersect(rays, order=order)[0][:, 10] != ho[:, 10]).sum() > 20
     # occlusion through the filter: occluded exactly where the filtered closest query hits
-    occ = dev.intersect(rays, dm.TraversalOptions(precision=precision, schedule="simple", order=order,
+    occ = dev.intersect(rays, dm.TraversalOptions(precision=precision, schedule=schedule, order=order,
                                                   mode="occluded", leaf_precision="f64"), np.float64)
     assert np.array_equal(occ["tri"] >= 0, hit)
     # the filter removed: the device query is the unfiltered one again
@@ -56,16 +58,17 @@ def test_filtered_device_equals_oracle(ctx, oracle, name, mapname, precision, or
 
 def test_filtered_scene_on_every_path(ctx):
     """A filtered scene runs its filter's passes on every path: a wavefront
-    query takes the one-thread-per-ray schedule (the filter's), the server
-    serves it, the path tracer renders it; each equals the explicit simple
-    schedule's answer."""
+    query (every round count, the rays that took a rejected crossing answered
+    again by the one-thread-per-ray schedule), the server, the path tracer;
+    each equals the explicit simple schedule's answer."""
     sc = scenes.quad_scene(16)
     dev = dm.Scene.from_synthetic(ctx, sc)
     rays = scenes.quad_camera_rays(24, 24)
     dev.set_opacity(checker(4))
     simple = dev.intersect(rays, dm.TraversalOptions(schedule="simple", leaf_precision="f64"), np.float32)
-    wave = dev.intersect(rays, dm.TraversalOptions(leaf_precision="f64"), np.float32)
-    assert wave.tobytes() == simple.tobytes()
+    for rounds in (0, 1, 3):
+        wave = dev.intersect(rays, dm.TraversalOptions(leaf_precision="f64", rounds=rounds), np.float32)
+        assert wave.tobytes() == simple.tobytes()
     unfiltered = dm.Scene.from_synthetic(ctx, sc).intersect(rays, dm.TraversalOptions(leaf_precision="f64"),
                                                              np.float32)
     assert (unfiltered["tri"] != simple["tri"]).sum() > 10  # the filter culled crossings
