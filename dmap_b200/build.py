@@ -5,8 +5,8 @@ reference (pyramid.cu, setup.cu, walk64.cu, walk32_exact.cu for the paths
 that run the FP64 leaf, shade.cu, tess.cu, emitter.cu)
 are compiled with -fmad=false so that each double operation rounds on its
 own, as the reference's CPU build does; FP32 code there asks for fused
-multiply-adds explicitly (fmaf, __fmaf_ru). walk32.cu (the FP32 walk and
-leaf rounds) is compiled with contraction.
+multiply-adds explicitly (fmaf, __fmaf_ru). walk32.cu (the FP32 walk
+rounds) is compiled with contraction.
 Usage: python -m dmap_b200.build [-j N] [--force]
 """
 from __future__ import annotations

@@ -1,7 +1,8 @@
 // The FP32 query's schedule and its contracted launches (compiled with FMA
-// contraction): the walk rounds and the FP32 leaf rounds, whose arithmetic is
-// conservative by its error bounds or judged by tolerance. The launches that
-// must round like the reference are in walk32_exact.cu.
+// contraction): the walk rounds, whose arithmetic is conservative by its
+// error bounds, and whose rounding never reaches a result (every leaf cell
+// the walk reaches is re-tested in FP64 before its leaf runs). The launches
+// that must round the same way wherever they run are in walk32_exact.cu.
 #include "walk32.cuh"
 
 namespace dmapk
@@ -35,23 +36,6 @@ cudaError_t walk_round(const Args &a, const int *q_in, int round, cudaStream_t s
         DMAP_ROUND_MODE(false);
 #undef DMAP_ROUND_MODE
 #undef DMAP_ROUND
-    return cudaGetLastError();
-}
-
-template <typename R, typename H, typename Fp>
-cudaError_t leaf32(const Args &a, int round, int *q_out, cudaStream_t stream)
-{
-    const int lgrid = sm_count() * 4;
-    const R *rr = static_cast<const R *>(a.rays);
-    H *hh = static_cast<H *>(a.hits);
-    RayState *states = static_cast<RayState *>(a.states);
-    LeafJob *leaves = static_cast<LeafJob *>(a.leaves);
-    if (a.stats)
-        wave_leaf32<true, R, H, Fp><<<lgrid, 128, 0, stream>>>(a.t32, a.t64, a.assets, rr, a.opt, hh, a.stats, states,
-                                                              leaves, round, q_out, a.counters, a.rerun);
-    else
-        wave_leaf32<false, R, H, Fp><<<lgrid, 128, 0, stream>>>(a.t32, a.t64, a.assets, rr, a.opt, hh, nullptr,
-                                                               states, leaves, round, q_out, a.counters, a.rerun);
     return cudaGetLastError();
 }
 

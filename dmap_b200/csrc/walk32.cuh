@@ -34,14 +34,14 @@
 //
 // The kernels live in this header and are instantiated by two translation
 // units (walk32_launch.h lists which launches each one owns):
-//  - walk32.cu, compiled with FMA contraction: the walk rounds and the FP32
-//    leaf rounds, whose arithmetic is conservative by its error bounds or
-//    judged by tolerance, so a fused multiply-add (one rounding instead of
-//    two) only tightens it;
+//  - walk32.cu, compiled with FMA contraction: the walk rounds, whose
+//    arithmetic is conservative by its error bounds, so a fused multiply-add
+//    (one rounding instead of two) stays inside them, and whose rounding
+//    never reaches a result (every leaf cell is re-tested in FP64);
 //  - walk32_exact.cu, compiled with -fmad=false: everything that must round
-//    like the reference, that is every path that runs the FP64 leaf (the
-//    simple schedule, the last walk with leaves inline, the FP64 leaf
-//    rounds) and the FP64 re-test of parked cells.
+//    like the reference or the same way wherever it runs: the simple
+//    schedule, the last walk with leaves inline, the leaf rounds of both
+//    leaves and the FP64 re-test of parked cells.
 // FP32 code asks for fused multiply-adds explicitly (fmaf) where its bounds
 // are written for one.
 #pragma once

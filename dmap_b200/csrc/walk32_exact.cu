@@ -1,6 +1,9 @@
-// The FP32 query's launches that must round like the reference (compiled
-// with -fmad=false): the simple schedule, the last walk with its leaves
-// inline, the FP64 re-test of parked cells and the FP64 leaf rounds.
+// The FP32 query's launches that must round like the reference, or the same
+// way wherever they run (compiled with -fmad=false): the simple schedule, the
+// last walk with its leaves inline, the FP64 re-test of parked cells, and the
+// leaf rounds of both leaves (the FP32 leaf also runs inline in the last
+// walk, so both places round alike and a ray's answer does not depend on the
+// round it finishes in).
 #include "walk32.cuh"
 
 namespace dmapk
@@ -81,11 +84,29 @@ cudaError_t leaf64(const Args &a, int round, int *q_out, cudaStream_t stream)
     return cudaGetLastError();
 }
 
+template <typename R, typename H, typename Fp>
+cudaError_t leaf32(const Args &a, int round, int *q_out, cudaStream_t stream)
+{
+    const int lgrid = sm_count() * 4;
+    const R *rr = static_cast<const R *>(a.rays);
+    H *hh = static_cast<H *>(a.hits);
+    RayState *states = static_cast<RayState *>(a.states);
+    LeafJob *leaves = static_cast<LeafJob *>(a.leaves);
+    if (a.stats)
+        wave_leaf32<true, R, H, Fp><<<lgrid, 128, 0, stream>>>(a.t32, a.t64, a.assets, rr, a.opt, hh, a.stats, states,
+                                                              leaves, round, q_out, a.counters, a.rerun);
+    else
+        wave_leaf32<false, R, H, Fp><<<lgrid, 128, 0, stream>>>(a.t32, a.t64, a.assets, rr, a.opt, hh, nullptr,
+                                                               states, leaves, round, q_out, a.counters, a.rerun);
+    return cudaGetLastError();
+}
+
 #define DMAP_W32_EXACT(R, H, Fp)                                                                                    \
     template cudaError_t simple<R, H, Fp>(const Args &, cudaStream_t);                                              \
     template cudaError_t simple_rerun<R, H, Fp>(const Args &, cudaStream_t);                                        \
     template cudaError_t walk_drain<R, H, Fp>(const Args &, const int *, int, cudaStream_t);                        \
-    template cudaError_t leaf64<R, H, Fp>(const Args &, int, int *, cudaStream_t);
+    template cudaError_t leaf64<R, H, Fp>(const Args &, int, int *, cudaStream_t);                                  \
+    template cudaError_t leaf32<R, H, Fp>(const Args &, int, int *, cudaStream_t);
 DMAP_W32_EXACT(float, dmapdev::Hit32, float)
 DMAP_W32_EXACT(float, dmapdev::Hit64, double)
 DMAP_W32_EXACT(double, dmapdev::Hit32, float)

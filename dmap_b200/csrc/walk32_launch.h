@@ -1,9 +1,8 @@
 // The FP32 query's launches, split between the two translation units that
 // instantiate walk32.cuh: walk32.cu (contracted FP32 arithmetic: the walk
-// rounds, the FP32 leaf rounds, and the schedule that orders the launches)
-// and walk32_exact.cu (-fmad=false: the simple schedule, the last walk with
-// its leaves inline, the FP64 re-test of parked cells and the FP64 leaf
-// rounds). Each entry is instantiated for the ray / hit record types
+// rounds, and the schedule that orders the launches) and walk32_exact.cu
+// (-fmad=false: the simple schedule, the last walk with its leaves inline,
+// the FP64 re-test of parked cells and the leaf rounds of both leaves). Each entry is instantiated for the ray / hit record types
 // (R, H, Fp) = (float | double, Hit32 | Hit64, float | double).
 #pragma once
 #include "launch.h"
@@ -45,12 +44,12 @@ template <typename R>
 cudaError_t filter(const Args &a, int round, cudaStream_t stream);
 template <typename R, typename H, typename Fp>
 cudaError_t leaf64(const Args &a, int round, int *q_out, cudaStream_t stream);
+template <typename R, typename H, typename Fp>
+cudaError_t leaf32(const Args &a, int round, int *q_out, cudaStream_t stream);
 
 // walk32.cu
 template <typename R, typename H, typename Fp>
 cudaError_t walk_round(const Args &a, const int *q_in, int round, cudaStream_t stream);
-template <typename R, typename H, typename Fp>
-cudaError_t leaf32(const Args &a, int round, int *q_out, cudaStream_t stream);
 
 } // namespace w32
 } // namespace dmapk
