@@ -20,17 +20,24 @@ __device__ __forceinline__ void ray_inverse(const double *d, double *inv)
 }
 
 // max(t_min, max over axes with d != 0 of min(ta, tb)), ta = (lo - o) / d
-// and tb = (hi - o) / d as products with 1 / d.
-__device__ __forceinline__ double entry_key(const TriDev &T, const double *o, const double *d, const double *inv,
-                                            double t_min)
+// and tb = (hi - o) / d as products with 1 / d, over the box lo .. hi.
+__device__ __forceinline__ double entry_key(const double *lo, const double *hi, const double *o, const double *d,
+                                            const double *inv, double t_min)
 {
     double key = t_min;
     for (int a = 0; a < 3; ++a)
         if (d[a] != 0.0) {
-            const double ta = (T.box_lo[a] - o[a]) * inv[a], tb = (T.box_hi[a] - o[a]) * inv[a];
+            const double ta = (lo[a] - o[a]) * inv[a], tb = (hi[a] - o[a]) * inv[a];
             key = dmax(key, dmin(ta, tb));
         }
     return key;
+}
+
+// The key of a triangle's object box.
+__device__ __forceinline__ double entry_key(const TriDev &T, const double *o, const double *d, const double *inv,
+                                            double t_min)
+{
+    return entry_key(T.box_lo, T.box_hi, o, d, inv, t_min);
 }
 
 // (key, t) comes after the cursor (ck, ct)

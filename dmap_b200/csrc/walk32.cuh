@@ -325,6 +325,9 @@ struct RayState
     int cl, ci, cj, el, ei, ej;
     int nah, lah;
     unsigned mask[kMaskWords];
+    // scenes of more than 256 triangles: the buffered candidates, kept
+    // across parks so a resumed ray does not walk the tree again
+    d32::NearBuf buf;
 };
 // Up to kCollect consecutive leaves of one triangle's walk, in walk order.
 // The walk goes on past a leaf with the t_max it has (it cannot know the
@@ -392,6 +395,20 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     // loops are never compiled into the kernels of larger scenes
     constexpr bool use_mask = !TREE;
     const d32::BvhView bvh = {opt.bvh_nodes, opt.bvh_tri, opt.bvh_range, opt.bvh_n_nodes};
+    // scenes of up to 256 triangles: their object boxes in shared memory
+    // (outward FP32 for the box tests, FP64 for the nearest order's keys),
+    // which every candidate test of the CTA reads
+    constexpr int kStaged = TREE ? 1 : 32 * kMaskWords;
+    __shared__ float s_box32[6 * kStaged];
+    __shared__ double s_box64[6 * kStaged];
+    if (!TREE) {
+        for (int k = threadIdx.x; k < 6 * n_tri; k += blockDim.x) {
+            const int t = k / 6, c = k - 6 * t;
+            s_box32[k] = c < 3 ? tris32[t].box_lo[c] : tris32[t].box_hi[c - 3];
+            s_box64[k] = c < 3 ? tris64[t].box_lo[c] : tris64[t].box_hi[c - 3];
+        }
+        __syncthreads();
+    }
     // items of this round: every ray in round 0, else the resume queue
     unsigned long long count = round == 0 ? (unsigned long long)n : *round_ctr(ctr, round - 1, 3);
     if (round == 0 && opt.n_dev && (unsigned long long)*opt.n_dev < count)
@@ -405,7 +422,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
     double ckey = -INFINITY;
     int cidx = -1;
     // the triangle tree (TREE): the lane's buffered candidates, refilled
-    // from the ray's cursor for each ray it takes
+    // from the ray's cursor for a fresh ray, kept in the ray's state across
+    // parks
     d32::NearBuf nbuf;
     nbuf.n = -1;
     nbuf.pos = 0;
@@ -444,6 +462,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
 #pragma unroll
         for (int w = 0; w < kMaskWords; ++w)
             s.mask[w] = mask[w];
+        if (TREE)
+            s.buf = nbuf;
         unsigned long long slot = atomicAdd(round_ctr(ctr, round, 1), 1ull);
         LeafJob job;
         job.ray = ray;
@@ -510,6 +530,8 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
 #pragma unroll
                         for (int w = 0; w < kMaskWords; ++w)
                             mask[w] = s.mask[w];
+                        if (TREE)
+                            nbuf = s.buf;
                         // back into the walk just after the leaf (displaced_intersector.cpp:229)
                         const TriDev32 &T = tris32[tri];
                         float t1 = __double2float_ru(t_max);
@@ -545,10 +567,10 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                 float s_tmin = __shfl_sync(FULL, tmin_f, src);
                 float s_tmax = __shfl_sync(FULL, __double2float_ru(t_max), src);
 #pragma unroll 1
-                for (int w = 0; w < kMaskWords; ++w) {
+                for (int w = 0; w < ((n_tri + 31) >> 5); ++w) {
                     int t = 32 * w + lane;
                     float t1 = s_tmax;
-                    bool pass = t < n_tri && object_box(tris32[t], so, sd, sv, s_tmin, t1);
+                    bool pass = t < n_tri && box_pass(s_box32 + 6 * t, s_box32 + 6 * t + 3, so, sd, sv, s_tmin, t1);
                     unsigned bits = __ballot_sync(FULL, pass);
                     if (lane == src) {
 #pragma unroll
@@ -581,31 +603,46 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     if (err)
                         atomicOr(status, dmapdev::kStatusCapped);
                 } else {
-                    // takes t when it is the best so far: one bit per
-                    // triangle whose box the ray met, each re-tested with
-                    // the current t_max
-                    auto consider = [&](int t) {
-                        const double key = d64::entry_key(tris64[t], o, d, inv, t_min);
-                        if (!d64::after_cursor(key, t, ckey, cidx) || !d64::before_best(key, t, bk, bt))
-                            return;
-                        float tt = tmf;
-                        if (!object_box(tris32[t], of, df, invf, tmin_f, tt))
-                            return;
-                        bk = key;
-                        bt = t;
-                        t1 = tt;
-                    };
+                    // the best (key, index) past the cursor among the bits
+                    // of the ray's mask (boxes met at the ray's start), each
+                    // box re-tested with the current t_max first; a bit whose
+                    // box no longer passes, or whose key is not past the
+                    // cursor, is cleared for good (t_max only shrinks, the
+                    // cursor only advances), so later picks scan fewer
+                    const int words = (n_tri + 31) >> 5;
 #pragma unroll 1
-                    for (int w = 0; w < kMaskWords; ++w) {
+                    for (int w = 0; w < words; ++w) {
                         unsigned bits = mask[0];
 #pragma unroll
                         for (int q = 1; q < kMaskWords; ++q)
                             bits = w == q ? mask[q] : bits;
+                        unsigned drop = 0u;
                         while (bits) {
-                            const int item = 32 * w + __ffs(bits) - 1;
+                            const int b = __ffs(bits) - 1;
                             bits &= bits - 1;
-                            if (item < n_tri)
-                                consider(item);
+                            const int t = 32 * w + b;
+                            float e = tmin_f, tt = tmf;
+                            if (!box_range(s_box32 + 6 * t, s_box32 + 6 * t + 3, of, df, invf, e, tt)) {
+                                drop |= 1u << b;
+                                continue;
+                            }
+                            if (bt >= 0 && (double)e > bk)
+                                continue; // its key (at least e) is past the best
+                            const double key = d64::entry_key(s_box64 + 6 * t, s_box64 + 6 * t + 3, o, d, inv, t_min);
+                            if (!d64::after_cursor(key, t, ckey, cidx)) {
+                                drop |= 1u << b;
+                                continue;
+                            }
+                            if (!d64::before_best(key, t, bk, bt))
+                                continue;
+                            bk = key;
+                            bt = t;
+                            t1 = tt;
+                        }
+                        if (drop) {
+#pragma unroll
+                            for (int q = 0; q < kMaskWords; ++q)
+                                mask[q] = w == q ? (mask[q] & ~drop) : mask[q];
                         }
                     }
                 }
@@ -647,7 +684,7 @@ __global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
                     }
                     tri = (w << 5) + __ffs(bits) - 1;
                     t1 = __double2float_ru(t_max); // the candidate again, with the current t_max
-                    if (tri < n_tri && object_box(tris32[tri], of, df, invf, tmin_f, t1)) {
+                    if (tri < n_tri && box_pass(s_box32 + 6 * tri, s_box32 + 6 * tri + 3, of, df, invf, tmin_f, t1)) {
                         hit_box = true;
                         break;
                     }
