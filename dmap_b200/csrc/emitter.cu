@@ -571,7 +571,7 @@ __global__ void pdf_kernel(Emit E, const int32_t *__restrict__ tri_of, const dou
     }
 }
 
-// ---- DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) ----------
+// ---- DisplacedEmitterLight (displaced_emitter_light.cpp:20-116) ----------
 // The sampler seen from a shading point (p, n): a sample as a direction,
 // distance and solid-angle pdf, and the pdf of a direction from the (u, v)
 // it reaches, directly or by the walk of the emitter's triangle

@@ -447,7 +447,7 @@ dmap_status dmap_emitter_pdf_host(dmap_emitter *emitter, const int32_t *tri, con
 
 /*
  * The displaced emitter as a light seen from shading points
- * (DisplacedEmitterLight, displaced_emitter_light.cpp:20-117; the light of
+ * (DisplacedEmitterLight, displaced_emitter_light.cpp:20-116; the light of
  * an emitter created with variant AREA / PRODUCT / PRODUCT_GEOMETRY is the
  * reference's AreaDescent / ProductDescent / ReceiverDescent, the last with
  * emitter_cosine 0 as the reference's light sets it). shade: 6 doubles per

@@ -2477,7 +2477,7 @@ double o_emitter_pdf_area(const o_emitter *e, double u, double v, const double *
     return p / sqrt_det;
 }
 
-/* ---- DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) ---------
+/* ---- DisplacedEmitterLight (displaced_emitter_light.cpp:20-116) ---------
  * The descent sampler as a light seen from a shading point (p, n): a sample
  * converted to a direction, distance and solid-angle pdf, and the pdf of a
  * direction from the (u, v) it reaches. The light's sampler is the

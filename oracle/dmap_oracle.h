@@ -146,7 +146,7 @@ int o_emitter_sample(const o_emitter *e, const float *u, int n_u, const double *
 double o_emitter_pdf_uv(const o_emitter *e, double u, double v, const double *recv6);
 double o_emitter_pdf_area(const o_emitter *e, double u, double v, const double *recv6);
 double o_emitter_leaf_prob(const o_emitter *e, int64_t i, int64_t j, const double *recv6);
-/* DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) over the
+/* DisplacedEmitterLight (displaced_emitter_light.cpp:20-116) over the
  * emitter's sampler, seen from shade6 = (p, n): a sample as out16 = u, v,
  * y[3], n_y[3], wi[3], dist, pdf_area, pdf_omega, Le, ok (returned); the
  * solid-angle pdf from (u, v); and by the walk of the emitter's triangle

@@ -300,7 +300,7 @@ class CpuEmitter:
     def leaf_prob(self, i, j, receiver=None):
         return self.lib._em_leaf_prob(self.h, i, j, _ptr(self._recv(receiver)))
 
-    # DisplacedEmitterLight (displaced_emitter_light.cpp:20-117) seen from
+    # DisplacedEmitterLight (displaced_emitter_light.cpp:20-116) seen from
     # shade = (p, n), 6 doubles
     def light_sample(self, u, shade):
         """(16 values u, v, y, n_y, wi, dist, pdf_area, pdf_omega, Le, ok)."""

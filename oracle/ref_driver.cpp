@@ -515,7 +515,7 @@ int r_emitter_light_sample(const r_emitter *e, const float *u, int n_u, const do
     return s.ok ? 1 : 0;
 }
 
-// DisplacedEmitterLight::pdf_omega_from_uv (displaced_emitter_light.cpp:103-117).
+// DisplacedEmitterLight::pdf_omega_from_uv (displaced_emitter_light.cpp:103-116).
 double r_emitter_light_pdf_uv(const r_emitter *e, const double *shade6, double u, double v)
 {
     return e->light->pdf_omega_from_uv(vec3d(shade6[0], shade6[1], shade6[2]),

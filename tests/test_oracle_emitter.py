@@ -100,7 +100,7 @@ def _shade_points(rng, n, centre, spread=1.5):
 
 @pytest.mark.parametrize("variant", ["area", "product", "product_geometry"])
 def test_light_wrapper_equals_reference(oracle, reference, scene, variant):
-    """DisplacedEmitterLight (displaced_emitter_light.cpp:20-117): light
+    """DisplacedEmitterLight (displaced_emitter_light.cpp:20-116): light
     samples seen from shading points, the solid-angle pdf from (u, v), and
     the pdf of a direction by the walk of the emitter's triangle
     (DisplacedAreaLight::pdf, displaced_area_light.cpp:174-186), the
