@@ -378,8 +378,15 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // One lane's walk from its parked or fresh state to the next leaf (parked,
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
+// The walk rounds are compiled for DMAP_WALK_MIN_BLOCKS CTAs per SM; the
+// last walk (INLINE_LEAF), which runs the few rays left with their leaves
+// inline, for DMAP_DRAIN_MIN_BLOCKS, so that the leaf it calls is not
+// squeezed into the rounds' register budget.
+#ifndef DMAP_DRAIN_MIN_BLOCKS
+#define DMAP_DRAIN_MIN_BLOCKS 2
+#endif
 template <bool ST, bool INLINE_LEAF, bool TREE, bool NEAR, typename R, typename H, typename Fp>
-__global__ void __launch_bounds__(128, DMAP_WALK_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, INLINE_LEAF ? DMAP_DRAIN_MIN_BLOCKS : DMAP_WALK_MIN_BLOCKS)
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
               H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,
