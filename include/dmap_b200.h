@@ -331,8 +331,10 @@ dmap_status dmap_surface_points_host(dmap_scene *scene, const void *hits_host, d
  * the map covers (the object whose material carries it); the others accept
  * every crossing. mask_host NULL removes the filter. The mask is copied.
  * FP32 queries on a filtered scene (dmap_intersect*, dmap_render and
- * the server alike) run the one-thread-per-ray schedule, whose triangle
- * walks take the filter's passes, whatever schedule the options name. While a server holds requests on the scene
+ * the server alike) take the filter's passes on either schedule: the
+ * wavefront answers without them and hands every ray that took a crossing
+ * the filter rejects to the one-thread-per-ray schedule, whose triangle
+ * walks take the passes. While a server holds requests on the scene
  * (queued or running), the filter cannot change: this call returns
  * DMAP_ERR_NOT_READY until they are done (dmap_server_drain); do not call it
  * concurrently with a submit on the same scene.
