@@ -3,6 +3,7 @@
 // C++ over the CUDA runtime; kernels live in pyramid.cu, setup.cu,
 // walk64.cu and walk32.cu.
 #include "api_internal.h"
+#include "instance.cuh"
 
 #include <algorithm>
 
@@ -273,8 +274,72 @@ dmap_status dmap_asset_pyramid_level(const dmap_asset *a, int level, int precisi
 
 // ---- scenes ----------------------------------------------------------------
 
+// Non-rigid instances (dmap_scene_create_instanced): per triangle 1 + its
+// instance (0: none), and the instance table (kInstDoubles each).
+struct InstanceSpec
+{
+    const int *tri_inst = nullptr;
+    std::vector<double> table;
+};
+
+// Moves the setup records of instanced triangles to world space where the
+// walk reads them: the object AABB becomes the AABB of its 8 corners moved
+// by the instance (widened by far more than their rounding), and the FP32
+// tangent transform takes the world ray directly (A Linv, origin L q0 + T).
+// The FP64 records stay in object space; the FP64 node test and the leaves
+// move the ray (instance.cuh).
+static void place_instances(std::vector<TriDev> &t64, std::vector<TriDev32> &t32, const InstanceSpec &spec)
+{
+    const int n_tri = (int)t64.size();
+    for (int k = 0; k < n_tri; ++k) {
+        const int inst = spec.tri_inst[k];
+        if (inst <= 0)
+            continue;
+        const double *xf = spec.table.data() + dmapdev::kInstDoubles * (inst - 1);
+        const double *L = xf, *Tr = xf + 9, *Li = xf + 12;
+        TriDev &T = t64[k];
+        TriDev32 &S = t32[k];
+        T.inst = inst;
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int c = 0; c < 8; ++c) {
+            const double p[3] = {(c & 1) ? T.box_hi[0] : T.box_lo[0], (c & 2) ? T.box_hi[1] : T.box_lo[1],
+                                 (c & 4) ? T.box_hi[2] : T.box_lo[2]};
+            for (int a = 0; a < 3; ++a) {
+                const double w = ((L[3 * a] * p[0] + L[3 * a + 1] * p[1]) + L[3 * a + 2] * p[2]) + Tr[a];
+                lo[a] = std::min(lo[a], w);
+                hi[a] = std::max(hi[a], w);
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            const double m = std::max(std::fabs(lo[a]), std::fabs(hi[a]));
+            const double pad = 1e-12 * (1.0 + m);
+            T.box_lo[a] = lo[a] - pad;
+            T.box_hi[a] = hi[a] + pad;
+            // the FP32 box as setup widens it (a few float ulps), rounded outward
+            const double fpad = 4.0 * 1.1920928955078125e-7 * (1.0 + m);
+            S.box_lo[a] = std::nextafter((float)(T.box_lo[a] - fpad), -INFINITY);
+            S.box_hi[a] = std::nextafter((float)(T.box_hi[a] + fpad), INFINITY);
+        }
+        double A2[3][3], q2[3];
+        for (int a = 0; a < 3; ++a) {
+            for (int b = 0; b < 3; ++b)
+                A2[a][b] = (T.A[a][0] * Li[b] + T.A[a][1] * Li[3 + b]) + T.A[a][2] * Li[6 + b];
+            q2[a] = ((L[3 * a] * T.q0[0] + L[3 * a + 1] * T.q0[1]) + L[3 * a + 2] * T.q0[2]) + Tr[a];
+        }
+        for (int a = 0; a < 3; ++a) {
+            S.q0[a] = q2[a];
+            S.q0f[a] = (float)q2[a];
+            for (int b = 0; b < 3; ++b) {
+                S.A[a][b] = A2[a][b];
+                S.Af[a][b] = (float)A2[a][b];
+            }
+        }
+    }
+}
+
 static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, int n_assets, const int *tri_asset,
-                                const double *tris, int stride, int n_tri, dmap_scene **out)
+                                const double *tris, int stride, int n_tri, dmap_scene **out,
+                                const InstanceSpec *inst = nullptr)
 {
     if (!ctx || !assets || n_assets <= 0 || !tri_asset || !tris || n_tri <= 0 || !out)
         return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create: bad argument");
@@ -310,6 +375,7 @@ static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, in
         cudaFree(s->bvh_nodes_dev);
         cudaFree(s->bvh_tri_dev);
         cudaFree(s->bvh_range_dev);
+        cudaFree(s->inst_dev);
         delete s;
         return st;
     };
@@ -331,6 +397,21 @@ static dmap_status scene_create(dmap_context *ctx, dmap_asset *const *assets, in
     dmap_status st = sync_and_check(ctx, "dmap_scene_create");
     if (st != DMAP_OK)
         return cleanup(st);
+    if (inst) {
+        std::vector<TriDev> t64(n_tri);
+        std::vector<TriDev32> t32(n_tri);
+        if ((e = cudaMemcpy(t64.data(), s->tris_dev, sizeof(TriDev) * n_tri, cudaMemcpyDeviceToHost)) ||
+            (e = cudaMemcpy(t32.data(), s->tris32_dev, sizeof(TriDev32) * n_tri, cudaMemcpyDeviceToHost)))
+            return cleanup(cuda_fail(ctx, e, "dmap_scene_create_instanced: readback"));
+        place_instances(t64, t32, *inst);
+        if ((e = cudaMemcpy(s->tris_dev, t64.data(), sizeof(TriDev) * n_tri, cudaMemcpyHostToDevice)) ||
+            (e = cudaMemcpy(s->tris32_dev, t32.data(), sizeof(TriDev32) * n_tri, cudaMemcpyHostToDevice)) ||
+            (e = cudaMalloc((void **)&s->inst_dev, sizeof(double) * inst->table.size())) ||
+            (e = cudaMemcpy(s->inst_dev, inst->table.data(), sizeof(double) * inst->table.size(),
+                            cudaMemcpyHostToDevice)))
+            return cleanup(cuda_fail(ctx, e, "dmap_scene_create_instanced: instances"));
+        s->n_inst = (int)(inst->table.size() / dmapdev::kInstDoubles);
+    }
     if (n_tri > 256) {
         // the triangle tree of the candidate orders (bvh.cu), over the
         // outward FP32 boxes the walk tests
@@ -391,8 +472,7 @@ dmap_status dmap_scene_create_instanced(dmap_context *ctx, dmap_asset *const *as
     for (int o = 0; o < n_objects; ++o)
         if (object_first[o] < 0 || object_first[o + 1] < object_first[o])
             return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: object ranges must be ordered");
-    std::vector<double> wt;
-    std::vector<int> wa;
+    bool rigid = true;
     for (int k = 0; k < n_instances; ++k) {
         const int o = instance_object[k];
         if (o < 0 || o >= n_objects)
@@ -406,30 +486,64 @@ dmap_status dmap_scene_create_instanced(dmap_context *ctx, dmap_asset *const *as
             for (int b = 0; b < 3; ++b) {
                 const double dot = (M[4 * a] * M[4 * b] + M[4 * a + 1] * M[4 * b + 1]) + M[4 * a + 2] * M[4 * b + 2];
                 if (std::fabs(dot - (a == b ? 1.0 : 0.0)) > 1e-9)
-                    return fail(ctx, DMAP_ERR_UNSUPPORTED,
-                                "dmap_scene_create_instanced: only rigid transforms move the displaced surface "
-                                "exactly (a scale or shear would scale the heights)");
+                    rigid = false;
             }
+    }
+    std::vector<double> wt;
+    std::vector<int> wa, wi;
+    InstanceSpec spec;
+    for (int k = 0; k < n_instances; ++k) {
+        const int o = instance_object[k];
+        const double *M = to_world + 12 * (size_t)k;
+        if (!rigid) {
+            // a scale or shear does not move the displaced surface with its
+            // base triangles (the heights would scale): the instance keeps the
+            // object's triangles and takes the rays to object space
+            const double L[9] = {M[0], M[1], M[2], M[4], M[5], M[6], M[8], M[9], M[10]};
+            const double c00 = L[4] * L[8] - L[5] * L[7], c01 = L[5] * L[6] - L[3] * L[8], c02 = L[3] * L[7] - L[4] * L[6];
+            const double det = (L[0] * c00 + L[1] * c01) + L[2] * c02;
+            double scale = 0.0;
+            for (int q = 0; q < 9; ++q)
+                scale = std::max(scale, std::fabs(L[q]));
+            if (!(std::fabs(det) > 1e-12 * scale * scale * scale))
+                return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: singular transform");
+            const double Li[9] = {c00 / det, (L[2] * L[7] - L[1] * L[8]) / det, (L[1] * L[5] - L[2] * L[4]) / det,
+                                  c01 / det, (L[0] * L[8] - L[2] * L[6]) / det, (L[2] * L[3] - L[0] * L[5]) / det,
+                                  c02 / det, (L[1] * L[6] - L[0] * L[7]) / det, (L[0] * L[4] - L[1] * L[3]) / det};
+            spec.table.insert(spec.table.end(), L, L + 9);
+            spec.table.insert(spec.table.end(), {M[3], M[7], M[11]});
+            spec.table.insert(spec.table.end(), Li, Li + 9);
+            spec.table.push_back(det > 0.0 ? 1.0 : -1.0);
+        }
         auto point = [&](const double *p, double *q, bool translate) {
             for (int a = 0; a < 3; ++a)
                 q[a] = ((M[4 * a] * p[0] + M[4 * a + 1] * p[1]) + M[4 * a + 2] * p[2]) + (translate ? M[4 * a + 3] : 0.0);
         };
         for (int t = object_first[o]; t < object_first[o + 1]; ++t) {
             const double *r = tris + 24 * (size_t)t;
-            double w[24];
-            for (int v = 0; v < 3; ++v) {
-                point(r + 3 * v, w + 3 * v, true);      // p0, p1, p2
-                point(r + 9 + 3 * v, w + 9 + 3 * v, false); // m0, m1, m2
+            if (rigid) {
+                double w[24];
+                for (int v = 0; v < 3; ++v) {
+                    point(r + 3 * v, w + 3 * v, true);      // p0, p1, p2
+                    point(r + 9 + 3 * v, w + 9 + 3 * v, false); // m0, m1, m2
+                }
+                for (int q = 18; q < 24; ++q)
+                    w[q] = r[q];
+                wt.insert(wt.end(), w, w + 24);
+            } else {
+                wt.insert(wt.end(), r, r + 24);
+                wi.push_back(k + 1);
             }
-            for (int q = 18; q < 24; ++q)
-                w[q] = r[q];
-            wt.insert(wt.end(), w, w + 24);
             wa.push_back(tri_asset[t]);
         }
     }
     if (wa.empty())
         return fail(ctx, DMAP_ERR_INVALID, "dmap_scene_create_instanced: no triangles");
-    return dmap_scene_create(ctx, assets, n_assets, wa.data(), wt.data(), (int)wa.size(), out);
+    if (rigid)
+        return dmap_scene_create(ctx, assets, n_assets, wa.data(), wt.data(), (int)wa.size(), out);
+    spec.tri_inst = wi.data();
+    return scene_create(ctx, assets, n_assets, wa.data(), wt.data(), dmapk::kVertexRecord, (int)wa.size(), out,
+                        &spec);
 }
 
 void dmap_scene_destroy(dmap_scene *s)
@@ -453,6 +567,7 @@ void dmap_scene_destroy(dmap_scene *s)
     cudaFree(s->bvh_nodes_dev);
     cudaFree(s->bvh_tri_dev);
     cudaFree(s->bvh_range_dev);
+    cudaFree(s->inst_dev);
     cudaFree(s->op_mask_dev);
     cudaFree(s->op_tri_dev);
     delete s;
@@ -569,6 +684,7 @@ dmap_status dmapi::check_query(dmap_scene *s, dmap_dtype ray_dtype, int64_t n, c
     q.bvh_nodes = reinterpret_cast<const float4 *>(s->bvh_nodes_dev);
     q.bvh_tri = reinterpret_cast<const float4 *>(s->bvh_tri_dev);
     q.bvh_range = reinterpret_cast<const int4 *>(s->bvh_range_dev);
+    q.inst_xf = s->inst_dev;
     q.bvh_n_nodes = s->bvh_n_nodes;
     apply_filter(s, q);
     return DMAP_OK;

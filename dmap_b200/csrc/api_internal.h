@@ -78,6 +78,8 @@ struct dmap_scene
     float *bvh_nodes_dev = nullptr; // more than 256 triangles: the triangle tree the candidate orders walk
     float *bvh_tri_dev = nullptr;
     int *bvh_range_dev = nullptr;
+    double *inst_dev = nullptr; // non-rigid instances: their transforms (instance.cuh), else null
+    int n_inst = 0;
     int bvh_n_nodes = 0;
     std::vector<TriDev> tris_host;
     bool all_f64 = true;

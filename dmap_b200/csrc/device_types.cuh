@@ -51,6 +51,9 @@ struct TriDev
     double h_min, h_max;
     int root_level, n_roots, asset, status;
     int roots_i[4], roots_j[4];
+    // 1 + the index of the non-rigid instance the triangle belongs to
+    // (instance.cuh), 0 for a triangle placed in world space
+    int inst, inst_pad;
 };
 
 // The FP32 record: the same geometry rounded to float, plus the FP64 frame

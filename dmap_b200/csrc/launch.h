@@ -29,6 +29,9 @@ struct QueryOpts
     // Scenes of more than 256 triangles: the tree over the triangles' FP32
     // boxes that both candidate orders walk (bvh.cuh gives the layout), bvh_n_nodes
     // inner nodes of 4 float4, 2 float4 per triangle list position.
+    // Non-rigid instances: kInstDoubles per instance (instance.cuh), indexed
+    // by TriDev::inst - 1; null when the scene has none.
+    const double *inst_xf = nullptr;
     const float4 *bvh_nodes = nullptr;
     const float4 *bvh_tri = nullptr;
     const int4 *bvh_range = nullptr;

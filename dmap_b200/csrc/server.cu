@@ -233,6 +233,7 @@ struct dmap_server
             qq.bvh_nodes = reinterpret_cast<const float4 *>(first->scene->bvh_nodes_dev);
             qq.bvh_tri = reinterpret_cast<const float4 *>(first->scene->bvh_tri_dev);
             qq.bvh_range = reinterpret_cast<const int4 *>(first->scene->bvh_range_dev);
+            qq.inst_xf = first->scene->inst_dev;
             qq.bvh_n_nodes = first->scene->bvh_n_nodes;
             qq.ray_dtype = qq.hit_dtype = 0;
             apply_filter(first->scene, qq); // a filtered scene's batch runs the filter's passes

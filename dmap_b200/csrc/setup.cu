@@ -285,6 +285,8 @@ __global__ void setup_kernel(const double *__restrict__ tris, int stride, const 
     TriDev T;
     T.asset = tri_asset[k];
     T.status = 0;
+    T.inst = 0;
+    T.inst_pad = 0;
     if (!init_triangle(T, tris + stride * (size_t)k, stride == dmapk::kChartRecord)) {
         T.status = 1;
         atomicOr(status, dmapdev::kStatusBadInput);

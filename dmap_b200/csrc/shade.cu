@@ -5,6 +5,7 @@
 // normal oriented along the base face's winding, the surface tangents scaled
 // by the object's uv map, and the object's uv
 // (DisplacedObject::object_uv, scene_spec.cpp:382-388).
+#include "instance.cuh"
 #include "api_internal.h"
 #include "f64_math.cuh"
 
@@ -23,7 +24,8 @@ __device__ __forceinline__ v3 eigen_normalized(v3 a)
 
 template <typename H>
 __global__ void surface_points_kernel(const TriDev *__restrict__ tris, const AssetDev *__restrict__ assets,
-                                      const H *__restrict__ hits, int64_t n, dmap_uv_map map, double *out)
+                                      const H *__restrict__ hits, int64_t n, dmap_uv_map map, double *out,
+                                      const double *__restrict__ inst_xf)
 {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n)
@@ -58,6 +60,19 @@ __global__ void surface_points_kernel(const TriDev *__restrict__ tris, const Ass
         ng = eigen_normalized(wn);
     double su = map.uv_scale[0], sv = map.flip_v ? -map.uv_scale[1] : map.uv_scale[1];
     v3 dpdu = mul3(su, Ss), dpdv = mul3(sv, St);
+    if (T.inst) {
+        // a non-rigid instance's point and tangents moved by its transform,
+        // the normal as instance.cuh moves it
+        const double *xf = inst_xf + dmapdev::kInstDoubles * (T.inst - 1), *L = xf, *Tr = xf + 9;
+        auto lin = [&](v3 x) {
+            return V3((L[0] * x.x + L[1] * x.y) + L[2] * x.z, (L[3] * x.x + L[4] * x.y) + L[5] * x.z,
+                      (L[6] * x.x + L[7] * x.y) + L[8] * x.z);
+        };
+        p = add3(lin(p), V3(Tr[0], Tr[1], Tr[2]));
+        dpdu = lin(dpdu);
+        dpdv = lin(dpdv);
+        dmapdev::world_normal(xf, ng);
+    }
     double uvx = (s - map.uv_offset[0]) / map.uv_scale[0], uvy = (t - map.uv_offset[1]) / map.uv_scale[1];
     if (map.flip_v)
         uvy = 1.0 - uvy;
@@ -88,10 +103,10 @@ dmap_status dmap_surface_points(dmap_scene *s, const void *hits_dev, dmap_dtype 
     unsigned grid = (unsigned)((n + 127) / 128);
     if (hit_dtype == DMAP_F64)
         surface_points_kernel<dmapdev::Hit64><<<grid, 128, 0, st>>>(
-            s->tris_dev, s->assets_dev, static_cast<const dmapdev::Hit64 *>(hits_dev), n, m, out_dev);
+            s->tris_dev, s->assets_dev, static_cast<const dmapdev::Hit64 *>(hits_dev), n, m, out_dev, s->inst_dev);
     else
         surface_points_kernel<dmapdev::Hit32><<<grid, 128, 0, st>>>(
-            s->tris_dev, s->assets_dev, static_cast<const dmapdev::Hit32 *>(hits_dev), n, m, out_dev);
+            s->tris_dev, s->assets_dev, static_cast<const dmapdev::Hit32 *>(hits_dev), n, m, out_dev, s->inst_dev);
     DMAP_CUDA(ctx, cudaGetLastError());
     ctx->launches += 1;
     return DMAP_OK;

@@ -446,6 +446,8 @@ dmap_status dmap_tessellate_uniform(dmap_scene *s, int n, float *vertices_dev, f
 {
     if (!s || n < 1 || !vertices_dev || !texcoords_dev || !normals_dev || !indices_dev)
         return fail(s ? s->ctx : nullptr, DMAP_ERR_INVALID, "dmap_tessellate_uniform: bad argument");
+    if (s->n_inst)
+        return fail(s->ctx, DMAP_ERR_UNSUPPORTED, "dmap_tessellate_uniform: scenes with non-rigid instances");
     dmap_context *ctx = s->ctx;
     const int64_t V = (int64_t)(n + 1) * (n + 2) / 2, F = (int64_t)n * n;
     const int64_t nv = V * s->n_tri, nf = F * s->n_tri;
@@ -507,6 +509,8 @@ dmap_status dmap_tessellate_texel(dmap_scene *s, int m, int64_t capacity, float 
     if (!s || m < 1 || !n_faces || capacity < 0 ||
         (vertices_dev && (!texcoords_dev || !normals_dev || !faces_dev)))
         return fail(s ? s->ctx : nullptr, DMAP_ERR_INVALID, "dmap_tessellate_texel: bad argument");
+    if (s->n_inst)
+        return fail(s->ctx, DMAP_ERR_UNSUPPORTED, "dmap_tessellate_texel: scenes with non-rigid instances");
     dmap_context *ctx = s->ctx;
     *n_faces = 0;
     if (s->n_tri == 0)

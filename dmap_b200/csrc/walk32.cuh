@@ -51,6 +51,7 @@
 #include "leaf32.cuh"
 #include "order.cuh"
 #include "filter.cuh"
+#include "instance.cuh"
 
 namespace
 {
@@ -119,14 +120,25 @@ __device__ __noinline__ bool leaf_cell(const TriDev32 &T32, const TriDev &T, con
                                        const double *d, double t_min, double t_max, int i, int j, d64::hit64 &h,
                                        int &flags, int64_t *st, const dmapk::QueryOpts &opt)
 {
+    // an instanced triangle meets the ray in its object space (instance.cuh)
+    double oo[3], od[3];
+    if (T.inst) {
+        dmapdev::object_ray(opt.inst_xf + dmapdev::kInstDoubles * (T.inst - 1), o, d, oo, od);
+        o = oo;
+        d = od;
+    }
+    bool ok;
     if (opt.leaf_precision != 1) {
         flags = DMAP_HIT_FP64_LEAF;
-        return leaf64(T, g, o, d, t_min, t_max, i, j, h, st, opt);
+        ok = leaf64(T, g, o, d, t_min, t_max, i, j, h, st, opt);
+    } else {
+        d64::v3 O = d64::V3(o[0], o[1], o[2]), D = d64::V3(d[0], d[1], d[2]);
+        ok = d64::leaf_cell_admitted(T, g, O, D, t_min, t_max, i, j, opt) &&
+             l32::intersect_newton32(T, T32, g, O, D, t_min, t_max, i, j, opt.polish_cond, h, flags, st);
     }
-    d64::v3 O = d64::V3(o[0], o[1], o[2]), D = d64::V3(d[0], d[1], d[2]);
-    if (!d64::leaf_cell_admitted(T, g, O, D, t_min, t_max, i, j, opt))
-        return false;
-    return l32::intersect_newton32(T, T32, g, O, D, t_min, t_max, i, j, opt.polish_cond, h, flags, st);
+    if (ok && T.inst)
+        dmapdev::world_normal(opt.inst_xf + dmapdev::kInstDoubles * (T.inst - 1), h.ng);
+    return ok;
 }
 
 // DisplacedIntersector::intersect with the FP32 node test.
@@ -859,6 +871,14 @@ __global__ void __launch_bounds__(128)
         t_max = states[job.ray].t_max;
         const TriDev &T = tris64[job.tri];
         const AssetDev &g = assets[T.asset];
+        if (T.inst) {
+            double oo[3], od[3];
+            dmapdev::object_ray(opt.inst_xf + dmapdev::kInstDoubles * (T.inst - 1), o, d, oo, od);
+            for (int a = 0; a < 3; ++a) {
+                o[a] = oo[a];
+                d[a] = od[a];
+            }
+        }
         d64::tray r = d64::tangent_ray64(T, d64::V3(o[0], o[1], o[2]), d64::V3(d[0], d[1], d[2]), t_min, t_max);
         int m = 0;
 #pragma unroll 1
@@ -934,6 +954,15 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
                     } else {
                         double o[3], d[3];
                         load_ray(rays, ray, o, d, t_min, t_max);
+                        if (tris64[tri].inst) {
+                            double oo[3], od[3];
+                            dmapdev::object_ray(opt.inst_xf + dmapdev::kInstDoubles * (tris64[tri].inst - 1), o, d,
+                                                oo, od);
+                            for (int a = 0; a < 3; ++a) {
+                                o[a] = oo[a];
+                                d[a] = od[a];
+                            }
+                        }
                         O = V3(o[0], o[1], o[2]);
                         D = V3(d[0], d[1], d[2]);
                         t_max = states[ray].t_max;
@@ -1036,6 +1065,8 @@ __global__ void __launch_bounds__(128, DMAP_LEAF_MIN_BLOCKS)
                 s.best_tri = tri;
                 s.flags |= kFoundInTri;
                 s.nah = s.lah = 0;
+                if (tris64[tri].inst)
+                    dmapdev::world_normal(opt.inst_xf + dmapdev::kInstDoubles * (tris64[tri].inst - 1), h.ng);
                 store_hit<H, Fp>(hits, ray, true, h, tri,
                                  DMAP_HIT_FP64_LEAF | ((s.flags & kCapped) ? DMAP_HIT_CAPPED : 0));
                 check_crossing(opt, tris64[tri], tri, h, ray, s.flags, ctr, rerun);
@@ -1103,6 +1134,15 @@ __global__ void __launch_bounds__(128, DMAP_LEAF32_MIN_BLOCKS)
                     } else {
                         double o[3], d[3];
                         load_ray(rays, ray, o, d, t_min, t_max);
+                        if (tris64[tri].inst) {
+                            double oo[3], od[3];
+                            dmapdev::object_ray(opt.inst_xf + dmapdev::kInstDoubles * (tris64[tri].inst - 1), o, d,
+                                                oo, od);
+                            for (int a = 0; a < 3; ++a) {
+                                o[a] = oo[a];
+                                d[a] = od[a];
+                            }
+                        }
                         O = V3(o[0], o[1], o[2]);
                         D = V3(d[0], d[1], d[2]);
                         t_max = states[ray].t_max;
@@ -1190,6 +1230,8 @@ __global__ void __launch_bounds__(128, DMAP_LEAF32_MIN_BLOCKS)
                 s.best_tri = tri;
                 s.flags |= kFoundInTri;
                 s.nah = s.lah = 0;
+                if (tris64[tri].inst)
+                    dmapdev::world_normal(opt.inst_xf + dmapdev::kInstDoubles * (tris64[tri].inst - 1), h.ng);
                 store_hit<H, Fp>(hits, ray, true, h, tri, fl | ((s.flags & kCapped) ? DMAP_HIT_CAPPED : 0));
                 check_crossing(opt, tris64[tri], tri, h, ray, s.flags, ctr, rerun);
                 if (opt.mode == 1) {

@@ -13,6 +13,7 @@
 #include "f64_walk.cuh"
 #include "order.cuh"
 #include "filter.cuh"
+#include "instance.cuh"
 #include "launch.h"
 
 namespace
@@ -24,8 +25,8 @@ using dmapdev::TriDev;
 // The intersect / occluded callback's passes over DisplacedIntersector::intersect
 // (displaced_geometry.cpp:53-106): a crossing the scene's filter rejects
 // raises t_min to its t and the triangle is walked again. No filter: one walk.
-__device__ bool triangle_filtered(const TriDev &T, int tri, const AssetDev &g, v3 o, v3 d, double t_min,
-                                  double t_max, const dmapk::QueryOpts &opt, hit64 &hit, int64_t *st)
+__device__ bool triangle_filtered_obj(const TriDev &T, int tri, const AssetDev &g, v3 o, v3 d, double t_min,
+                                      double t_max, const dmapk::QueryOpts &opt, hit64 &hit, int64_t *st)
 {
     if (!opt.op_mask)
         return triangle_intersect(T, g, o, d, t_min, t_max, opt, hit, st);
@@ -38,6 +39,24 @@ __device__ bool triangle_filtered(const TriDev &T, int tri, const AssetDev &g, v
         t_lo = hit.t; // the walk accepts t > t_min only
     }
     return false;
+}
+
+// The same for a triangle of a non-rigid instance: the ray moved to the
+// object's space first, the hit's normal moved back (instance.cuh).
+__device__ bool triangle_filtered(const TriDev &T, int tri, const AssetDev &g, v3 o, v3 d, double t_min,
+                                  double t_max, const dmapk::QueryOpts &opt, hit64 &hit, int64_t *st)
+{
+    if (!T.inst)
+        return triangle_filtered_obj(T, tri, g, o, d, t_min, t_max, opt, hit, st);
+    const double *xf = opt.inst_xf + dmapdev::kInstDoubles * (T.inst - 1);
+    const double ow[3] = {o.x, o.y, o.z}, dw[3] = {d.x, d.y, d.z};
+    double oo[3], od[3];
+    dmapdev::object_ray(xf, ow, dw, oo, od);
+    if (!triangle_filtered_obj(T, tri, g, V3(oo[0], oo[1], oo[2]), V3(od[0], od[1], od[2]), t_min, t_max, opt, hit,
+                               st))
+        return false;
+    dmapdev::world_normal(xf, hit.ng);
+    return true;
 }
 
 template <typename R>

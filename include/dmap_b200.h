@@ -152,14 +152,20 @@ dmap_status dmap_scene_create_charts(dmap_context *ctx, dmap_asset *const *asset
  * triangles: object o holds triangles object_first[o] .. object_first[o+1]-1
  * of tris_host / tri_asset_host (n_objects + 1 offsets). Instance k places
  * object instance_object[k] by the row-major 3x4 matrix instance_to_world +
- * 12 k (rotation R, translation t). The scene holds, for every instance in
- * order, its object's triangles moved to world space (positions R p + t,
- * vertex normals R m; texture coordinates and assets unchanged), so the
- * instances share the assets' pyramids; hit.tri counts through the
- * instances' triangles in that order. Only rigid transforms (R orthogonal
- * within 1e-9, mirrors included) are taken: a rigid motion moves the
- * displaced surface exactly, S = R (P + h N) + t = (R P + t) + h (R N); a
- * scale or shear would also scale the heights (DMAP_ERR_UNSUPPORTED).
+ * 12 k (linear part L, translation t). hit.tri counts through the
+ * instances' triangles in instance order; the instances share the assets'
+ * pyramids. When every L is a rotation (orthogonal within 1e-9, mirrors
+ * included), the scene holds each instance's triangles moved to world
+ * space (positions L p + t, vertex normals L m): a rigid motion moves the
+ * displaced surface exactly, S = L (P + h N) + t = (L P + t) + h (L N).
+ * Otherwise (a scale or shear, which would scale the heights if the base
+ * triangles were moved) every instance keeps its object's triangles and a
+ * ray meets them in object space, x = Linv (w - t) with t unchanged, as the
+ * reference's embree instancing hands the instanced geometry its ray; hit
+ * normals are returned in world space (sign(det L) Linv^T n, normalized),
+ * dmap_surface_points moves points and tangents by L, and
+ * dmap_tessellate_* refuse such a scene (DMAP_ERR_UNSUPPORTED). A singular
+ * L is DMAP_ERR_INVALID.
  */
 dmap_status dmap_scene_create_instanced(dmap_context *ctx, dmap_asset *const *assets, int n_assets,
                                         const int *tri_asset_host, const double *tris_host,
