@@ -284,6 +284,8 @@ def main():
     ap.add_argument("--requests", type=int, default=4096, help="serve: requests in the arrival trace")
     ap.add_argument("--interarrival-ms", type=float, default=15.0, help="serve: mean Poisson inter-arrival time")
     ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-request comparison")
+    ap.add_argument("--policy", default="oldest", choices=["oldest", "shortest"],
+                    help="serve: the server's slot-filling policy")
     ap.add_argument("--build", default="fold", choices=["fold", "direct"], help="pyramid: the build to time")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="keep --rounds / --blocks-per-sm instead of the autotuner's choice")
@@ -293,7 +295,7 @@ def main():
                     help="the FP32 path's certified leaf: the reference's FP64 leaf or the FP32 leaf")
     ap.add_argument("--order", default="nearest", choices=["nearest", "index"],
                     help="triangle order: nearest box entry first, or the reference's flat loop")
-    ap.add_argument("--rounds", type=int, default=6)
+    ap.add_argument("--rounds", type=int, default=2)
     ap.add_argument("--blocks-per-sm", type=int, default=5)
     ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
@@ -878,7 +880,7 @@ def run_serve(args, rank, world, local, dist):
     srv.close()
 
     # served
-    srv = dm.Server(ctx, hbm_budget_bytes=120 * 10 ** 9, slots=2, options=opt)
+    srv = dm.Server(ctx, hbm_budget_bytes=120 * 10 ** 9, slots=2, options=opt, policy=args.policy)
     ring_at, outstanding = 0, []
     t0 = time.perf_counter()
     with Clocks(local) as clk:
@@ -953,7 +955,7 @@ def run_serve(args, rank, world, local, dist):
                                    "60% primary / 30% path-traced (4 spp, depth 3) / 10% shadow-only, scenes: quad "
                                    f"{128 if small else 512}^2, cube sphere 96 x {256 if small else 2048}^2, "
                                    "cube sphere + ground + emitter (shared assets), 120 GB budget",
-                       "resident_scene_bytes": resident},
+                       "resident_scene_bytes": resident, "policy": args.policy},
             "served": served, "plain": plain, "plain_wavefront": plain_wave,
             "served_over_plain": (served["mrays_s"] / plain["mrays_s"]) if plain else None,
             "served_over_plain_wavefront": (served["mrays_s"] / plain_wave["mrays_s"]) if plain_wave else None,

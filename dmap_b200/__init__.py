@@ -107,7 +107,7 @@ TEXEL_FACE = np.dtype([("triangle", np.int32), ("interior", np.int32), ("st", np
 
 class _ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch_rays", C.c_int64), ("max_inflight", C.c_int),
-                ("slots", C.c_int), ("options", _Options)]
+                ("slots", C.c_int), ("options", _Options), ("policy", C.c_int)]
 
 
 class _ServerStats(C.Structure):
@@ -208,7 +208,7 @@ class TraversalOptions:
     mode: str = "closest"
     polish_cond: float = 1e4
     schedule: str = "wavefront"
-    rounds: int = 6
+    rounds: int = 2
     blocks_per_sm: int = 5
     order: str = "nearest"
     node_visit_cap: int = 0
@@ -546,9 +546,11 @@ class Server:
     Submitted buffers are kept alive here until their request completes."""
 
     def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_batch_rays: int = 0, max_inflight: int = 0,
-                 slots: int = 0, options: Optional[TraversalOptions] = None):
+                 slots: int = 0, options: Optional[TraversalOptions] = None, policy: str = "oldest"):
+        """policy: "oldest" (arrival order) or "shortest" (fewest queries left first)."""
         self.ctx = ctx
-        cfg = _ServerConfig(hbm_budget_bytes, max_batch_rays, max_inflight, slots, (options or TraversalOptions()).c())
+        cfg = _ServerConfig(hbm_budget_bytes, max_batch_rays, max_inflight, slots, (options or TraversalOptions()).c(),
+                            {"oldest": 0, "shortest": 1}[policy])
         h = C.c_void_p()
         ctx.check(lib().dmap_server_create(ctx.h, C.byref(cfg), C.byref(h)), "dmap_server_create")
         self.h = h

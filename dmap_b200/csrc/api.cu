@@ -89,7 +89,7 @@ void dmap_options_default(dmap_options *opt)
     opt->mode = DMAP_MODE_CLOSEST;
     opt->polish_cond = 1e4;
     opt->schedule = DMAP_SCHEDULE_WAVEFRONT;
-    opt->rounds = 6;
+    opt->rounds = 2;
     opt->blocks_per_sm = 5;
     opt->order = DMAP_ORDER_NEAREST;
     opt->node_visit_cap = 0;

@@ -171,15 +171,36 @@ struct dmap_server
         }
     }
 
-    // Puts the oldest admitted work into an idle slot; false when there is none.
+    // Queries a request has left to issue: its unsent rays, or a render's
+    // unsent batches' share of its paths times two queries per vertex.
+    static int64_t work_left(const Request *r)
+    {
+        if (r->kind == Kind::Rays)
+            return r->n - r->next;
+        const int64_t batches = render_batches(r->job), left = batches - render_enqueued(r->job);
+        const int64_t paths = (int64_t)r->desc.camera.width * r->desc.camera.height * r->desc.spp;
+        return batches > 0 ? paths * left / batches * 2 * r->desc.max_depth : 0;
+    }
+
+    // Puts admitted work into an idle slot: the oldest request's
+    // (DMAP_SERVE_OLDEST) or the one with the least work left
+    // (DMAP_SERVE_SHORTEST, the oldest of equals); false when there is none.
     bool fill(Slot &sl)
     {
         Request *first = nullptr;
+        int64_t first_left = 0;
         for (Request *r : active) {
-            if (r->kind == Kind::Rays ? r->next < r->n
-                                      : (!r->running && r->job && render_enqueued(r->job) < render_batches(r->job))) {
+            if (!(r->kind == Kind::Rays ? r->next < r->n
+                                        : (!r->running && r->job && render_enqueued(r->job) < render_batches(r->job))))
+                continue;
+            if (cfg.policy != DMAP_SERVE_SHORTEST) {
                 first = r;
                 break;
+            }
+            const int64_t left = work_left(r);
+            if (!first || left < first_left) {
+                first = r;
+                first_left = left;
             }
         }
         if (!first)
@@ -372,7 +393,8 @@ dmap_status dmap_server_create(dmap_context *ctx, const dmap_server_config *cfg,
     if (!ctx || !cfg || !out)
         return fail(ctx, DMAP_ERR_INVALID, "dmap_server_create: null argument");
     *out = nullptr;
-    if (cfg->max_batch_rays < 0 || cfg->max_inflight < 0 || cfg->slots < 0 || cfg->slots > 8)
+    if (cfg->max_batch_rays < 0 || cfg->max_inflight < 0 || cfg->slots < 0 || cfg->slots > 8 ||
+        (cfg->policy != DMAP_SERVE_OLDEST && cfg->policy != DMAP_SERVE_SHORTEST))
         return fail(ctx, DMAP_ERR_INVALID, "dmap_server_create: bad configuration");
     auto S = std::make_unique<dmap_server>();
     S->ctx = ctx;

@@ -230,7 +230,7 @@ typedef struct dmap_options {
                            reference's FP64 Newton (default 1e4) */
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
-                           default 6; 0 = one walk with every leaf inline) */
+                           default 2; 0 = one walk with every leaf inline) */
     int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 5, at most 5 resident) */
     int order;          /* DMAP_ORDER_*, default NEAREST */
     int node_visit_cap; /* FP32 path: cells one triangle's walk may visit before it gives up (0 = the default,
@@ -603,7 +603,17 @@ typedef struct dmap_server_config {
     int max_inflight;        /* admitted requests at once (0 = 256) */
     int slots;               /* launch slots in flight (0 = 2) */
     dmap_options options;    /* query options of every request (FP32 path) */
+    int policy;              /* which admitted request an idle slot serves first: DMAP_SERVE_* */
 } dmap_server_config;
+
+/* Slot-filling policies (no reference counterpart: the serving loop is this
+ * library's). OLDEST serves admitted requests in arrival order; SHORTEST
+ * serves the one with the fewest queries left to issue (the oldest of
+ * equals), so small requests overtake large ones that are in progress.
+ * Either way a launch packs every admitted ray request of the chosen one's
+ * scene and mode, and admission stays in arrival order. */
+#define DMAP_SERVE_OLDEST 0
+#define DMAP_SERVE_SHORTEST 1
 
 typedef struct dmap_server_stats {
     int64_t submitted, completed, failed, cancelled, queued, active;

@@ -153,3 +153,29 @@ def test_filter_cannot_change_under_served_requests(world):
     scene.set_opacity(None)
     srv.pause(False)
     srv.close()
+
+
+@pytest.mark.parametrize("policy", ["oldest", "shortest"])
+def test_policy_orders_the_slots(world, policy):
+    """With one slot and admission held, a large closest-hit request
+    submitted before a small occlusion request (different modes: never in
+    one launch) finishes first under the arrival-order policy and last under
+    the shortest-first one; both answer as they do alone."""
+    ctx, devs, pools, pt = world
+    srv = dm.Server(ctx, max_batch_rays=1024, slots=1, policy=policy)
+    srv.pause()
+    big_rays, small_rays = pools["sphere"][:12000], pools["sphere"][:300]
+    big, big_out = srv.submit_rays(devs["sphere"], big_rays, "closest")
+    small, small_out = srv.submit_rays(devs["sphere"], small_rays, "occluded")
+    srv.pause(False)
+    assert srv.drain(120.0) == 0
+    t_big, t_small = srv.latency_ms(big), srv.latency_ms(small)
+    if policy == "oldest":
+        assert t_small > t_big
+    else:
+        assert t_small < t_big
+    alone = devs["sphere"].intersect(big_rays, dm.TraversalOptions(), np.float32)
+    assert big_out.tobytes() == alone.tobytes()
+    occ = devs["sphere"].intersect(small_rays, dm.TraversalOptions(mode="occluded"), np.float32)
+    assert np.array_equal(small_out["tri"], occ["tri"])
+    srv.close()
