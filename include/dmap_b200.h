@@ -595,7 +595,10 @@ dmap_status dmap_render(dmap_scene *scene, const dmap_render_desc *desc, const d
  * fills the next, so requests that arrive mid-launch join the next launch.
  * Each result equals the one the request would get alone (a ray's answer
  * does not depend on the rays it shares a launch with; a render's image
- * does not depend on its batching). Latency is submit to completion.
+ * does not depend on its batching). Latency is submit to completion. The
+ * server's calls (submit, poll, wait, cancel, pause, drain, stats) may come
+ * from several threads at once: it is the entry point for concurrent
+ * callers of one device.
  */
 typedef struct dmap_server_config {
     size_t hbm_budget_bytes; /* device bytes the server may hold, scene assets included (0 = no limit) */
