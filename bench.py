@@ -296,7 +296,8 @@ def main():
     ap.add_argument("--order", default="nearest", choices=["nearest", "index"],
                     help="triangle order: nearest box entry first, or the reference's flat loop")
     ap.add_argument("--rounds", type=int, default=2)
-    ap.add_argument("--blocks-per-sm", type=int, default=5)
+    ap.add_argument("--blocks-per-sm", type=int, default=0,
+                    help="walk CTAs per SM (0: the occupancy the scene's walk is compiled for)")
     ap.add_argument("--small", action="store_true", help="reduced sizes for quick checks (not a bench number)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     args = ap.parse_args()

@@ -209,7 +209,7 @@ class TraversalOptions:
     polish_cond: float = 1e4
     schedule: str = "wavefront"
     rounds: int = 2
-    blocks_per_sm: int = 5
+    blocks_per_sm: int = 0
     order: str = "nearest"
     node_visit_cap: int = 0
     leaf_precision: str = "f32"

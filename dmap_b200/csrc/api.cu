@@ -90,7 +90,7 @@ void dmap_options_default(dmap_options *opt)
     opt->polish_cond = 1e4;
     opt->schedule = DMAP_SCHEDULE_WAVEFRONT;
     opt->rounds = 2;
-    opt->blocks_per_sm = 5;
+    opt->blocks_per_sm = 0;
     opt->order = DMAP_ORDER_NEAREST;
     opt->node_visit_cap = 0;
     opt->leaf_precision = DMAP_PRECISION_F32;

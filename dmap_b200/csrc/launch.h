@@ -18,7 +18,7 @@ struct QueryOpts
     int precision;            // DMAP_PRECISION_*
     int schedule;             // DMAP_SCHEDULE_*
     int rounds;               // wavefront: walk/leaf rounds before the inline-leaf drain
-    int blocks_per_sm;        // wavefront walk: resident 128-thread CTAs per SM
+    int blocks_per_sm;        // wavefront walk: 128-thread CTAs per SM (0: the walk's compiled occupancy)
     int order = 1;            // DMAP_ORDER_*: 0 index order, 1 nearest box entry first
     int guard_cap = 1 << 26;  // FP32 walk: cells one triangle walk may visit before it gives up
     int leaf_precision = 0;   // FP32 walk: DMAP_PRECISION_F64 (the reference's leaf) or _F32 (leaf32.cuh)

@@ -95,8 +95,9 @@ extern "C" dmap_status dmap_autotune(dmap_scene *s, const void *rays_dev, dmap_d
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     // rounds: how long rays park at leaves before the inline drain takes the
-    // rest; blocks per SM: resident walk warps (the kernels are compiled for
-    // at most 5 CTAs of 128 threads per SM)
+    // rest; blocks per SM: resident walk warps (the walk rounds are compiled
+    // for 4 CTAs of 128 threads per SM over the candidate mask, 5 over the
+    // triangle tree; more than that wait for a resident CTA to finish)
     const int rounds_c[] = {2, 3, 4, 6, 8, 12};
     const int bps_c[] = {3, 4, 5};
     t_best = 1e30;

@@ -61,7 +61,10 @@ cudaError_t launch(Args a, const WaveScratch &ws, cudaStream_t stream)
         rounds = kMaxRounds;
     if ((e = cudaMemsetAsync(ws.counters, 0, sizeof(unsigned long long) * kWaveCounters, stream)) != cudaSuccess)
         return e;
-    const int bps = a.opt.blocks_per_sm > 0 ? a.opt.blocks_per_sm : 4;
+    // blocks_per_sm 0: the occupancy the scene's walk is compiled for
+    const int bps = a.opt.blocks_per_sm > 0              ? a.opt.blocks_per_sm
+                    : a.n_tri > 32 * kMaskWords ? DMAP_WALK_TREE_MIN_BLOCKS
+                                                         : DMAP_WALK_MIN_BLOCKS;
     const int64_t need = (a.n + 127) / 128;
     a.grid = sm_count() * bps;
     if (need < a.grid)

@@ -61,9 +61,15 @@ using dmapdev::TriDev;
 using dmapdev::TriDev32;
 
 // Resident 128-thread CTAs per SM the walk and leaf kernels are compiled for
-// (register budget: 65536 / (128 x blocks) per thread).
+// (register budget: 65536 / (128 x blocks) per thread). The walk rounds over
+// the per-ray candidate mask (scenes of up to 256 triangles) take 4 (119
+// registers, no spills: faster than 5 at 96 registers with spills); over the
+// triangle tree, whose candidate buffer lives in local memory either way, 5.
 #ifndef DMAP_WALK_MIN_BLOCKS
-#define DMAP_WALK_MIN_BLOCKS 5
+#define DMAP_WALK_MIN_BLOCKS 4
+#endif
+#ifndef DMAP_WALK_TREE_MIN_BLOCKS
+#define DMAP_WALK_TREE_MIN_BLOCKS 5
 #endif
 #ifndef DMAP_LEAF_MIN_BLOCKS
 #define DMAP_LEAF_MIN_BLOCKS 1
@@ -390,15 +396,17 @@ __device__ __forceinline__ unsigned long long *round_ctr(unsigned long long *c, 
 // One lane's walk from its parked or fresh state to the next leaf (parked,
 // job written) or to the end of the ray. Every lane of the warp executes one
 // node test per step; lanes that finish take another ray.
-// The walk rounds are compiled for DMAP_WALK_MIN_BLOCKS CTAs per SM; the
-// last walk (INLINE_LEAF), which runs the few rays left with their leaves
-// inline, for DMAP_DRAIN_MIN_BLOCKS, so that the leaf it calls is not
-// squeezed into the rounds' register budget.
+// The walk rounds are compiled for DMAP_WALK_MIN_BLOCKS (mask) or
+// DMAP_WALK_TREE_MIN_BLOCKS (tree) CTAs per SM; the last walk (INLINE_LEAF),
+// which runs the few rays left with their leaves inline, for
+// DMAP_DRAIN_MIN_BLOCKS, so that the leaf it calls is not squeezed into the
+// rounds' register budget.
 #ifndef DMAP_DRAIN_MIN_BLOCKS
 #define DMAP_DRAIN_MIN_BLOCKS 2
 #endif
 template <bool ST, bool INLINE_LEAF, bool TREE, bool NEAR, typename R, typename H, typename Fp>
-__global__ void __launch_bounds__(128, INLINE_LEAF ? DMAP_DRAIN_MIN_BLOCKS : DMAP_WALK_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, INLINE_LEAF ? DMAP_DRAIN_MIN_BLOCKS
+                                                  : (TREE ? DMAP_WALK_TREE_MIN_BLOCKS : DMAP_WALK_MIN_BLOCKS))
     wave_walk(const TriDev32 *__restrict__ tris32, const TriDev *__restrict__ tris64, int n_tri,
               const AssetDev *__restrict__ assets, const R *__restrict__ rays, int64_t n, dmapk::QueryOpts opt,
               H *__restrict__ hits, int64_t *__restrict__ stats, RayState *__restrict__ states,

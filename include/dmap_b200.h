@@ -231,7 +231,9 @@ typedef struct dmap_options {
     int schedule;       /* DMAP_SCHEDULE_*, FP32 path only, default WAVEFRONT */
     int rounds;         /* wavefront: walk/leaf rounds before the last walk finishes the rest inline (0..32,
                            default 2; 0 = one walk with every leaf inline) */
-    int blocks_per_sm;  /* wavefront: resident 128-thread walk blocks per SM (default 5, at most 5 resident) */
+    int blocks_per_sm;  /* wavefront: 128-thread walk blocks per SM (0..16; default 0 = the occupancy the walk
+                           is compiled for: 4 on scenes of up to 256 triangles, 5 above, where the triangle
+                           tree takes the candidates) */
     int order;          /* DMAP_ORDER_*, default NEAREST */
     int node_visit_cap; /* FP32 path: cells one triangle's walk may visit before it gives up (0 = the default,
                            2^26, far above any walk of a well-formed scene). A ray whose walk gives up keeps
