@@ -197,3 +197,21 @@ def test_f32_nearest_tree_refills(ctx, oracle, k):
     h32 = dev.intersect(rays, dm.TraversalOptions(order="nearest"), np.float64)
     from test_gpu_leaf32 import judge
     judge(h32, ho, rays, sc.extent)
+
+
+@pytest.mark.parametrize("tree", [False, True])
+def test_f32_default_launch_shape(ctx, tree):
+    """blocks_per_sm 0 (the default) launches the walk at the occupancy it is
+    compiled for (4 CTAs per SM over the candidate mask, 5 over the triangle
+    tree); its records equal those of explicit launch shapes, fewer and more
+    CTAs than can be resident, bit for bit."""
+    assert dm.TraversalOptions().blocks_per_sm == 0
+    sc = scenes.cube_sphere_scene(16, 8 if tree else 4)   # 768 or 192 triangles
+    assert (len(sc.tris) > 256) == tree
+    dev = dm.Scene.from_synthetic(ctx, sc)
+    rays = scenes.sphere_camera_rays(128, 72)
+    ref = dev.intersect(rays, dm.TraversalOptions(), np.float64)
+    assert (ref["tri"] >= 0).sum() > 1000
+    for bps in (1, 3, 4, 5, 8):
+        got = dev.intersect(rays, dm.TraversalOptions(blocks_per_sm=bps), np.float64)
+        assert got.tobytes() == ref.tobytes(), bps
